@@ -1,0 +1,976 @@
+// capi.cu -- the C-ABI of include/avbd.h: context lifetime, set-up staging,
+// finalize (adjacency, coloring, HBM layout) and the step driver.
+//
+// Device layout chosen at finalize:
+//   * particles are renumbered color-major (internal order): every color is a
+//     contiguous slab [solved positional | oriented | fixed], so a color phase
+//     reads and writes its vertices' x, y and contact state with unit stride;
+//   * every solved vertex owns a contiguous run of 64-byte NeoHookean
+//     incidence records in slab order, streamed once per color phase;
+//   * one CUDA graph holds a whole fixed-iteration step.
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <thread>
+
+#include "engine.h"
+
+using namespace avbd;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_OR_FAIL(x)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (x);                                                                \
+        if (e_ != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace avbd {
+void count_launch(avbd_ctx* c, unsigned k) { c->stats.kernel_launches += k; }
+}
+
+static bool use64(const avbd_ctx* c) { return c->solver.precision == AVBD_PRECISION_FP64; }
+
+template <typename T>
+static int dalloc(avbd_ctx* c, T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    c->allocations.push_back((void*)*p);
+    return AVBD_OK;
+}
+
+static void free_device(avbd_ctx* c) {
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    for (void* p : c->allocations) cudaFree(p);
+    c->allocations.clear();
+    c->f = DevState<float>();
+    c->d = DevState<double>();
+    c->lbvh = LbvhState();
+    c->d_residual = nullptr;
+    c->d_h2d = nullptr;
+    c->h2d_cap = 0;
+    c->d_counters = nullptr;
+    c->d_perm = nullptr;
+    c->d_inv = nullptr;
+    c->d_error = nullptr;
+    c->finalized = false;
+    c->graph_dirty = true;
+}
+
+static int check_ctx(avbd_ctx* c) {
+    if (!c) return fail(AVBD_ERR_INVALID_ARG, "null context");
+    return AVBD_OK;
+}
+
+static int staging_only(avbd_ctx* c) {
+    if (c->finalized) {
+        // adding after finalize invalidates the device layout; it is rebuilt at the next finalize
+        free_device(c);
+    }
+    return AVBD_OK;
+}
+
+extern "C" {
+
+const char* avbd_last_error_string(void) { return g_err.c_str(); }
+const char* avbd_version(void) { return "avbd-b200 0.1 (sm_100a)"; }
+
+int avbd_create(avbd_ctx** out, int device, unsigned particles_capacity, unsigned oriented_capacity,
+                unsigned energies_capacity, unsigned primitives_capacity, unsigned sdf_capacity) {
+    if (!out) return fail(AVBD_ERR_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(AVBD_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(AVBD_ERR_INVALID_ARG, "bad device index");
+    CUDA_OR_FAIL(cudaSetDevice(device));
+    avbd_ctx* c = new avbd_ctx();
+    c->device = device;
+    c->cap_particles = particles_capacity;
+    c->cap_oriented = oriented_capacity;
+    c->cap_energies = energies_capacity;
+    c->cap_prims = primitives_capacity;
+    c->cap_sdf = sdf_capacity;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(AVBD_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return AVBD_OK;
+}
+
+int avbd_destroy(avbd_ctx* c) {
+    if (!c) return AVBD_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_device(c);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return AVBD_OK;
+}
+
+int avbd_set_stream(avbd_ctx* c, void* s) {
+    if (int r = check_ctx(c)) return r;
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    c->graph_dirty = true;
+    return AVBD_OK;
+}
+
+int avbd_set_params(avbd_ctx* c, const avbd_params* p) {
+    if (int r = check_ctx(c)) return r;
+    if (!p || !(p->dt > 0)) return fail(AVBD_ERR_INVALID_ARG, "dt must be positive");
+    c->params = *p;
+    c->graph_dirty = true;
+    return AVBD_OK;
+}
+
+int avbd_set_solver(avbd_ctx* c, const avbd_solver_params* s) {
+    if (int r = check_ctx(c)) return r;
+    if (!s) return fail(AVBD_ERR_INVALID_ARG, "null solver params");
+    if (s->precision != AVBD_PRECISION_FP32 && s->precision != AVBD_PRECISION_FP64)
+        return fail(AVBD_ERR_INVALID_ARG, "unknown precision");
+    if (c->finalized && s->precision != c->solver.precision) free_device(c);
+    c->solver = *s;
+    c->graph_dirty = true;
+    return AVBD_OK;
+}
+
+int avbd_begin_scene(avbd_ctx* c, unsigned* scene_index) {
+    if (int r = check_ctx(c)) return r;
+    staging_only(c);
+    unsigned n = (unsigned)c->mass.size();
+    if (c->scene_begin.back() != n) c->scene_begin.push_back(n);
+    if (scene_index) *scene_index = (unsigned)c->scene_begin.size() - 1;
+    return AVBD_OK;
+}
+
+int avbd_particles_add(avbd_ctx* c, unsigned n, const double* pos, const double* mass, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (n && (!pos || !mass)) return fail(AVBD_ERR_INVALID_ARG, "null positions/masses");
+    if (c->mass.size() + n > c->cap_particles) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    staging_only(c);
+    if (first) *first = (unsigned)c->mass.size();
+    c->x.insert(c->x.end(), pos, pos + 3ull * n);
+    c->v.insert(c->v.end(), 3ull * n, 0.0);
+    c->vp.insert(c->vp.end(), 3ull * n, 0.0);
+    c->mass.insert(c->mass.end(), mass, mass + n);
+    c->fixed.insert(c->fixed.end(), n, 0);
+    c->rot.insert(c->rot.end(), n, UINT32_MAX);
+    return AVBD_OK;
+}
+
+int avbd_particles_add_oriented(avbd_ctx* c, unsigned n, const double* pos, const double* rot, const double* mass,
+                                const double* inertia, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (n && (!rot || !inertia)) return fail(AVBD_ERR_INVALID_ARG, "null rotations/inertias");
+    unsigned no = (unsigned)c->inertia.size() / 3;
+    if (no + n > c->cap_oriented) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    unsigned f0 = 0;
+    if (int r = avbd_particles_add(c, n, pos, mass, &f0)) return r;
+    for (unsigned i = 0; i < n; i++) c->rot[f0 + i] = no + i;
+    c->q.insert(c->q.end(), rot, rot + 4ull * n);
+    c->inertia.insert(c->inertia.end(), inertia, inertia + 3ull * n);
+    if (first) *first = f0;
+    return AVBD_OK;
+}
+
+int avbd_particles_set_fixed(avbd_ctx* c, unsigned n, const unsigned* slots, const uint8_t* fixed) {
+    if (int r = check_ctx(c)) return r;
+    for (unsigned i = 0; i < n; i++)
+        if (slots[i] >= c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "particle index out of range");
+    staging_only(c);
+    for (unsigned i = 0; i < n; i++) c->fixed[slots[i]] = fixed ? fixed[i] : 1;
+    return AVBD_OK;
+}
+
+int avbd_num_particles(avbd_ctx* c, unsigned* n) {
+    if (int r = check_ctx(c)) return r;
+    *n = (unsigned)c->mass.size();
+    return AVBD_OK;
+}
+
+// ------------------------------------------------------------- energies
+int avbd_neo_hookean_add(avbd_ctx* c, unsigned n, const unsigned* idx, const double* lam, const double* mu,
+                         const double* kd, const double* Q, const double* V, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (c->nh.size() + n > c->cap_energies) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    size_t np = c->mass.size();
+    for (size_t i = 0; i < 4ull * n; i++)
+        if (idx[i] >= np) return fail(AVBD_ERR_INVALID_ARG, "tet particle index out of range");
+    staging_only(c);
+    if (first) *first = (unsigned)c->nh.size();
+    for (unsigned i = 0; i < n; i++) {
+        HostNH e;
+        for (int k = 0; k < 4; k++) e.idx[k] = idx[4 * i + k];
+        e.lambda = lam[i];
+        e.mu = mu[i];
+        e.kd = kd[i];
+        for (int k = 0; k < 9; k++) e.Q[k] = Q[9 * i + k];
+        e.V = V[i];
+        c->nh.push_back(e);
+    }
+    return AVBD_OK;
+}
+
+int avbd_ground_collision_add(avbd_ctx* c, unsigned n, const unsigned* p, const double* ks, const double* ms,
+                              const double* mk, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (c->ground.size() + n > c->cap_energies) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    for (unsigned i = 0; i < n; i++)
+        if (p[i] >= c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "particle index out of range");
+    staging_only(c);
+    if (first) *first = (unsigned)c->ground.size();
+    for (unsigned i = 0; i < n; i++) c->ground.push_back(HostGround{p[i], ks[i], ms[i], mk[i]});
+    return AVBD_OK;
+}
+
+int avbd_cosserat_rod_add(avbd_ctx* c, unsigned n, const unsigned* idx, const double* K, const double* L,
+                          const double* kappa, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (c->rods.size() + n > c->cap_energies) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    for (size_t i = 0; i < 2ull * n; i++)
+        if (idx[i] >= c->mass.size() || c->rot[idx[i]] == UINT32_MAX)
+            return fail(AVBD_ERR_INVALID_ARG, "rod element needs oriented particles");
+    staging_only(c);
+    if (first) *first = (unsigned)c->rods.size();
+    for (unsigned i = 0; i < n; i++) {
+        HostRod e;
+        e.idx[0] = idx[2 * i];
+        e.idx[1] = idx[2 * i + 1];
+        for (int k = 0; k < 6; k++) e.K[k] = K[6 * i + k];
+        e.L = L[i];
+        for (int k = 0; k < 3; k++) e.kappa[k] = kappa[3 * i + k];
+        c->rods.push_back(e);
+    }
+    return AVBD_OK;
+}
+
+int avbd_rigid_body_ground_collision_add(avbd_ctx* c, unsigned n, const unsigned* p, const uint8_t* shape,
+                                         const double* radius, const double* cp, const double* ks, const double* ms,
+                                         const double* mk, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (c->rground.size() + n > c->cap_energies) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    for (unsigned i = 0; i < n; i++)
+        if (p[i] >= c->mass.size() || c->rot[p[i]] == UINT32_MAX)
+            return fail(AVBD_ERR_INVALID_ARG, "rigid-body ground contact needs an oriented particle");
+    staging_only(c);
+    if (first) *first = (unsigned)c->rground.size();
+    for (unsigned i = 0; i < n; i++) {
+        HostRGround e;
+        e.p = p[i];
+        e.shape = shape[i];
+        e.radius = radius[i];
+        for (int k = 0; k < 3; k++) e.cp[k] = cp[3 * i + k];
+        e.k_start = ks[i];
+        e.mu_s = ms[i];
+        e.mu_k = mk[i];
+        c->rground.push_back(e);
+    }
+    return AVBD_OK;
+}
+
+int avbd_one_sided_fixed_joint_add(avbd_ctx* c, unsigned n, const unsigned* p, const double* po, const double* ro,
+                                   const double* rp, const double* rq, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (c->joints.size() + n > c->cap_energies) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    for (unsigned i = 0; i < n; i++)
+        if (p[i] >= c->mass.size() || c->rot[p[i]] == UINT32_MAX)
+            return fail(AVBD_ERR_INVALID_ARG, "joint needs an oriented particle");
+    staging_only(c);
+    if (first) *first = (unsigned)c->joints.size();
+    for (unsigned i = 0; i < n; i++) {
+        HostJoint e;
+        e.p = p[i];
+        for (int k = 0; k < 3; k++) { e.po[k] = po[3 * i + k]; e.rp[k] = rp[3 * i + k]; }
+        for (int k = 0; k < 4; k++) { e.ro[k] = ro[4 * i + k]; e.rq[k] = rq[4 * i + k]; }
+        c->joints.push_back(e);
+    }
+    return AVBD_OK;
+}
+
+static int add_prims(avbd_ctx* c, unsigned n, uint8_t type, const unsigned* idx, int k, const double* radius,
+                     double rconst, const unsigned* obj, unsigned objconst, unsigned* first) {
+    if (int r = check_ctx(c)) return r;
+    if (c->prims.size() + n > c->cap_prims) return fail(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    for (size_t i = 0; i < (size_t)k * n; i++)
+        if (idx[i] >= c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "primitive particle index out of range");
+    staging_only(c);
+    if (first) *first = (unsigned)c->prims.size();
+    for (unsigned i = 0; i < n; i++) {
+        HostPrim p{};
+        p.type = type;
+        for (int j = 0; j < k; j++) p.idx[j] = idx[k * i + j];
+        p.object_id = obj ? obj[i] : objconst;
+        p.radius = radius ? radius[i] : rconst;
+        c->prims.push_back(p);
+    }
+    return AVBD_OK;
+}
+
+int avbd_collision_add_triangles(avbd_ctx* c, unsigned n, const unsigned* idx, unsigned object_id, unsigned* first) {
+    return add_prims(c, n, AVBD_SHAPE_TRIANGLE, idx, 3, nullptr, 0.0, nullptr, object_id, first);
+}
+int avbd_collision_add_rod_segments(avbd_ctx* c, unsigned n, const unsigned* idx, double radius, unsigned object_id,
+                                    unsigned* first) {
+    return add_prims(c, n, AVBD_SHAPE_ROD_SEGMENT, idx, 2, nullptr, radius, nullptr, object_id, first);
+}
+int avbd_collision_add_spheres(avbd_ctx* c, unsigned n, const unsigned* p, const double* radius,
+                               const unsigned* object_id, unsigned* first) {
+    for (unsigned i = 0; i < n; i++)
+        if (p[i] >= c->mass.size() || c->rot[p[i]] == UINT32_MAX)
+            return fail(AVBD_ERR_INVALID_ARG, "sphere primitive needs an oriented particle");
+    return add_prims(c, n, AVBD_SHAPE_SPHERE, p, 1, radius, 0.0, object_id, 0, first);
+}
+
+}  // extern "C"
+
+// ============================================================== finalize
+
+namespace {
+
+// Vertex-vertex adjacency of the static energies (StaticParticleAdjacency::
+// buildAdjacency, common/StaticParticleAdjacency.hpp:42-133): the distinct
+// other particles of every energy a particle belongs to.
+void build_neighbors(avbd_ctx* c, const std::vector<unsigned>& inc_off, const std::vector<uint32_t>& inc_tet,
+                     std::vector<unsigned>& p_off, std::vector<unsigned>& p_nbr) {
+    const unsigned n = (unsigned)c->mass.size();
+    // rod neighbours
+    std::vector<std::vector<unsigned>> rodn;
+    if (!c->rods.empty()) {
+        rodn.resize(n);
+        for (auto& e : c->rods) {
+            rodn[e.idx[0]].push_back(e.idx[1]);
+            rodn[e.idx[1]].push_back(e.idx[0]);
+        }
+    }
+    std::vector<unsigned> deg(n, 0);
+    std::vector<std::vector<unsigned>> lists;
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n < 20000) nt = 1;
+    std::vector<std::vector<unsigned>> chunk_nbr(nt);
+    std::vector<std::vector<unsigned>> chunk_deg(nt);
+    auto work = [&](unsigned t) {
+        unsigned b = (unsigned)((uint64_t)n * t / nt), e = (unsigned)((uint64_t)n * (t + 1) / nt);
+        std::vector<unsigned> tmp;
+        auto& out = chunk_nbr[t];
+        auto& dg = chunk_deg[t];
+        for (unsigned p = b; p < e; p++) {
+            tmp.clear();
+            for (unsigned k = inc_off[p]; k < inc_off[p + 1]; k++) {
+                const HostNH& h = c->nh[inc_tet[k]];
+                for (int j = 0; j < 4; j++)
+                    if (h.idx[j] != p) tmp.push_back(h.idx[j]);
+            }
+            if (!rodn.empty())
+                for (unsigned q : rodn[p]) if (q != p) tmp.push_back(q);
+            std::sort(tmp.begin(), tmp.end());
+            tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+            dg.push_back((unsigned)tmp.size());
+            out.insert(out.end(), tmp.begin(), tmp.end());
+        }
+    };
+    if (nt == 1) work(0);
+    else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; t++) th.emplace_back(work, t);
+        for (auto& t : th) t.join();
+    }
+    p_off.assign(n + 1, 0);
+    size_t total = 0;
+    for (unsigned t = 0; t < nt; t++) total += chunk_nbr[t].size();
+    p_nbr.clear();
+    p_nbr.reserve(total);
+    unsigned p = 0;
+    for (unsigned t = 0; t < nt; t++) {
+        for (unsigned d : chunk_deg[t]) { p_off[p + 1] = p_off[p] + d; p++; }
+        p_nbr.insert(p_nbr.end(), chunk_nbr[t].begin(), chunk_nbr[t].end());
+    }
+}
+
+template <typename R>
+int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_off,
+                 const std::vector<uint32_t>& inc_tet, const std::vector<uint16_t>& inc_local,
+                 const std::vector<int>& ground_of) {
+    using V4 = typename Vec4Of<R>::T;
+    const unsigned n = (unsigned)c->mass.size();
+    s.n = n;
+    std::vector<V4> x(n), y(n), v(n), vp(n);
+    std::vector<uint8_t> flags(n, 0);
+    for (unsigned i = 0; i < n; i++) {
+        unsigned e = c->perm[i];
+        V3<R> xe = mk3<R>((R)c->x[3 * e], (R)c->x[3 * e + 1], (R)c->x[3 * e + 2]);
+        x[i] = make4<R>(xe, R(0));
+        y[i] = make4<R>(xe, (R)c->mass[e]);
+        v[i] = make4<R>(mk3<R>((R)c->v[3 * e], (R)c->v[3 * e + 1], (R)c->v[3 * e + 2]), R(0));
+        vp[i] = make4<R>(mk3<R>((R)c->vp[3 * e], (R)c->vp[3 * e + 1], (R)c->vp[3 * e + 2]), R(0));
+        uint8_t f = 0;
+        if (c->fixed[e]) f |= VF_FIXED;
+        if (c->rot[e] != UINT32_MAX) f |= VF_ORIENTED;
+        if (ground_of[e] >= 0) f |= VF_GROUND;
+        flags[i] = f;
+    }
+    // incidence records in internal order; only solved positional vertices get records
+    std::vector<uint32_t> begin(n + 1, 0);
+    for (unsigned i = 0; i < n; i++) {
+        unsigned e = c->perm[i];
+        bool solved = !(flags[i] & (VF_FIXED | VF_ORIENTED));
+        begin[i + 1] = begin[i] + (solved ? inc_off[e + 1] - inc_off[e] : 0);
+    }
+    const size_t nrec = begin[n];
+    std::vector<IncRec<R>> rec(nrec);
+    {
+        unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        if (n < 20000) nt = 1;
+        auto work = [&](unsigned t) {
+            unsigned b = (unsigned)((uint64_t)n * t / nt), en = (unsigned)((uint64_t)n * (t + 1) / nt);
+            for (unsigned i = b; i < en; i++) {
+                unsigned e = c->perm[i];
+                if (begin[i + 1] == begin[i]) continue;
+                size_t w = begin[i];
+                for (unsigned k = inc_off[e]; k < inc_off[e + 1]; k++, w++) {
+                    const HostNH& h = c->nh[inc_tet[k]];
+                    unsigned loc = inc_local[k];
+                    double D[4][3];
+                    for (int j = 0; j < 3; j++) {
+                        D[0][j] = h.Q[0 * 3 + j];
+                        D[1][j] = h.Q[1 * 3 + j];
+                        D[2][j] = h.Q[2 * 3 + j];
+                        D[3][j] = -(h.Q[j] + h.Q[3 + j] + h.Q[6 + j]);
+                    }
+                    IncRec<R>& r = rec[w];
+                    int o = 0;
+                    for (int j = 0; j < 4; j++) {
+                        if ((unsigned)j == loc) continue;
+                        r.o[o] = c->inv[h.idx[j]];
+                        r.d[3 * o] = (R)D[j][0];
+                        r.d[3 * o + 1] = (R)D[j][1];
+                        r.d[3 * o + 2] = (R)D[j][2];
+                        o++;
+                    }
+                    r.tet = inc_tet[k];
+                    r.vlam = (R)(h.V * h.lambda);
+                    r.vmu = (R)(h.V * h.mu);
+                    r.shift = (R)(h.mu / h.lambda + 1.0);
+                }
+            }
+        };
+        if (nt == 1) work(0);
+        else {
+            std::vector<std::thread> th;
+            for (unsigned t = 0; t < nt; t++) th.emplace_back(work, t);
+            for (auto& t : th) t.join();
+        }
+    }
+    int rc;
+    if ((rc = dalloc(c, &s.x, n)) || (rc = dalloc(c, &s.y, n)) || (rc = dalloc(c, &s.xp, n)) ||
+        (rc = dalloc(c, &s.xl, n)) || (rc = dalloc(c, &s.xll, n)) || (rc = dalloc(c, &s.v, n)) ||
+        (rc = dalloc(c, &s.vp, n)) || (rc = dalloc(c, &s.flags, n)) || (rc = dalloc(c, &s.inc, nrec)) ||
+        (rc = dalloc(c, &s.inc_begin, n + 1)))
+        return rc;
+    cudaStream_t st = c->stream;
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.x, x.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.y, y.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.xp, x.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.xl, x.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.xll, x.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.v, v.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.vp, vp.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.flags, flags.data(), n, cudaMemcpyHostToDevice, st));
+    if (nrec) CUDA_OR_FAIL(cudaMemcpyAsync(s.inc, rec.data(), sizeof(IncRec<R>) * nrec, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaMemcpyAsync(s.inc_begin, begin.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));
+
+    // ground contact, one record per particle (internal order)
+    if (!c->ground.empty()) {
+        std::vector<V4> gk(n), glam(n), gcp(n);
+        std::vector<uint8_t> gfl(n, 0);
+        for (unsigned i = 0; i < n; i++) {
+            int gi = ground_of[c->perm[i]];
+            if (gi < 0) {
+                gk[i] = make4<R>(mk3<R>(0, 0, 0), R(0));
+                glam[i] = gk[i];
+                gcp[i] = gk[i];
+                continue;
+            }
+            const HostGround& g = c->ground[gi];
+            gk[i] = make4<R>(mk3<R>((R)g.k_start, (R)g.k_start, (R)g.k_start), (R)g.k_start);
+            glam[i] = make4<R>(mk3<R>(0, 0, 0), R(0));
+            gcp[i] = make4<R>(mk3<R>(0, 0, (R)g.mu_s), (R)g.mu_k);
+        }
+        if ((rc = dalloc(c, &s.gk, n)) || (rc = dalloc(c, &s.glam, n)) || (rc = dalloc(c, &s.gcp, n)) ||
+            (rc = dalloc(c, &s.gflag, n)))
+            return rc;
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.gk, gk.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.glam, glam.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.gcp, gcp.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.gflag, gfl.data(), n, cudaMemcpyHostToDevice, st));
+    }
+    // per-tet data for strain-rate damping
+    s.ntets = 0;
+    if (c->damping) {
+        const unsigned nt = (unsigned)c->nh.size();
+        std::vector<uint4> ti(nt);
+        std::vector<V4> tq(3ull * nt), te(2ull * nt);
+        for (unsigned t = 0; t < nt; t++) {
+            const HostNH& h = c->nh[t];
+            ti[t] = make_uint4(c->inv[h.idx[0]], c->inv[h.idx[1]], c->inv[h.idx[2]], c->inv[h.idx[3]]);
+            for (int r = 0; r < 3; r++)
+                tq[3 * t + r] = make4<R>(mk3<R>((R)h.Q[3 * r], (R)h.Q[3 * r + 1], (R)h.Q[3 * r + 2]), R(0));
+            te[2 * t] = make4<R>(mk3<R>(0, 0, 0), R(0));
+            te[2 * t + 1] = make4<R>(mk3<R>(0, 0, (R)(h.V * h.kd)), R(0));
+        }
+        if ((rc = dalloc(c, &s.tet_idx, nt)) || (rc = dalloc(c, &s.tet_q, 3ull * nt)) ||
+            (rc = dalloc(c, &s.tet_e, 2ull * nt)))
+            return rc;
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.tet_idx, ti.data(), sizeof(uint4) * nt, cudaMemcpyHostToDevice, st));
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.tet_q, tq.data(), sizeof(V4) * 3 * nt, cudaMemcpyHostToDevice, st));
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.tet_e, te.data(), sizeof(V4) * 2 * nt, cudaMemcpyHostToDevice, st));
+        s.ntets = nt;
+    }
+    s.err = c->d_error;
+    CUDA_OR_FAIL(cudaStreamSynchronize(st));
+    return AVBD_OK;
+}
+
+}  // namespace
+
+extern "C" int avbd_finalize(avbd_ctx* c) {
+    if (int r = check_ctx(c)) return r;
+    CUDA_OR_FAIL(cudaSetDevice(c->device));
+    free_device(c);
+    const unsigned n = (unsigned)c->mass.size();
+    if (n == 0) return fail(AVBD_ERR_STATE, "no particles");
+    if (!c->rods.empty() || !c->rground.empty() || !c->joints.empty())
+        return fail(AVBD_ERR_UNSUPPORTED, "oriented-particle energies are not enabled in this build");
+    for (auto& p : c->prims)
+        if (p.type != AVBD_SHAPE_TRIANGLE)
+            return fail(AVBD_ERR_UNSUPPORTED, "only triangle collision primitives are enabled in this build");
+
+    // scenes: [scene_begin[s], scene_begin[s+1])
+    std::vector<unsigned> sb = c->scene_begin;
+    if (sb.back() != n) sb.push_back(n);
+    std::vector<unsigned> scene_of(n);
+    for (size_t s = 0; s + 1 < sb.size(); s++)
+        for (unsigned p = sb[s]; p < sb[s + 1]; p++) scene_of[p] = (unsigned)s;
+
+    // NeoHookean incidences per particle, in pool-slot order
+    // (StaticParticleAdjacency::buildAdjacency scatter, common/StaticParticleAdjacency.hpp:100-118)
+    std::vector<unsigned> inc_off(n + 1, 0);
+    c->damping = false;
+    for (auto& h : c->nh) {
+        for (int k = 0; k < 4; k++) inc_off[h.idx[k] + 1]++;
+        if (h.kd != 0) c->damping = true;
+        unsigned s0 = scene_of[h.idx[0]];
+        for (int k = 1; k < 4; k++)
+            if (scene_of[h.idx[k]] != s0) return fail(AVBD_ERR_INVALID_ARG, "energy spans two scenes");
+        if (!(h.lambda != 0)) return fail(AVBD_ERR_INVALID_ARG, "NeoHookean lambda must be non-zero");
+    }
+    for (unsigned p = 0; p < n; p++) inc_off[p + 1] += inc_off[p];
+    std::vector<uint32_t> inc_tet(inc_off[n]);
+    std::vector<uint16_t> inc_local(inc_off[n]);
+    {
+        std::vector<unsigned> cur(inc_off.begin(), inc_off.end() - 1);
+        for (unsigned t = 0; t < c->nh.size(); t++)
+            for (int k = 0; k < 4; k++) {
+                unsigned p = c->nh[t].idx[k];
+                inc_tet[cur[p]] = t;
+                inc_local[cur[p]] = (uint16_t)k;
+                cur[p]++;
+            }
+    }
+    std::vector<int> ground_of(n, -1);
+    for (unsigned g = 0; g < c->ground.size(); g++) {
+        unsigned p = c->ground[g].p;
+        if (ground_of[p] >= 0)
+            return fail(AVBD_ERR_UNSUPPORTED, "more than one ground energy on a particle");
+        ground_of[p] = (int)g;
+    }
+
+    // coloring
+    std::vector<unsigned> p_off, p_nbr;
+    build_neighbors(c, inc_off, inc_tet, p_off, p_nbr);
+    for (unsigned p = 0; p < n; p++)
+        if (p_off[p + 1] - p_off[p] > 0xFFFFu) return fail(AVBD_ERR_UNSUPPORTED, "vertex degree above 65535");
+    {
+        std::string err;
+        int rc = gpu_dsatur(p_off, p_nbr, sb, c->color, c->num_colors, c->stream, err);
+        if (rc) return fail(rc, err);
+    }
+
+    // color-major permutation: [solved positional | oriented | fixed] per color
+    const unsigned nc = c->num_colors;
+    std::vector<unsigned> cnt(3ull * nc, 0);
+    auto cls = [&](unsigned e) -> int {
+        if (c->fixed[e]) return 2;
+        if (c->rot[e] != UINT32_MAX) return 1;
+        return 0;
+    };
+    for (unsigned e = 0; e < n; e++) cnt[3ull * c->color[e] + cls(e)]++;
+    c->color_begin.assign(nc + 1, 0);
+    c->color_solve.assign(nc, 0);
+    std::vector<unsigned> cur(3ull * nc);
+    unsigned run = 0;
+    for (unsigned k = 0; k < nc; k++) {
+        c->color_begin[k] = run;
+        c->color_solve[k] = cnt[3ull * k];
+        for (int t = 0; t < 3; t++) { cur[3ull * k + t] = run; run += cnt[3ull * k + t]; }
+    }
+    c->color_begin[nc] = run;
+    c->max_color_solve = *std::max_element(c->color_solve.begin(), c->color_solve.end());
+    c->perm.assign(n, 0);
+    c->inv.assign(n, 0);
+    for (unsigned e = 0; e < n; e++) {
+        unsigned i = cur[3ull * c->color[e] + cls(e)]++;
+        c->perm[i] = e;
+        c->inv[e] = i;
+    }
+
+    // device buffers
+    int rc;
+    if ((rc = dalloc(c, &c->d_counters, 4)) || (rc = dalloc(c, &c->d_residual, 4)) ||
+        (rc = dalloc(c, &c->d_perm, n)) || (rc = dalloc(c, &c->d_inv, n)) || (rc = dalloc(c, &c->d_error, 1)))
+        return rc;
+    CUDA_OR_FAIL(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    CUDA_OR_FAIL(cudaMemsetAsync(c->d_error, 0, sizeof(int), c->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(c->d_perm, c->perm.data(), sizeof(unsigned) * n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(c->d_inv, c->inv.data(), sizeof(unsigned) * n, cudaMemcpyHostToDevice, c->stream));
+    rc = use64(c) ? upload_state<double>(c, c->d, inc_off, inc_tet, inc_local, ground_of)
+                  : upload_state<float>(c, c->f, inc_off, inc_tet, inc_local, ground_of);
+    if (rc) return rc;
+    if (!c->prims.empty()) {
+        std::string err;
+        if (int r2 = lbvh_allocate(c, err)) return fail(r2, err);
+    }
+    c->stats.num_colors = nc;
+    c->stats.num_scenes = (unsigned)sb.size() - 1;
+    c->finalized = true;
+    c->graph_dirty = true;
+    return AVBD_OK;
+}
+
+// ================================================================== step
+
+namespace {
+
+double omega_at(unsigned i, double rho, double prev) {
+    // Chebyshev schedule (simulation/VBDSolver.hpp:69-74)
+    if (i > 2) return 4 / (4 - rho * rho * prev);
+    if (i == 2) return 2 / (2 - rho * rho);
+    return 1;
+}
+
+template <typename R>
+void enqueue_iteration(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st) {
+    for (unsigned col = 0; col < c->num_colors; col++)
+        if (c->color_solve[col]) launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st);
+    launch_chebyshev_dual<R>(c, s, k, omega, st);
+}
+
+template <typename R>
+void enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
+    if (c->damping) launch_tet_eprev<R>(c, s, k, st);
+    launch_begin_step<R>(c, s, k, st);
+    double omega = 1;
+    for (unsigned i = 0; i < c->solver.solver_iters; i++) {
+        omega = omega_at(i, c->solver.iter_acceleration, omega);
+        enqueue_iteration<R>(c, s, k, omega, st);
+    }
+    launch_velocity<R>(c, s, k, st);
+}
+
+StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_accel, c->kappa_max}; }
+
+template <typename R>
+int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
+    StepConsts k = consts(c);
+    cudaStream_t st = c->stream;
+    if (c->solver.residual_tolerance > 0) {
+        // run-to-tolerance: the residual is checked on the host after every sweep
+        unsigned max_it = c->solver.max_iters ? c->solver.max_iters : 1000;
+        for (unsigned t = 0; t < n_steps; t++) {
+            if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
+            if (c->damping) launch_tet_eprev<R>(c, s, k, st);
+            launch_begin_step<R>(c, s, k, st);
+            double omega = 1;
+            unsigned it = 0;
+            for (; it < max_it;) {
+                omega = omega_at(it, c->solver.iter_acceleration, omega);
+                enqueue_iteration<R>(c, s, k, omega, st);
+                it++;
+                launch_residual<R>(c, s, k, c->d_residual, st);
+                double h[2];
+                CUDA_OR_FAIL(cudaMemcpyAsync(h, c->d_residual, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+                CUDA_OR_FAIL(cudaStreamSynchronize(st));
+                double R2 = h[1] > 0 ? std::sqrt(h[0]) / std::sqrt(h[1]) : std::sqrt(h[0]);
+                c->stats.last_residual = R2;
+                if (R2 <= c->solver.residual_tolerance) break;
+            }
+            c->stats.iterations += it;
+            launch_velocity<R>(c, s, k, st);
+        }
+        return AVBD_OK;
+    }
+    bool capturable = c->use_graph && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+    if (capturable && (c->graph_dirty || !c->graph)) {
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+        unsigned long long before = c->stats.kernel_launches;
+        cudaGraph_t g;
+        CUDA_OR_FAIL(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue_step_fixed<R>(c, s, k, st);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        c->launches_per_step = c->stats.kernel_launches - before;
+        c->stats.kernel_launches = before;
+        c->graph_dirty = false;
+    }
+    for (unsigned t = 0; t < n_steps; t++) {
+        if (capturable) {
+            CUDA_OR_FAIL(cudaGraphLaunch(c->graph, st));
+            c->stats.kernel_launches += c->launches_per_step;
+        } else {
+            enqueue_step_fixed<R>(c, s, k, st);
+        }
+        c->stats.iterations += c->solver.solver_iters;
+    }
+    CUDA_OR_FAIL(cudaGetLastError());
+    return AVBD_OK;
+}
+
+int device_error(avbd_ctx* c) {
+    int h = 0;
+    if (!c->d_error) return AVBD_OK;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&h, c->d_error, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    if (h == AVBD_ERR_NAN) return fail(h, "non-finite particle state");
+    if (h == AVBD_ERR_UNSUPPORTED_PAIR) return fail(h, "Unsupported collision!");
+    if (h) return fail(h, "device-side error");
+    return AVBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int avbd_step(avbd_ctx* c, unsigned n_steps) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "avbd_finalize must run before avbd_step");
+    CUDA_OR_FAIL(cudaSetDevice(c->device));
+    return use64(c) ? step_impl<double>(c, c->d, n_steps) : step_impl<float>(c, c->f, n_steps);
+}
+
+int avbd_synchronize(avbd_ctx* c) {
+    if (int r = check_ctx(c)) return r;
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return device_error(c);
+}
+
+int avbd_collision_stage(avbd_ctx* c) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (c->prims.empty()) return AVBD_OK;
+    if (use64(c)) lbvh_stage<double>(c, c->d, c->stream);
+    else lbvh_stage<float>(c, c->f, c->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    return avbd_synchronize(c);
+}
+
+int avbd_get_stats(avbd_ctx* c, avbd_stats* out) {
+    if (int r = check_ctx(c)) return r;
+    if (!out) return fail(AVBD_ERR_INVALID_ARG, "null stats");
+    if (c->finalized) {
+        unsigned long long h[4] = {0, 0, 0, 0};
+        CUDA_OR_FAIL(cudaMemcpyAsync(h, c->d_counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        if (c->lbvh.pair_count) {
+            uint32_t pc = 0;
+            CUDA_OR_FAIL(cudaMemcpyAsync(&pc, c->lbvh.pair_count, sizeof(pc), cudaMemcpyDeviceToHost, c->stream));
+            CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+            c->stats.candidate_pairs = pc;
+        }
+        CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+        c->stats.fp64_fallbacks = h[0];
+    }
+    *out = c->stats;
+    return AVBD_OK;
+}
+
+// ----------------------------------------------------------- state I/O
+static int ensure_h2d(avbd_ctx* c, size_t doubles) {
+    if (c->h2d_cap >= doubles) return AVBD_OK;
+    if (c->d_h2d) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->d_h2d);
+        c->allocations.erase(std::find(c->allocations.begin(), c->allocations.end(), (void*)c->d_h2d));
+        c->d_h2d = nullptr;
+    }
+    if (int r = dalloc(c, &c->d_h2d, doubles)) return r;
+    c->h2d_cap = doubles;
+    return AVBD_OK;
+}
+
+static int load_dev(avbd_ctx* c, const double* src, unsigned first, unsigned n, int mode) {
+    size_t nd = mode == 2 ? 6ull * n : 3ull * n;
+    if (int r = ensure_h2d(c, nd)) return r;
+    if (mode == 2) {
+        CUDA_OR_FAIL(cudaMemcpyAsync(c->d_h2d, src, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+        CUDA_OR_FAIL(cudaMemcpyAsync(c->d_h2d + 3ull * n, src + 3ull * n, sizeof(double) * 3 * n,
+                                     cudaMemcpyHostToDevice, c->stream));
+    } else {
+        CUDA_OR_FAIL(cudaMemcpyAsync(c->d_h2d, src, sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (use64(c)) launch_load_positions<double>(c->d, c->d_h2d, c->d_inv, first, n, mode, c->stream);
+    else launch_load_positions<float>(c->f, c->d_h2d, c->d_inv, first, n, mode, c->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    return AVBD_OK;
+}
+
+int avbd_set_positions(avbd_ctx* c, unsigned first, unsigned n, const double* pos) {
+    if (int r = check_ctx(c)) return r;
+    if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
+    std::copy(pos, pos + 3ull * n, c->x.begin() + 3ull * first);
+    if (!c->finalized) return AVBD_OK;
+    return load_dev(c, pos, first, n, 1);
+}
+
+int avbd_set_velocities(avbd_ctx* c, unsigned first, unsigned n, const double* v, const double* vp) {
+    if (int r = check_ctx(c)) return r;
+    if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
+    if (!vp) vp = v;
+    std::copy(v, v + 3ull * n, c->v.begin() + 3ull * first);
+    std::copy(vp, vp + 3ull * n, c->vp.begin() + 3ull * first);
+    if (!c->finalized) return AVBD_OK;
+    std::vector<double> both(6ull * n);
+    std::copy(v, v + 3ull * n, both.begin());
+    std::copy(vp, vp + 3ull * n, both.begin() + 3ull * n);
+    int r = load_dev(c, both.data(), first, n, 2);
+    if (r) return r;
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return AVBD_OK;
+}
+
+// Per-step drop-in upload of the host-owned state: positions and velocities
+// of all particles (velocities also become the previous velocities' source
+// only through the step itself).
+int avbd_set_state(avbd_ctx* c, const double* pos, const double* vel) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    unsigned n = (unsigned)c->mass.size();
+    if (pos)
+        if (int r = load_dev(c, pos, 0, n, 0)) return r;
+    if (vel) {
+        size_t nd = 3ull * n;
+        if (int r = ensure_h2d(c, 2 * nd)) return r;
+        (void)nd;
+        // velocities only: reuse mode 2 with previous velocities read back unchanged is not needed;
+        // the state upload overwrites v and keeps v_prev on the device
+        CUDA_OR_FAIL(cudaMemcpyAsync(c->d_h2d, vel, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+        if (use64(c)) launch_load_positions<double>(c->d, c->d_h2d, c->d_inv, 0, n, 3, c->stream);
+        else launch_load_positions<float>(c->f, c->d_h2d, c->d_inv, 0, n, 3, c->stream);
+        CUDA_OR_FAIL(cudaGetLastError());
+    }
+    return AVBD_OK;
+}
+
+static int get_vec(avbd_ctx* c, int which, unsigned first, unsigned n, double* out) {
+    if (int r = check_ctx(c)) return r;
+    if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
+    if (!c->finalized) {
+        const std::vector<double>& src = which == 0 ? c->x : c->v;
+        std::copy(src.begin() + 3ull * first, src.begin() + 3ull * (first + n), out);
+        return AVBD_OK;
+    }
+    if (int r = ensure_h2d(c, 3ull * n)) return r;
+    if (use64(c)) launch_store_vec<double>(c->d, which, c->d_h2d, c->d_inv + first, n, c->stream);
+    else launch_store_vec<float>(c->f, which, c->d_h2d, c->d_inv + first, n, c->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    CUDA_OR_FAIL(cudaMemcpyAsync(out, c->d_h2d, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return device_error(c);
+}
+
+int avbd_get_positions(avbd_ctx* c, unsigned first, unsigned n, double* out) { return get_vec(c, 0, first, n, out); }
+int avbd_get_velocities(avbd_ctx* c, unsigned first, unsigned n, double* out) { return get_vec(c, 1, first, n, out); }
+
+int avbd_get_rotations(avbd_ctx* c, unsigned first, unsigned n, double* out) {
+    if (int r = check_ctx(c)) return r;
+    if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
+    for (unsigned i = 0; i < n; i++) {
+        unsigned e = first + i;
+        if (c->rot[e] == UINT32_MAX) {
+            out[4 * i] = 1; out[4 * i + 1] = out[4 * i + 2] = out[4 * i + 3] = 0;
+        } else {
+            for (int k = 0; k < 4; k++) out[4 * i + k] = c->q[4ull * c->rot[e] + k];
+        }
+    }
+    return AVBD_OK;
+}
+
+int avbd_get_angular_velocities(avbd_ctx* c, unsigned first, unsigned n, double* w) {
+    if (int r = check_ctx(c)) return r;
+    if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
+    std::fill(w, w + 3ull * n, 0.0);
+    return AVBD_OK;
+}
+
+int avbd_get_coloring(avbd_ctx* c, unsigned* colors, unsigned* num_colors) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (colors) std::copy(c->color.begin(), c->color.end(), colors);
+    if (num_colors) *num_colors = c->num_colors;
+    return AVBD_OK;
+}
+
+int avbd_debug_block(avbd_ctx* c, unsigned p, double* G, double* H, int* dof) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (p >= c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "particle index out of range");
+    double h[12] = {0};
+    CUDA_OR_FAIL(cudaMemsetAsync(c->d_residual, 0, 4 * sizeof(double), c->stream));
+    double* out = nullptr;
+    if (int r = ensure_h2d(c, 12)) return r;
+    out = c->d_h2d;
+    CUDA_OR_FAIL(cudaMemsetAsync(out, 0, 12 * sizeof(double), c->stream));
+    StepConsts k = consts(c);
+    if (use64(c)) launch_debug_block<double>(c, c->d, k, c->inv[p], out, c->stream);
+    else launch_debug_block<float>(c, c->f, k, c->inv[p], out, c->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    CUDA_OR_FAIL(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < 3; i++) G[i] = h[i];
+    for (int i = 0; i < 9; i++) H[i] = h[3 + i];
+    if (dof) *dof = 3;
+    return AVBD_OK;
+}
+
+int avbd_residual(avbd_ctx* c, double* residual) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    StepConsts k = consts(c);
+    if (use64(c)) launch_residual<double>(c, c->d, k, c->d_residual, c->stream);
+    else launch_residual<float>(c, c->f, k, c->d_residual, c->stream);
+    double h[2];
+    CUDA_OR_FAIL(cudaMemcpyAsync(h, c->d_residual, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    *residual = h[1] > 0 ? std::sqrt(h[0]) / std::sqrt(h[1]) : std::sqrt(h[0]);
+    return AVBD_OK;
+}
+
+}  // extern "C"

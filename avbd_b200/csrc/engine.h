@@ -1,0 +1,210 @@
+// engine.h -- host-side context of the engine and the launch wrappers each
+// .cu file exports.  Everything here is internal; the public surface is
+// include/avbd.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "../../include/avbd.h"
+
+namespace avbd {
+
+// ------------------------------------------------------------ device data
+
+// One NeoHookean incidence (tet, local vertex) of a solved vertex, stored in
+// the order the color phases stream them.  The tet is restated relative to the
+// solved vertex i: F = sum_k (x_ok - x_i) (x) d_k over the three other
+// vertices o_k, where d_k are the rows of D = [Q; -1^T Q] belonging to them
+// (NeoHookeanEnergySolver::computeF, energy/elastic/NeoHookeanEnergySolver.hpp:96-109).
+// The solved vertex's own row is -(d_1 + d_2 + d_3).
+template <typename R> struct IncRec;
+template <> struct alignas(16) IncRec<float> {
+    uint32_t o[3];
+    uint32_t tet;
+    float d[9];
+    float vlam, vmu, shift;  // V*lambda, V*mu, mu/lambda + 1
+};
+template <> struct alignas(16) IncRec<double> {
+    uint32_t o[3];
+    uint32_t tet;
+    double d[9];
+    double vlam, vmu, shift;
+};
+static_assert(sizeof(IncRec<float>) == 64, "FP32 incidence record must be 64 B");
+static_assert(sizeof(IncRec<double>) == 112, "FP64 incidence record must be 112 B");
+
+enum VertexFlags : uint8_t { VF_FIXED = 1, VF_ORIENTED = 2, VF_GROUND = 4 };
+enum GroundFlags : uint8_t { GF_USE_STATIC = 1, GF_UNCLAMPED = 2 };
+
+// Device arrays of one precision.  All per-vertex arrays use the internal
+// (color-major) vertex order.
+template <typename R>
+struct DevState {
+    using V4 = typename Vec4Of<R>::T;
+    unsigned n = 0;
+    V4 *x = nullptr, *y = nullptr, *xp = nullptr, *xl = nullptr, *xll = nullptr, *v = nullptr, *vp = nullptr;
+    uint8_t* flags = nullptr;
+    IncRec<R>* inc = nullptr;
+    uint32_t* inc_begin = nullptr;
+    // per-tet data (damping path only)
+    unsigned ntets = 0;
+    uint4* tet_idx = nullptr;
+    V4* tet_q = nullptr;   // 3 rows per tet
+    V4* tet_e = nullptr;   // E_prev (00,11,22,01) (02,12,V*kd,0) per tet
+    // per-vertex ground contact (GroundCollisionEnergyInfo)
+    V4* gk = nullptr;      // k_n, k_t, k_b, k_start
+    V4* glam = nullptr;    // lam_n, lam_t, lam_b, C_n_prev
+    V4* gcp = nullptr;     // cp_x, cp_z, mu_s, mu_k
+    uint8_t* gflag = nullptr;
+    int* err = nullptr;    // device-side status (AVBD_ERR_*), 0 when healthy
+};
+
+// Scalar arguments of a step.
+struct StepConsts {
+    double dt;
+    double g;            // magnitude of gravity along -y
+    double kappa_max;    // condition threshold of the FP64 block fallback
+};
+
+// ---------------------------------------------------------- host staging
+
+struct HostNH { unsigned idx[4]; double lambda, mu, kd, Q[9], V; };
+struct HostGround { unsigned p; double k_start, mu_s, mu_k; };
+struct HostRod { unsigned idx[2]; double K[6], L, kappa[3]; };
+struct HostRGround { unsigned p; uint8_t shape; double radius, cp[3], k_start, mu_s, mu_k; };
+struct HostJoint { unsigned p; double po[3], ro[4], rp[3], rq[4]; };
+struct HostPrim { uint8_t type; unsigned idx[3]; unsigned object_id; double radius; };
+
+// ------------------------------------------------------------ LBVH state
+struct LbvhState {
+    unsigned n = 0;                 // primitives
+    uint8_t* type = nullptr;
+    uint4* pidx = nullptr;          // particle indices (internal order) of each primitive
+    double* radius = nullptr;
+    double* aabb = nullptr;         // 6 per primitive
+    uint64_t* morton = nullptr;
+    uint64_t* keys_tmp = nullptr;
+    uint32_t* sorted = nullptr;
+    uint32_t* sorted_tmp = nullptr;
+    uint32_t* hist = nullptr;       // radix histograms
+    uint32_t* left = nullptr;
+    uint32_t* right = nullptr;
+    uint32_t* parent = nullptr;
+    uint32_t* subtree = nullptr;
+    uint32_t* visited = nullptr;
+    double* nbounds = nullptr;      // 6 per node
+    double* scene_box = nullptr;    // 6 doubles (+ scratch)
+    uint32_t* root = nullptr;
+    uint2* pairs = nullptr;
+    uint2* range = nullptr;         // leaf range [lo, hi] of each internal node
+    uint32_t* pair_count = nullptr;
+    unsigned pair_capacity = 0;
+    double* xd = nullptr;           // FP64 copies of positions / velocities
+    double* vd = nullptr;
+    unsigned hist_blocks = 0;
+};
+
+}  // namespace avbd
+
+// The context behind the opaque avbd_ctx handle.
+struct avbd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    avbd_params params{1e-3, 60, 9.81, 33, 1e-3};
+    avbd_solver_params solver{1, 0.5, 0.0, 0, AVBD_PRECISION_FP32};
+    double kappa_max = 1e4;
+
+    // capacities (SimulationContext(particles, oriented, energies, prims, sdf))
+    unsigned cap_particles, cap_oriented, cap_energies, cap_prims, cap_sdf;
+
+    // host staging in the reference's FP64 layout (external order)
+    std::vector<double> x, v, vp, mass;
+    std::vector<uint8_t> fixed;
+    std::vector<unsigned> rot;          // rotation slot or UINT32_MAX
+    std::vector<double> q, inertia;     // 4 / 3 per oriented particle
+    std::vector<unsigned> scene_begin{0};
+    std::vector<avbd::HostNH> nh;
+    std::vector<avbd::HostGround> ground;
+    std::vector<avbd::HostRod> rods;
+    std::vector<avbd::HostRGround> rground;
+    std::vector<avbd::HostJoint> joints;
+    std::vector<avbd::HostPrim> prims;
+
+    // set-up products
+    bool finalized = false;
+    bool damping = false;
+    std::vector<unsigned> color;        // external order
+    unsigned num_colors = 0;
+    std::vector<unsigned> perm;         // internal -> external
+    std::vector<unsigned> inv;          // external -> internal
+    std::vector<unsigned> color_begin;  // internal offset of each color slab
+    std::vector<unsigned> color_solve;  // vertices of the slab that run the 3-DOF solve
+    unsigned max_color_solve = 0;
+
+    avbd::DevState<float> f;
+    avbd::DevState<double> d;
+    avbd::LbvhState lbvh;
+    double* d_residual = nullptr;       // FP64 reduction scratch
+    double* d_h2d = nullptr;            // FP64 staging for host uploads/downloads
+    size_t h2d_cap = 0;
+    unsigned long long* d_counters = nullptr;  // [0] fp64 fallbacks
+    uint32_t* d_perm = nullptr;         // internal -> external
+    uint32_t* d_inv = nullptr;          // external -> internal
+    int* d_error = nullptr;             // device-side status
+    unsigned long long launches_per_step = 0;
+
+    // CUDA graph of one full step (fixed-iteration mode)
+    cudaGraphExec_t graph = nullptr;
+    bool graph_dirty = true;
+    bool use_graph = true;
+    int lanes = 8;                      // threads per vertex in the tet solve
+    int block = 256;
+
+    avbd_stats stats{};
+    std::vector<void*> allocations;
+};
+
+namespace avbd {
+
+// ---- solve kernels (solve.cu)
+template <typename R>
+void launch_begin_step(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+template <typename R>
+void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+template <typename R>
+void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
+                        cudaStream_t st);
+template <typename R>
+void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st);
+template <typename R>
+void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+template <typename R>
+void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st);
+template <typename R>
+void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st);
+template <typename R>
+void launch_load_positions(DevState<R>& s, const double* src, const uint32_t* inv_map, unsigned first, unsigned n,
+                           int mode, cudaStream_t st);
+template <typename R>
+void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32_t* perm, unsigned n, cudaStream_t st);
+
+// ---- coloring (coloring.cu): exact DSATUR, one CTA per scene
+int gpu_dsatur(const std::vector<unsigned>& p_off, const std::vector<unsigned>& p_nbr,
+               const std::vector<unsigned>& scene_begin, std::vector<unsigned>& color, unsigned& num_colors,
+               cudaStream_t st, std::string& err);
+
+// ---- LBVH (lbvh.cu)
+int lbvh_allocate(avbd_ctx* c, std::string& err);
+template <typename R>
+void lbvh_stage(avbd_ctx* c, DevState<R>& s, cudaStream_t st);
+
+// counts launches for the stats
+void count_launch(avbd_ctx* c, unsigned k = 1);
+
+}  // namespace avbd

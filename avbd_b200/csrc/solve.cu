@@ -1,0 +1,566 @@
+// solve.cu -- per-step kernels of the AVBD solve for positional (3-DOF)
+// vertices: step-start energy hooks + inertial prediction, the per-color
+// vertex block solve over NeoHookean tets and ground contact, Chebyshev
+// acceleration fused with the contact dual update, the velocity update and
+// the residual reduction.
+//
+// Reference behaviour followed:
+//   VBDSolver::solve_Parallel step schedule     simulation/VBDSolver.hpp:48-103
+//   _particleInertialUpdate                      simulation/VBDSolver.hpp:208-248
+//   _solveParticle<3>                            simulation/VBDSolver.hpp:285-511
+//   _particleChebyshevAcceleration               simulation/VBDSolver.hpp:513-536
+//   _particleVelocityUpdate                      simulation/VBDSolver.hpp:538-566
+//   NeoHookeanEnergySolver::accumulate           energy/elastic/NeoHookeanEnergySolver.hpp:121-227
+//   NeoHookeanEnergySolver::updateAfterTimeStep  energy/elastic/NeoHookeanEnergySolver.hpp:70-90
+//   CollisionConstraintEnergySolver (ground)     energy/collision/CollisionConstraintEnergySolver.hpp:60-285
+//   GroundCollisionEnergySolver                  energy/collision/GroundCollisionEnergySolver.hpp:14-91
+#include "engine.h"
+
+namespace avbd {
+
+template <typename R>
+struct Consts {
+    R dt, inv_dt, inv_dt2, g, kappa_max;
+};
+
+template <typename R>
+static Consts<R> mkc(const StepConsts& k) {
+    return Consts<R>{(R)k.dt, (R)(1.0 / k.dt), (R)(1.0 / (k.dt * k.dt)), (R)k.g, (R)k.kappa_max};
+}
+
+static inline unsigned nblocks(unsigned n, unsigned per) { return (n + per - 1) / per; }
+
+// ----------------------------------------------------------- step start
+// Energy hooks of the step start for per-vertex ground contact
+// (GroundCollisionEnergySolver::updateContactPoints + CollisionConstraintEnergySolver::
+// updateAfterTimeStep) followed by the inertial prediction with adaptive
+// initialisation.  Both read the positions at the start of the step; the hook
+// runs first, as in the reference (VBDSolver.hpp:54-62).
+template <typename R>
+__global__ void __launch_bounds__(256) k_begin_step(DevState<R> s, Consts<R> c) {
+    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n) return;
+    using V4 = typename Vec4Of<R>::T;
+    uint8_t fl = s.flags[p];
+    V4 x4 = s.x[p];
+    if (fl & VF_GROUND) {
+        V4 k = s.gk[p], lam = s.glam[p], cp = s.gcp[p];
+        uint8_t gf = s.gflag[p];
+        cp.x = x4.x;
+        cp.y = x4.z;
+        if (lam.x > R(0)) lam.w = -x4.y;
+        if ((gf & GF_UNCLAMPED) && !(gf & GF_USE_STATIC)) gf |= GF_USE_STATIC;
+        lam.x *= R(AVBD_ALPHA * AVBD_GAMMA);
+        lam.y *= R(AVBD_GAMMA);
+        lam.z *= R(AVBD_GAMMA);
+        R gk;
+        gk = R(AVBD_GAMMA) * k.x; k.x = (gk < k.w) ? k.w : gk;
+        gk = R(AVBD_GAMMA) * k.y; k.y = (gk < k.w) ? k.w : gk;
+        gk = R(AVBD_GAMMA) * k.z; k.z = (gk < k.w) ? k.w : gk;
+        s.gk[p] = k;
+        s.glam[p] = lam;
+        s.gcp[p] = cp;
+        s.gflag[p] = gf;
+    }
+    if (fl & (VF_FIXED | VF_ORIENTED)) return;
+    V3<R> x = xyz(x4);
+    V3<R> v = xyz(s.v[p]), vp = xyz(s.vp[p]);
+    V3<R> a = c.inv_dt * (v - vp);
+    V3<R> aext = mk3<R>(0, -c.g, 0);
+    R an = c.g;
+    R t = 0;
+    if (an > R(1e-12)) {
+        R al = dot3(a, aext) / an;
+        if (al > an) t = 1;
+        else if (al < R(0)) t = 0;
+        else t = al / an;
+    }
+    V3<R> at = t * aext;
+    R dt2 = c.dt * c.dt;
+    V3<R> y = (x + c.dt * v) + dt2 * aext;
+    V3<R> xn = x + (c.dt * v + dt2 * at);
+    V4 y4 = s.y[p];
+    s.y[p] = make4<R>(y, y4.w);
+    V4 o = make4<R>(xn, x4.w);
+    s.x[p] = o;
+    s.xl[p] = o;
+    s.xll[p] = o;
+}
+
+// E_prev = 1/2 (F_prev^T F_prev - I) of every tet from the previous positions
+// (NeoHookeanEnergySolver::updateAfterTimeStep).  Only run when some tet has
+// strain-rate damping; without damping E_prev is never read.
+template <typename R>
+__global__ void __launch_bounds__(256) k_tet_eprev(DevState<R> s) {
+    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= s.ntets) return;
+    uint4 id = s.tet_idx[t];
+    V3<R> x0 = xyz(s.xp[id.x]), x1 = xyz(s.xp[id.y]), x2 = xyz(s.xp[id.z]), x3 = xyz(s.xp[id.w]);
+    V3<R> q0 = xyz(s.tet_q[3 * t]), q1 = xyz(s.tet_q[3 * t + 1]), q2 = xyz(s.tet_q[3 * t + 2]);
+    V3<R> a = x0 - x3, b = x1 - x3, d = x2 - x3;
+    // F = [a b d] Q: column j = a Q0j + b Q1j + d Q2j
+    V3<R> F0 = q0.x * a + q1.x * b + q2.x * d;
+    V3<R> F1 = q0.y * a + q1.y * b + q2.y * d;
+    V3<R> F2 = q0.z * a + q1.z * b + q2.z * d;
+    typename Vec4Of<R>::T e0, e1 = s.tet_e[2 * t + 1];
+    e0.x = R(0.5) * (dot3(F0, F0) - R(1));
+    e0.y = R(0.5) * (dot3(F1, F1) - R(1));
+    e0.z = R(0.5) * (dot3(F2, F2) - R(1));
+    e0.w = R(0.5) * dot3(F0, F1);
+    e1.x = R(0.5) * dot3(F0, F2);
+    e1.y = R(0.5) * dot3(F1, F2);
+    s.tet_e[2 * t] = e0;
+    s.tet_e[2 * t + 1] = e1;
+}
+
+// ------------------------------------------------------- vertex block
+template <typename R>
+AVBD_D IncRec<R> load_rec(const IncRec<R>* p);
+
+template <>
+AVBD_D IncRec<float> load_rec<float>(const IncRec<float>* p) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    float4 a = __ldcs(q), b = __ldcs(q + 1), c = __ldcs(q + 2), d = __ldcs(q + 3);
+    IncRec<float> r;
+    r.o[0] = __float_as_uint(a.x); r.o[1] = __float_as_uint(a.y); r.o[2] = __float_as_uint(a.z);
+    r.tet = __float_as_uint(a.w);
+    r.d[0] = b.x; r.d[1] = b.y; r.d[2] = b.z; r.d[3] = b.w;
+    r.d[4] = c.x; r.d[5] = c.y; r.d[6] = c.z; r.d[7] = c.w;
+    r.d[8] = d.x; r.vlam = d.y; r.vmu = d.z; r.shift = d.w;
+    return r;
+}
+template <>
+AVBD_D IncRec<double> load_rec<double>(const IncRec<double>* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const uint4 h = __ldcs(reinterpret_cast<const uint4*>(p));
+    IncRec<double> r;
+    r.o[0] = h.x; r.o[1] = h.y; r.o[2] = h.z; r.tet = h.w;
+    double2 v;
+    v = __ldcs(q + 1); r.d[0] = v.x; r.d[1] = v.y;
+    v = __ldcs(q + 2); r.d[2] = v.x; r.d[3] = v.y;
+    v = __ldcs(q + 3); r.d[4] = v.x; r.d[5] = v.y;
+    v = __ldcs(q + 4); r.d[6] = v.x; r.d[7] = v.y;
+    v = __ldcs(q + 5); r.d[8] = v.x; r.vlam = v.y;
+    v = __ldcs(q + 6); r.vmu = v.x; r.shift = v.y;
+    return r;
+}
+
+template <typename R>
+struct Block3 {
+    R g0 = 0, g1 = 0, g2 = 0;
+    R h00 = 0, h11 = 0, h22 = 0, h01 = 0, h02 = 0, h12 = 0;
+};
+
+// One NeoHookean incidence: NeoHookeanEnergySolver::accumulate with the tet
+// restated relative to the solved vertex (see IncRec).
+template <typename R, bool DAMP>
+AVBD_D void accumulate_tet(const DevState<R>& s, const IncRec<R>& r, V3<R> xi, R dt, Block3<R>& B) {
+    V3<R> e1 = xyz(ld_ro(s.x + r.o[0])) - xi;
+    V3<R> e2 = xyz(ld_ro(s.x + r.o[1])) - xi;
+    V3<R> e3 = xyz(ld_ro(s.x + r.o[2])) - xi;
+    V3<R> d1 = mk3(r.d[0], r.d[1], r.d[2]);
+    V3<R> d2 = mk3(r.d[3], r.d[4], r.d[5]);
+    V3<R> d3 = mk3(r.d[6], r.d[7], r.d[8]);
+    V3<R> dw = mk3(-(d1.x + d2.x + d3.x), -(d1.y + d2.y + d3.y), -(d1.z + d2.z + d3.z));
+    // columns of F
+    V3<R> F0 = d1.x * e1 + d2.x * e2 + d3.x * e3;
+    V3<R> F1 = d1.y * e1 + d2.y * e2 + d3.y * e3;
+    V3<R> F2 = d1.z * e1 + d2.z * e2 + d3.z * e3;
+    V3<R> c0 = cross3(F1, F2), c1 = cross3(F2, F0), c2 = cross3(F0, F1);
+    R J = dot3(F0, c0);
+    V3<R> Fc = dw.x * c0 + dw.y * c1 + dw.z * c2;   // cof(F) d
+    V3<R> Fd = dw.x * F0 + dw.y * F1 + dw.z * F2;   // F d
+    R hyd = r.vlam * (J - r.shift);
+    R dev = r.vmu;
+    R qn2 = dot3(dw, dw);
+    B.g0 += hyd * Fc.x + dev * Fd.x;
+    B.g1 += hyd * Fc.y + dev * Fd.y;
+    B.g2 += hyd * Fc.z + dev * Fd.z;
+    R dg = dev * qn2;
+    B.h00 += r.vlam * Fc.x * Fc.x + dg;
+    B.h11 += r.vlam * Fc.y * Fc.y + dg;
+    B.h22 += r.vlam * Fc.z * Fc.z + dg;
+    B.h01 += r.vlam * Fc.x * Fc.y;
+    B.h02 += r.vlam * Fc.x * Fc.z;
+    B.h12 += r.vlam * Fc.y * Fc.z;
+    if constexpr (DAMP) {
+        typename Vec4Of<R>::T e0 = s.tet_e[2 * r.tet], e1v = s.tet_e[2 * r.tet + 1];
+        R vkd = e1v.z;
+        if (vkd != R(0)) {
+            R idt = R(1) / dt;
+            // Edot = (1/2 (F^T F - I) - E_prev) / dt
+            R E00 = (R(0.5) * (dot3(F0, F0) - R(1)) - e0.x) * idt;
+            R E11 = (R(0.5) * (dot3(F1, F1) - R(1)) - e0.y) * idt;
+            R E22 = (R(0.5) * (dot3(F2, F2) - R(1)) - e0.z) * idt;
+            R E01 = (R(0.5) * dot3(F0, F1) - e0.w) * idt;
+            R E02 = (R(0.5) * dot3(F0, F2) - e1v.x) * idt;
+            R E12 = (R(0.5) * dot3(F1, F2) - e1v.y) * idt;
+            V3<R> Ed = mk3(E00 * dw.x + E01 * dw.y + E02 * dw.z, E01 * dw.x + E11 * dw.y + E12 * dw.z,
+                           E02 * dw.x + E12 * dw.y + E22 * dw.z);
+            R damp = R(2) * idt * vkd;
+            V3<R> FEd = Ed.x * F0 + Ed.y * F1 + Ed.z * F2;
+            B.g0 += damp * FEd.x;
+            B.g1 += damp * FEd.y;
+            B.g2 += damp * FEd.z;
+            R diag = damp * dot3(dw, Ed);
+            R al = R(0.5) * damp * idt;
+            // F F^T = sum_c F_c F_c^T
+            R f00 = F0.x * F0.x + F1.x * F1.x + F2.x * F2.x;
+            R f11 = F0.y * F0.y + F1.y * F1.y + F2.y * F2.y;
+            R f22 = F0.z * F0.z + F1.z * F1.z + F2.z * F2.z;
+            R f01 = F0.x * F0.y + F1.x * F1.y + F2.x * F2.y;
+            R f02 = F0.x * F0.z + F1.x * F1.z + F2.x * F2.z;
+            R f12 = F0.y * F0.z + F1.y * F1.z + F2.y * F2.z;
+            B.h00 += diag + al * (f00 * qn2 + Fd.x * Fd.x);
+            B.h11 += diag + al * (f11 * qn2 + Fd.y * Fd.y);
+            B.h22 += diag + al * (f22 * qn2 + Fd.z * Fd.z);
+            B.h01 += al * (f01 * qn2 + Fd.x * Fd.y);
+            B.h02 += al * (f02 * qn2 + Fd.x * Fd.z);
+            B.h12 += al * (f12 * qn2 + Fd.y * Fd.z);
+        }
+    }
+}
+
+// Ground contact term of the block (CollisionConstraintEnergySolver::accumulate<3>
+// with GroundCollisionConstraintSolver): the Hessian k grad C grad C^T is always
+// added, the gradient is gated by the clamped multipliers.
+template <typename R>
+AVBD_D void accumulate_ground(const DevState<R>& s, unsigned p, V3<R> xi, Block3<R>& B) {
+    typename Vec4Of<R>::T k = s.gk[p], lam = s.glam[p], cp = s.gcp[p];
+    uint8_t gf = s.gflag[p];
+    R Cn = -xi.y, Ct = xi.x - cp.x, Cb = xi.z - cp.y;
+    R cc = Cn - R(AVBD_ALPHA) * lam.w;
+    R ln = k.x * cc + lam.x;
+    R lnp = ln > R(0) ? ln : R(0);
+    R lt = k.y * Ct + lam.y, lb = k.z * Cb + lam.z;
+    R mag = sqrt(lt * lt + lb * lb);
+    R mu = (gf & GF_USE_STATIC) ? cp.z : cp.w;
+    R mx = mu * lnp;
+    if (mag > mx) {
+        R sc = mx / (mag + R(1e-8));
+        lt = lt * sc;
+        lb = lb * sc;
+    }
+    B.g0 += lt;
+    B.g1 += -lnp;
+    B.g2 += lb;
+    B.h00 += k.y;
+    B.h11 += k.x;
+    B.h22 += k.z;
+}
+
+template <typename R, int LANES>
+AVBD_D void reduce_block(Block3<R>& B) {
+#pragma unroll
+    for (int m = LANES / 2; m >= 1; m >>= 1) {
+        B.g0 += shfl_xor(B.g0, m);
+        B.g1 += shfl_xor(B.g1, m);
+        B.g2 += shfl_xor(B.g2, m);
+        B.h00 += shfl_xor(B.h00, m);
+        B.h11 += shfl_xor(B.h11, m);
+        B.h22 += shfl_xor(B.h22, m);
+        B.h01 += shfl_xor(B.h01, m);
+        B.h02 += shfl_xor(B.h02, m);
+        B.h12 += shfl_xor(B.h12, m);
+    }
+}
+
+enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2 };
+
+// Vertex block solve of one color slab: LANES threads per vertex stream the
+// vertex's incidence records, each lane accumulating its tets, then a shuffle
+// reduction and the 3x3 solve by the group's first lane.  MODE_RESIDUAL
+// evaluates |m/h^2 (x-y) + grad| instead of updating; MODE_DEBUG exports the
+// accumulated block.
+template <typename R, int LANES, bool DAMP, bool GROUND, int MODE>
+__global__ void __launch_bounds__(256) k_solve_tet(DevState<R> s, unsigned begin, unsigned count, Consts<R> c,
+                                                   unsigned long long* counters, double* out) {
+    unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned gi = tid / LANES;
+    unsigned lane = tid % LANES;
+    bool active = gi < count;
+    unsigned p = begin + (active ? gi : 0);
+    uint8_t fl = active ? s.flags[p] : 0;
+    if (MODE != MODE_SOLVE && (fl & (VF_FIXED | VF_ORIENTED))) active = false;
+    Block3<R> B;
+    V3<R> xi = mk3<R>(0, 0, 0);
+    if (active) {
+        xi = xyz(s.x[p]);
+        unsigned b = s.inc_begin[p], e = s.inc_begin[p + 1];
+        for (unsigned k = b + lane; k < e; k += LANES) {
+            IncRec<R> r = load_rec<R>(s.inc + k);
+            accumulate_tet<R, DAMP>(s, r, xi, c.dt, B);
+        }
+    }
+    reduce_block<R, LANES>(B);
+    if (!active || lane != 0) {
+        if constexpr (MODE == MODE_RESIDUAL) {
+            // keep the warp reduction below well defined
+        } else {
+            return;
+        }
+    }
+    double r2 = 0.0, mg2 = 0.0;
+    if (active && lane == 0) {
+        if (GROUND && (fl & VF_GROUND)) accumulate_ground<R>(s, p, xi, B);
+        typename Vec4Of<R>::T y4 = s.y[p];
+        R m = y4.w;
+        R cm = m * c.inv_dt2;
+        V3<R> d = xi - xyz(y4);
+        if constexpr (MODE == MODE_SOLVE) {
+            Sym3<R> A{cm + B.h00, cm + B.h11, cm + B.h22, B.h01, B.h02, B.h12};
+            V3<R> rhs = mk3(-cm * d.x - B.g0, -cm * d.y - B.g1, -cm * d.z - B.g2);
+            V3<R> dx;
+            R kappa = solve_sym3<R>(A, rhs, dx);
+            if (!(kappa <= c.kappa_max)) {
+                double M[3][3] = {{(double)A.a00, (double)A.a01, (double)A.a02},
+                                  {(double)A.a01, (double)A.a11, (double)A.a12},
+                                  {(double)A.a02, (double)A.a12, (double)A.a22}};
+                double bb[3] = {(double)rhs.x, (double)rhs.y, (double)rhs.z}, xx[3];
+                lu_solve_d<3>(M, bb, xx);
+                dx = mk3<R>((R)xx[0], (R)xx[1], (R)xx[2]);
+                atomicAdd(counters, 1ull);
+            }
+            typename Vec4Of<R>::T o = make4<R>(xi + dx, R(0));
+            s.x[p] = o;
+        } else if constexpr (MODE == MODE_RESIDUAL) {
+            double u0 = (double)cm * (double)d.x + (double)B.g0;
+            double u1 = (double)cm * (double)d.y + (double)B.g1;
+            double u2 = (double)cm * (double)d.z + (double)B.g2;
+            r2 = u0 * u0 + u1 * u1 + u2 * u2;
+            double mgv = (double)m * (double)c.g;
+            mg2 = mgv * mgv;
+        } else {
+            out[0] = B.g0; out[1] = B.g1; out[2] = B.g2;
+            out[3] = B.h00; out[4] = B.h01; out[5] = B.h02;
+            out[6] = B.h01; out[7] = B.h11; out[8] = B.h12;
+            out[9] = B.h02; out[10] = B.h12; out[11] = B.h22;
+        }
+    }
+    if constexpr (MODE == MODE_RESIDUAL) {
+        // FP64 reduction: warp, then one atomic per warp
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) {
+            r2 += __shfl_xor_sync(0xffffffffu, r2, m);
+            mg2 += __shfl_xor_sync(0xffffffffu, mg2, m);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(out, r2);
+            atomicAdd(out + 1, mg2);
+        }
+    }
+}
+
+// Chebyshev acceleration of every particle fused with the ground-contact dual
+// update that follows it (CollisionConstraintEnergySolver::updateAfterIteration);
+// a ground energy reads only its own particle, so the fusion is exact.
+template <typename R>
+__global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega) {
+    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n) return;
+    uint8_t fl = s.flags[p];
+    if (fl & VF_ORIENTED) return;
+    typename Vec4Of<R>::T x4 = s.x[p], l4 = s.xl[p], ll4 = s.xll[p];
+    V3<R> x = xyz(x4), ll = xyz(ll4);
+    V3<R> xn = omega * (x - ll) + ll;
+    typename Vec4Of<R>::T o = make4<R>(xn, x4.w);
+    s.x[p] = o;
+    s.xll[p] = l4;
+    s.xl[p] = o;
+    if (fl & VF_GROUND) {
+        typename Vec4Of<R>::T k = s.gk[p], lam = s.glam[p], cp = s.gcp[p];
+        uint8_t gf = s.gflag[p];
+        R Cn = -xn.y, Ct = xn.x - cp.x, Cb = xn.z - cp.y;
+        R cc = Cn - R(AVBD_ALPHA) * lam.w;
+        R ln = k.x * cc + lam.x;
+        R lt = k.y * Ct + lam.y;
+        R lb = k.z * Cb + lam.z;
+        if (ln > R(0)) k.x += R(AVBD_BETA) * fabs(cc);
+        lam.x = ln > R(0) ? ln : R(0);
+        R mag = sqrt(lt * lt + lb * lb);
+        bool st = gf & GF_USE_STATIC;
+        R mx = (st ? cp.z : cp.w) * lam.x;
+        if (mag < mx) {
+            k.y += R(AVBD_BETA) * fabs(Ct);
+            k.z += R(AVBD_BETA) * fabs(Cb);
+            lam.y = lt;
+            lam.z = lb;
+            gf |= GF_UNCLAMPED;
+        } else {
+            if (st) {
+                gf &= ~GF_USE_STATIC;
+                mx = cp.w * ln;
+            }
+            lam.y = lt / (mag + R(1e-8)) * mx;
+            lam.z = lb / (mag + R(1e-8)) * mx;
+            gf &= ~GF_UNCLAMPED;
+        }
+        s.gk[p] = k;
+        s.glam[p] = lam;
+        s.gflag[p] = gf;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_velocity(DevState<R> s, R inv_dt) {
+    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n) return;
+    if (s.flags[p] & VF_ORIENTED) return;
+    typename Vec4Of<R>::T x4 = s.x[p], xp4 = s.xp[p];
+    s.vp[p] = s.v[p];
+    s.v[p] = make4<R>(inv_dt * (xyz(x4) - xyz(xp4)), R(0));
+    s.xp[p] = x4;
+    if (!isfinite(x4.x + x4.y + x4.z)) atomicExch(s.err, (int)AVBD_ERR_NAN);
+}
+
+// Host FP64 (external order) -> device state.  mode 0: positions only,
+// mode 1: positions and every derived position array (ParticlePool::addParticle
+// reset), mode 2: velocities (src) and previous velocities (src + 3n),
+// mode 3: velocities only.
+template <typename R>
+__global__ void k_load(DevState<R> s, const double* src, const uint32_t* inv_map, unsigned first, unsigned n,
+                       int mode) {
+    unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned p = inv_map[first + i];
+    V3<R> v = mk3<R>((R)src[3 * i], (R)src[3 * i + 1], (R)src[3 * i + 2]);
+    if (mode == 2) {
+        V3<R> w = mk3<R>((R)src[3 * (n + i)], (R)src[3 * (n + i) + 1], (R)src[3 * (n + i) + 2]);
+        s.v[p] = make4<R>(v, R(0));
+        s.vp[p] = make4<R>(w, R(0));
+        return;
+    }
+    if (mode == 3) {
+        s.v[p] = make4<R>(v, R(0));
+        return;
+    }
+    typename Vec4Of<R>::T o = make4<R>(v, R(0));
+    s.x[p] = o;
+    if (mode == 1) {
+        typename Vec4Of<R>::T y4 = s.y[p];
+        s.y[p] = make4<R>(v, y4.w);
+        s.xp[p] = o;
+        s.xl[p] = o;
+        s.xll[p] = o;
+    }
+}
+
+// Device state -> host FP64 (external order).  which: 0 x, 1 v, 2 xp.
+template <typename R>
+__global__ void k_store(DevState<R> s, int which, double* dst, const uint32_t* inv_map, unsigned first, unsigned n) {
+    unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned p = inv_map[first + i];
+    typename Vec4Of<R>::T a = which == 0 ? s.x[p] : which == 1 ? s.v[p] : s.xp[p];
+    dst[3 * i] = (double)a.x;
+    dst[3 * i + 1] = (double)a.y;
+    dst[3 * i + 2] = (double)a.z;
+}
+
+// ---------------------------------------------------------------- host
+template <typename R>
+void launch_begin_step(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    k_begin_step<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, mkc<R>(k));
+    count_launch(c);
+}
+
+template <typename R>
+void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    (void)k;
+    if (s.ntets == 0) return;
+    k_tet_eprev<R><<<nblocks(s.ntets, 256), 256, 0, st>>>(s);
+    count_launch(c);
+}
+
+template <typename R, int LANES, int MODE>
+static void solve_dispatch(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
+                           cudaStream_t st, double* out) {
+    unsigned threads = count * LANES;
+    unsigned blocks = nblocks(threads, 256);
+    if (blocks == 0) return;
+    bool damp = c->damping, ground = !c->ground.empty();
+    auto kc = mkc<R>(k);
+    if (damp && ground)
+        k_solve_tet<R, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+    else if (damp)
+        k_solve_tet<R, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+    else if (ground)
+        k_solve_tet<R, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+    else
+        k_solve_tet<R, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+    count_launch(c);
+}
+
+template <typename R, int MODE>
+static void solve_lanes(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
+                        cudaStream_t st, double* out) {
+    switch (c->lanes) {
+        case 4: solve_dispatch<R, 4, MODE>(c, s, k, begin, count, st, out); break;
+        case 16: solve_dispatch<R, 16, MODE>(c, s, k, begin, count, st, out); break;
+        case 32: solve_dispatch<R, 32, MODE>(c, s, k, begin, count, st, out); break;
+        default: solve_dispatch<R, 8, MODE>(c, s, k, begin, count, st, out); break;
+    }
+}
+
+template <typename R>
+void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
+                        cudaStream_t st) {
+    solve_lanes<R, MODE_SOLVE>(c, s, k, begin, count, st, nullptr);
+}
+
+template <typename R>
+void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st) {
+    (void)k;
+    k_chebyshev_dual<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)omega);
+    count_launch(c);
+}
+
+template <typename R>
+void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    k_velocity<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)(1.0 / k.dt));
+    count_launch(c);
+}
+
+template <typename R>
+void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st) {
+    cudaMemsetAsync(out2, 0, 2 * sizeof(double), st);
+    solve_lanes<R, MODE_RESIDUAL>(c, s, k, 0, s.n, st, out2);
+}
+
+template <typename R>
+void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st) {
+    solve_lanes<R, MODE_DEBUG>(c, s, k, p, 1, st, out);
+}
+
+template <typename R>
+void launch_load_positions(DevState<R>& s, const double* src, const uint32_t* inv_map, unsigned first, unsigned n,
+                           int mode, cudaStream_t st) {
+    if (n == 0) return;
+    k_load<R><<<nblocks(n, 256), 256, 0, st>>>(s, src, inv_map, first, n, mode);
+}
+
+template <typename R>
+void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32_t* inv_map, unsigned n,
+                      cudaStream_t st) {
+    if (n == 0) return;
+    k_store<R><<<nblocks(n, 256), 256, 0, st>>>(s, which, dst, inv_map, 0, n);
+}
+
+#define INST(R)                                                                                                  \
+    template void launch_begin_step<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);               \
+    template void launch_tet_eprev<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                \
+    template void launch_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,         \
+                                        cudaStream_t);                                                          \
+    template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t);   \
+    template void launch_velocity<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                 \
+    template void launch_residual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double*, cudaStream_t);        \
+    template void launch_debug_block<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, double*,          \
+                                        cudaStream_t);                                                          \
+    template void launch_load_positions<R>(DevState<R>&, const double*, const uint32_t*, unsigned, unsigned, int, \
+                                           cudaStream_t);                                                       \
+    template void launch_store_vec<R>(const DevState<R>&, int, double*, const uint32_t*, unsigned, cudaStream_t);
+INST(float)
+INST(double)
+#undef INST
+
+}  // namespace avbd

@@ -1,0 +1,265 @@
+/*
+ * avbd.h -- C-ABI of the B200-native Augmented Vertex Block Descent engine.
+ *
+ * This is the drop-in boundary for the per-step solve of smtobin/avbd.  Every
+ * entry point below replaces one piece of that project's C++ step API; the
+ * replaced interface is cited as reference-path:line next to each declaration.
+ * The signatures use only plain pointers, sizes and PODs: positions, velocities
+ * and energy parameters cross the boundary in the reference's own FP64 layout
+ * (a std::vector<Vec3r> is `double[3*n]`, a Quaternion is `double[4]` in
+ * (w, x, y, z) order, a Mat3r is `double[9]` row-major).
+ *
+ * Conventions
+ *  - Every function returns an int status (AVBD_OK == 0).  No C++ exception
+ *    crosses this boundary; avbd_last_error_string() describes the last
+ *    failure on the calling thread.
+ *  - A context is used by one host thread at a time (calls on one context are
+ *    not re-entrant).  Contexts are independent: there is no process-wide
+ *    state, unlike the reference's static WorkerThreadContext::NUM_THREADS
+ *    (common/WorkerThreadContext.hpp:15).
+ *  - "Slots" are indices into the corresponding pool, exactly like the value
+ *    returned by the reference's TombstonePool::allocSlot
+ *    (common/TombstonePool.hpp:58-65).  Bulk adds return the first slot; the
+ *    n slots are consecutive.
+ */
+#ifndef AVBD_H
+#define AVBD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AVBD_API __attribute__((visibility("default")))
+#else
+#define AVBD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define AVBD_OK                   0
+#define AVBD_ERR_INVALID_ARG      1  /* bad pointer / index / size                         */
+#define AVBD_ERR_CAPACITY         2  /* pool overflow (TombstonePool.hpp:61-65)            */
+#define AVBD_ERR_COLORS           3  /* more than 256 colors (ColorList.hpp:36)            */
+#define AVBD_ERR_UNSUPPORTED_PAIR 4  /* sphere-rod / sphere-sphere (CollisionDetector.cpp:211,686) */
+#define AVBD_ERR_NAN              5  /* non-finite state detected after a step             */
+#define AVBD_ERR_BARRIER_TIMEOUT  6  /* a bounded device-side wait gave up                 */
+#define AVBD_ERR_CUDA             7  /* CUDA runtime failure                               */
+#define AVBD_ERR_STATE            8  /* call out of order (e.g. step before finalize)      */
+#define AVBD_ERR_UNSUPPORTED      9  /* configuration this engine does not implement       */
+#define AVBD_ERR_NO_DEVICE       10  /* no CUDA device visible                             */
+
+/* Shape types, values of Collision::CollisionGeometryType
+ * (collision/CollisionGeometryType.hpp:16-27). */
+#define AVBD_SHAPE_TRIANGLE     0
+#define AVBD_SHAPE_ROD_SEGMENT  1
+#define AVBD_SHAPE_SPHERE       2
+
+/* Arithmetic of the solve.  FP32 is the production path (FP32 accumulation,
+ * FP64 block inverse on ill-conditioned blocks, FP64 residual reduction);
+ * FP64 runs every kernel in double precision and is the parity/debug path. */
+#define AVBD_PRECISION_FP32 0
+#define AVBD_PRECISION_FP64 1
+
+typedef struct avbd_ctx avbd_ctx;
+
+/* Sim::SimulationParams (simulation/SimulationParams.hpp:9-16). */
+typedef struct avbd_params {
+    double dt;
+    double end_time;
+    double g_accel;
+    double viewer_refresh_time_ms;
+    double collision_margin;
+} avbd_params;
+
+/* Arguments of VBDSolver(ctx, solver_iters, iter_acceleration)
+ * (simulation/VBDSolver.hpp:37-42) plus the engine's own options.
+ * residual_tolerance == 0 keeps the reference behaviour: exactly solver_iters
+ * iterations per step.  residual_tolerance > 0 iterates until the residual
+ * R <= residual_tolerance (checked after every full sweep) or max_iters. */
+typedef struct avbd_solver_params {
+    unsigned solver_iters;
+    double   iter_acceleration;
+    double   residual_tolerance;
+    unsigned max_iters;
+    int      precision;
+} avbd_solver_params;
+
+/* Execution statistics of the last avbd_step call. */
+typedef struct avbd_stats {
+    unsigned long long kernel_launches;   /* kernels launched by the engine   */
+    unsigned long long iterations;        /* solver iterations executed       */
+    unsigned long long fp64_fallbacks;    /* blocks solved in FP64            */
+    unsigned long long candidate_pairs;   /* broad-phase pairs of last step   */
+    double   last_residual;               /* R after the last sweep (or -1)   */
+    unsigned num_colors;
+    unsigned num_scenes;
+} avbd_stats;
+
+/* ------------------------------------------------------------- lifetime */
+
+/* Sim::SimulationContext(particles, oriented, energies, prims, sdf)
+ * (simulation/SimulationContext.hpp:46-59).  Binds the context to CUDA device
+ * `device` and creates its stream. */
+AVBD_API int avbd_create(avbd_ctx** out, int device,
+                unsigned particles_capacity, unsigned oriented_capacity,
+                unsigned energies_capacity, unsigned primitives_capacity,
+                unsigned sdf_capacity);
+AVBD_API int avbd_destroy(avbd_ctx* ctx);
+
+/* Replaces the context's stream with a caller-owned one (not destroyed by the
+ * engine).  Pass NULL to go back to the engine's own stream. */
+AVBD_API int avbd_set_stream(avbd_ctx* ctx, void* cuda_stream);
+
+/* SimulationContext::params (simulation/SimulationContext.hpp:39). */
+AVBD_API int avbd_set_params(avbd_ctx* ctx, const avbd_params* params);
+/* VBDSolver(ctx, solver_iters, iter_acceleration) (simulation/VBDSolver.hpp:37-42). */
+AVBD_API int avbd_set_solver(avbd_ctx* ctx, const avbd_solver_params* solver);
+
+/* Starts a new independent scene: particles added after this call form scene
+ * k+1.  Scenes never share energies; they are colored independently and
+ * advance together in one launch per color phase.  A context that never calls
+ * this holds one scene. */
+AVBD_API int avbd_begin_scene(avbd_ctx* ctx, unsigned* scene_index);
+
+/* ------------------------------------------------------------ particles */
+
+/* ParticlePool::addParticle(position, mass) x n (common/ParticlePool.hpp:217-240). */
+AVBD_API int avbd_particles_add(avbd_ctx* ctx, unsigned n, const double* positions,
+                       const double* masses, unsigned* first_slot);
+/* ParticlePool::addOrientedParticle(position, rotation, mass, inertia) x n
+ * (common/ParticlePool.hpp:257-263).  rotations are (w,x,y,z). */
+AVBD_API int avbd_particles_add_oriented(avbd_ctx* ctx, unsigned n, const double* positions,
+                                const double* rotations, const double* masses,
+                                const double* rotational_inertias, unsigned* first_slot);
+/* ParticlePool::fixed[idx] = flag (common/ParticlePool.hpp:87). */
+AVBD_API int avbd_particles_set_fixed(avbd_ctx* ctx, unsigned n, const unsigned* slots,
+                             const uint8_t* fixed);
+
+/* State transfer for n consecutive particles starting at `first`.
+ * set_positions also resets previous/inertial/last-iterate positions like
+ * ParticlePool::addParticle; set_state only overwrites positions and
+ * velocities (the per-step drop-in upload). */
+AVBD_API int avbd_set_positions(avbd_ctx* ctx, unsigned first, unsigned n, const double* positions);
+AVBD_API int avbd_set_velocities(avbd_ctx* ctx, unsigned first, unsigned n,
+                        const double* velocities, const double* previous_velocities);
+AVBD_API int avbd_set_state(avbd_ctx* ctx, const double* positions, const double* velocities);
+AVBD_API int avbd_get_positions(avbd_ctx* ctx, unsigned first, unsigned n, double* positions);
+AVBD_API int avbd_get_velocities(avbd_ctx* ctx, unsigned first, unsigned n, double* velocities);
+AVBD_API int avbd_get_rotations(avbd_ctx* ctx, unsigned first, unsigned n, double* rotations);
+AVBD_API int avbd_get_angular_velocities(avbd_ctx* ctx, unsigned first, unsigned n, double* w);
+AVBD_API int avbd_num_particles(avbd_ctx* ctx, unsigned* n);
+
+/* -------------------------------------------------------------- energies */
+
+/* NeoHookeanEnergyPool::addEnergy(indices, lambda, mu, kd, Q, rest_volume) x n
+ * (energy/elastic/NeoHookeanEnergyPool.hpp:40-67).  Q is row-major 3x3. */
+AVBD_API int avbd_neo_hookean_add(avbd_ctx* ctx, unsigned n, const unsigned* indices4,
+                         const double* lambda, const double* mu, const double* kd,
+                         const double* Q9, const double* rest_volume, unsigned* first_slot);
+
+/* CosseratRodEnergyPool::addEnergy(indices, stiffness, rest_length, precurvature) x n
+ * (energy/elastic/CosseratRodEnergyPool.hpp:36-51). */
+AVBD_API int avbd_cosserat_rod_add(avbd_ctx* ctx, unsigned n, const unsigned* indices2,
+                          const double* stiffness6, const double* rest_length,
+                          const double* precurvature3, unsigned* first_slot);
+
+/* GroundCollisionEnergyPool::addEnergy(particle_index, k_start, mu_s, mu_k) x n
+ * (energy/collision/GroundCollisionEnergyPool.hpp:32-43). */
+AVBD_API int avbd_ground_collision_add(avbd_ctx* ctx, unsigned n, const unsigned* particle_index,
+                              const double* k_start, const double* mu_s, const double* mu_k,
+                              unsigned* first_slot);
+
+/* RigidBodyGroundCollisionEnergyPool::addEnergy(particle_index, shape_params,
+ * cp_rb_local, k_start, mu_s, mu_k) x n
+ * (energy/collision/RigidBodyGroundCollisionEnergyPool.hpp:36-58).
+ * shape_type is AVBD_SHAPE_SPHERE or AVBD_SHAPE_ROD_SEGMENT; shape_radius is
+ * CollisionShapeParams::sphere.radius / rod.radius. */
+AVBD_API int avbd_rigid_body_ground_collision_add(avbd_ctx* ctx, unsigned n,
+                                         const unsigned* particle_index,
+                                         const uint8_t* shape_type, const double* shape_radius,
+                                         const double* cp_rb_local3, const double* k_start,
+                                         const double* mu_s, const double* mu_k,
+                                         unsigned* first_slot);
+
+/* OneSidedFixedJointEnergyPool::addEnergy(particle_index, pos_offset, rot_offset,
+ * ref_position, ref_rotation) x n (energy/joint/OneSidedFixedJointEnergyPool.hpp:36-55).
+ * k_start = 1e4 on all six rows (OneSidedFixedJointEnergyPool.hpp:27). */
+AVBD_API int avbd_one_sided_fixed_joint_add(avbd_ctx* ctx, unsigned n, const unsigned* particle_index,
+                                   const double* position_offset3, const double* rotation_offset4,
+                                   const double* ref_position3, const double* ref_rotation4,
+                                   unsigned* first_slot);
+
+/* --------------------------------------------------- collision primitives */
+
+/* CollisionPrimitivePool::addObject(TetMeshObject) surface triangles
+ * (collision/CollisionPrimitivePool.cpp:36-50): one Triangle per face. */
+AVBD_API int avbd_collision_add_triangles(avbd_ctx* ctx, unsigned n, const unsigned* indices3,
+                                 unsigned object_id, unsigned* first_slot);
+/* CollisionPrimitivePool::addObject(Rod): one RodSegment per element. */
+AVBD_API int avbd_collision_add_rod_segments(avbd_ctx* ctx, unsigned n, const unsigned* indices2,
+                                    double radius, unsigned object_id, unsigned* first_slot);
+/* CollisionPrimitivePool::addObject(RigidSphere). */
+AVBD_API int avbd_collision_add_spheres(avbd_ctx* ctx, unsigned n, const unsigned* particle_index,
+                               const double* radius, const unsigned* object_id,
+                               unsigned* first_slot);
+
+/* ------------------------------------------------------------ set-up/step */
+
+/* StaticParticleAdjacency::buildAdjacency + DynamicParticleAdjacency::buildAdjacency
+ * + ColorList::buildInitialColorList (simulation/Simulation.cpp:86-89):
+ * builds the per-vertex energy CSR, exact DSATUR coloring on the GPU (one CTA
+ * per scene) and an empty conflict CSR, and uploads everything to HBM. */
+AVBD_API int avbd_finalize(avbd_ctx* ctx);
+
+/* SimulationExecutor::timeStep() (simulation/SimulationExecutor.hpp:107-115):
+ * collision stage (LBVH build + self traversal) then VBDSolver::solve_Parallel
+ * (simulation/VBDSolver.hpp:48-103), n_steps times, stream-ordered. */
+AVBD_API int avbd_step(avbd_ctx* ctx, unsigned n_steps);
+/* Waits for the context's stream. */
+AVBD_API int avbd_synchronize(avbd_ctx* ctx);
+
+/* Runs only the collision stage (LBVH build + candidate pairs) on the current
+ * state, without advancing time. */
+AVBD_API int avbd_collision_stage(avbd_ctx* ctx);
+
+AVBD_API int avbd_get_stats(avbd_ctx* ctx, avbd_stats* stats);
+
+/* -------------------------------------------------------- parity queries */
+
+/* ColorList::color / num_colors (common/ColorList.hpp:66-67). */
+AVBD_API int avbd_get_coloring(avbd_ctx* ctx, unsigned* colors, unsigned* num_colors);
+
+/* LBVH of the last collision stage: CollisionPrimitivePool::morton_code and
+ * sorted_order (collision/CollisionPrimitivePool.hpp:57-60) and the SoA nodes
+ * of Collision::LBVH (collision/LBVH.hpp:17-85).  Arrays sized n (primitives)
+ * and 2n-1 (nodes); bounds6 is min_x,min_y,min_z,max_x,max_y,max_z per node.
+ * Any output pointer may be NULL. */
+AVBD_API int avbd_get_lbvh(avbd_ctx* ctx, unsigned* num_primitives, uint64_t* morton,
+                  unsigned* sorted_order, unsigned* left, unsigned* right,
+                  unsigned* parent, unsigned* subtree_size, double* bounds6,
+                  unsigned* root);
+/* Candidate leaf pairs (a<b, sorted-leaf indices) of LBVHTraversal
+ * (collision/LBVHTraversal.hpp:30-88), sorted lexicographically. */
+AVBD_API int avbd_get_candidate_pairs(avbd_ctx* ctx, unsigned capacity, unsigned* pairs2,
+                             unsigned* count);
+
+/* Block gradient and Hessian of particle p at the current state: the
+ * grad/hess accumulated by VBDSolver::_solveParticle<DOF>
+ * (simulation/VBDSolver.hpp:293-447).  G is 3 or 6 doubles, H is 9 or 36
+ * (row-major); *dof receives 3 or 6. */
+AVBD_API int avbd_debug_block(avbd_ctx* ctx, unsigned p, double* G, double* H, int* dof);
+
+/* Residual R of the current iterate (sqrt(sum_v |m/h^2 (x-y) + g_v|^2) /
+ * sqrt(sum_v |m g|^2)), FP64 reduction on the device. */
+AVBD_API int avbd_residual(avbd_ctx* ctx, double* residual);
+
+AVBD_API const char* avbd_last_error_string(void);
+AVBD_API const char* avbd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AVBD_H */

@@ -1,0 +1,1619 @@
+// avbd_oracle.cpp -- FP64 CPU restatement of smtobin/avbd's per-step solve.
+//
+// TEST INFRASTRUCTURE.  This file is the checker, never the product: only the
+// tests, the smoke check and bench.py's CPU-baseline leg load it.  The engine
+// under avbd_b200/ never links, calls or falls back to it.
+//
+// What it restates (each function cites the reference file:line it follows):
+//   * VBDSolver::solve_Parallel step schedule, inertial / Chebyshev / velocity
+//     updates and the per-vertex 3x3 / 6x6 block solve
+//     (simulation/VBDSolver.hpp:48-566);
+//   * NeoHookean, Cosserat rod, ground, rigid-body-ground and one-sided fixed
+//     joint energies with their AVBD dual updates (energy/**);
+//   * static adjacency, DSATUR coloring and the work list
+//     (common/StaticParticleAdjacency.hpp:42-133, common/ColorList.hpp:149-363);
+//   * swept AABBs, 63-bit Morton codes, stable LSD radix sort, Karras tree,
+//     refit and self traversal (collision/*).
+//
+// Parity status.  The reference cannot be compiled here (it needs Eigen3,
+// which is not installed), so no reference output exists to pin this file
+// against.  Parity is therefore UNPINNED against the reference binary; it is
+// pinned against what the reference's own tests hold: the finite-difference
+// checks of test/test_neohookean_accumulate.cpp, test_cosserat_accumulate.cpp
+// and test_one_sided_fixed_joint_accumulate.cpp (same inputs, same FD scheme,
+// test/finite_difference.hpp), and the Karras-2012 radix-tree example of
+// test/test_lbvh.cpp:38-47 (topology derived by hand from the published
+// figure).  Build flags disable FMA contraction (-ffp-contract=off) so that the
+// FP64 Morton codes are reproducible operation by operation.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <queue>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <array>
+#include <chrono>
+#include <atomic>
+#include <functional>
+#include <thread>
+
+namespace orc {
+
+// ----------------------------------------------------------------- math
+struct V3 {
+    double x = 0, y = 0, z = 0;
+    V3() {}
+    V3(double a, double b, double c) : x(a), y(b), z(c) {}
+    double& operator[](int i) { return (&x)[i]; }
+    double operator[](int i) const { return (&x)[i]; }
+};
+static inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+static inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+static inline V3 operator/(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline V3& operator+=(V3& a, V3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+static inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+static inline double sqnorm(V3 a) { return dot(a, a); }
+static inline double norm(V3 a) { return std::sqrt(sqnorm(a)); }
+
+struct M3 {
+    double a[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    static M3 zero() { return M3(); }
+    static M3 eye() { M3 m; m.a[0][0] = m.a[1][1] = m.a[2][2] = 1; return m; }
+    V3 row(int r) const { return {a[r][0], a[r][1], a[r][2]}; }
+    V3 col(int c) const { return {a[0][c], a[1][c], a[2][c]}; }
+    M3 T() const { M3 m; for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) m.a[i][j] = a[j][i]; return m; }
+};
+static inline M3 operator*(const M3& A, const M3& B) {
+    M3 C;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double s = 0;
+            for (int k = 0; k < 3; k++) s += A.a[i][k] * B.a[k][j];
+            C.a[i][j] = s;
+        }
+    return C;
+}
+static inline V3 operator*(const M3& A, V3 v) {
+    return {A.a[0][0] * v.x + A.a[0][1] * v.y + A.a[0][2] * v.z,
+            A.a[1][0] * v.x + A.a[1][1] * v.y + A.a[1][2] * v.z,
+            A.a[2][0] * v.x + A.a[2][1] * v.y + A.a[2][2] * v.z};
+}
+static inline M3 operator*(double s, const M3& A) {
+    M3 C; for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) C.a[i][j] = s * A.a[i][j]; return C;
+}
+static inline M3 operator+(const M3& A, const M3& B) {
+    M3 C; for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) C.a[i][j] = A.a[i][j] + B.a[i][j]; return C;
+}
+static inline M3 operator-(const M3& A, const M3& B) {
+    M3 C; for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) C.a[i][j] = A.a[i][j] - B.a[i][j]; return C;
+}
+static inline M3 outer(V3 u, V3 v) {
+    M3 C; for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) C.a[i][j] = u[i] * v[j]; return C;
+}
+static inline double det(const M3& F) { return dot(F.col(0), cross(F.col(1), F.col(2))); }
+
+// Math::Skew3 (common/Math.hpp:13-20)
+static inline M3 skew(V3 v) {
+    M3 m;
+    m.a[0][1] = -v.z; m.a[0][2] = v.y;
+    m.a[1][0] = v.z;  m.a[1][2] = -v.x;
+    m.a[2][0] = -v.y; m.a[2][1] = v.x;
+    return m;
+}
+
+struct Q4 { double w = 1, x = 0, y = 0, z = 0; };
+static inline Q4 qmul(Q4 a, Q4 b) {   // Hamilton product
+    Q4 r;
+    r.w = a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z;
+    r.x = a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y;
+    r.y = a.w * b.y + a.y * b.w + a.z * b.x - a.x * b.z;
+    r.z = a.w * b.z + a.z * b.w + a.x * b.y - a.y * b.x;
+    return r;
+}
+static inline Q4 qconj(Q4 q) { return {q.w, -q.x, -q.y, -q.z}; }
+static inline V3 qvec(Q4 q) { return {q.x, q.y, q.z}; }
+// rotation of a vector by a unit quaternion: v + 2w (u x v) + u x (2 u x v)
+static inline V3 qrot(Q4 q, V3 v) {
+    V3 u = qvec(q);
+    V3 uv = cross(u, v);
+    uv = uv + uv;
+    return v + q.w * uv + cross(u, uv);
+}
+static inline M3 qmat(Q4 q) {   // rotation matrix of a unit quaternion
+    double tx = 2 * q.x, ty = 2 * q.y, tz = 2 * q.z;
+    double twx = tx * q.w, twy = ty * q.w, twz = tz * q.w;
+    double txx = tx * q.x, txy = ty * q.x, txz = tz * q.x;
+    double tyy = ty * q.y, tyz = tz * q.y, tzz = tz * q.z;
+    M3 R;
+    R.a[0][0] = 1 - (tyy + tzz); R.a[0][1] = txy - twz;       R.a[0][2] = txz + twy;
+    R.a[1][0] = txy + twz;       R.a[1][1] = 1 - (txx + tzz); R.a[1][2] = tyz - twx;
+    R.a[2][0] = txz - twy;       R.a[2][1] = tyz + twx;       R.a[2][2] = 1 - (txx + tyy);
+    return R;
+}
+static inline Q4 qnormalize(Q4 q) {
+    double n = std::sqrt(q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z);
+    return {q.w / n, q.x / n, q.y / n, q.z / n};
+}
+
+// Math::Exp_s3 (common/Math.hpp:197-222)
+static inline Q4 exp_s3(V3 v) {
+    double th = norm(v);
+    if (th < 1e-6) {
+        Q4 q{1.0, 0.5 * v.x, 0.5 * v.y, 0.5 * v.z};
+        return qnormalize(q);
+    }
+    double h = 0.5 * th, s = std::sin(h) / th;
+    return {std::cos(h), s * v.x, s * v.y, s * v.z};
+}
+// Math::Log_S3 (common/Math.hpp:224-236)
+static inline V3 log_s3(Q4 q) {
+    V3 v = qvec(q);
+    double m = norm(v);
+    if (m < 1e-6) return 2.0 * v;
+    double th = 2 * std::atan2(m, q.w);
+    return (th / m) * v;
+}
+// Math::Minus_S3 / Plus_S3 (common/Math.hpp:238-246)
+static inline V3 minus_s3(Q4 q1, Q4 q2) { return log_s3(qmul(qconj(q2), q1)); }
+static inline Q4 plus_s3(Q4 q, V3 r) { return qmul(q, exp_s3(r)); }
+
+// Math::ExpMap_RightJacobian (common/Math.hpp:28-38)
+static inline M3 right_jac(V3 th) {
+    double n = norm(th);
+    M3 S = skew(th);
+    if (n < 1e-8) return M3::eye() - 0.5 * S;
+    return M3::eye() - ((1 - std::cos(n)) / (n * n)) * S + ((n - std::sin(n)) / (n * n * n)) * (S * S);
+}
+// Math::ExpMap_InvRightJacobian (common/Math.hpp:136-147)
+static inline M3 inv_right_jac(V3 th) {
+    double n = norm(th);
+    M3 S = skew(th);
+    if (n < 1e-8) return M3::eye() + 0.5 * S;
+    return M3::eye() + 0.5 * S + (1 / (n * n) - (1 + std::cos(n)) / (2 * n * std::sin(n))) * (S * S);
+}
+// Math::Exp_so3 (common/Math.hpp:149-158)
+static inline M3 exp_so3(V3 v) {
+    M3 S = skew(v);
+    double m = norm(v);
+    if (m < 1e-8) return M3::eye() + S;
+    return M3::eye() + (std::sin(m) / m) * S + ((1 - std::cos(m)) / (m * m)) * (S * S);
+}
+
+// Dense LU with partial (row) pivoting, the factorisation behind
+// Mat3r/Mat6r::partialPivLu().solve (simulation/VBDSolver.hpp:472,498).
+template <int N>
+static void lu_solve(double A[N][N], const double* b_in, double* x) {
+    double b[N];
+    for (int i = 0; i < N; i++) b[i] = b_in[i];
+    for (int k = 0; k < N; k++) {
+        int p = k;
+        double best = std::fabs(A[k][k]);
+        for (int i = k + 1; i < N; i++)
+            if (std::fabs(A[i][k]) > best) { best = std::fabs(A[i][k]); p = i; }
+        if (p != k) {
+            for (int j = 0; j < N; j++) std::swap(A[k][j], A[p][j]);
+            std::swap(b[k], b[p]);
+        }
+        for (int i = k + 1; i < N; i++) {
+            double l = A[i][k] / A[k][k];
+            A[i][k] = l;
+            for (int j = k + 1; j < N; j++) A[i][j] -= l * A[k][j];
+            b[i] -= l * b[k];
+        }
+    }
+    for (int i = N - 1; i >= 0; i--) {
+        double s = b[i];
+        for (int j = i + 1; j < N; j++) s -= A[i][j] * x[j];
+        x[i] = s / A[i][i];
+    }
+}
+
+// AVBD constants (common/common.hpp:13-15)
+static constexpr double BETA = 10;
+static constexpr double GAMMA = 0.99;
+static constexpr double ALPHA = 0.95;
+
+// Worker pool: the caller is worker 0, the other workers spin on a generation
+// counter and split every range statically, the execution model of
+// SimulationExecutor (simulation/SimulationExecutor.hpp:107-139) and
+// WorkerThreadContext::computeStartEnd (common/WorkerThreadContext.hpp:48-53).
+struct Pool {
+    int nt = 1;
+    std::vector<std::thread> th;
+    std::atomic<unsigned> gen{0};
+    std::atomic<int> done{0};
+    std::atomic<bool> stop{false};
+    const std::function<void(int)>* job = nullptr;
+
+    void start(int n) {
+        shutdown();
+        nt = n < 1 ? 1 : n;
+        stop = false;
+        for (int t = 1; t < nt; t++) th.emplace_back([this, t] { worker(t); });
+    }
+    void worker(int t) {
+        unsigned seen = gen.load();
+        for (;;) {
+            unsigned g;
+            int spins = 0;
+            while ((g = gen.load(std::memory_order_acquire)) == seen) {
+                if (++spins > 4096) { std::this_thread::yield(); spins = 0; }
+            }
+            seen = g;
+            if (stop.load()) return;
+            (*job)(t);
+            done.fetch_add(1, std::memory_order_acq_rel);
+        }
+    }
+    void run(const std::function<void(int)>& f) {
+        if (nt == 1) { f(0); return; }
+        job = &f;
+        done.store(0);
+        gen.fetch_add(1, std::memory_order_release);
+        f(0);
+        while (done.load(std::memory_order_acquire) != nt - 1) {}
+    }
+    template <typename F>
+    void parallel_for(long lo, long hi, F&& fn) {
+        long n = hi - lo;
+        if (n <= 0) return;
+        if (nt == 1 || n < 64) { for (long i = lo; i < hi; i++) fn(i); return; }
+        std::function<void(int)> f = [&](int t) {
+            long b = lo + n * t / nt, e = lo + n * (t + 1) / nt;
+            for (long i = b; i < e; i++) fn(i);
+        };
+        run(f);
+    }
+    void shutdown() {
+        if (th.empty()) return;
+        stop = true;
+        gen.fetch_add(1, std::memory_order_release);
+        for (auto& t : th) t.join();
+        th.clear();
+    }
+    ~Pool() { shutdown(); }
+};
+
+// ------------------------------------------------------------ the state
+enum StaticType : uint8_t { NEO_HOOKEAN = 0, COSSERAT_ROD = 1, GROUND = 2, RIGID_GROUND = 3, JOINT = 4, NTYPES = 5 };
+
+// CollisionConstraintEnergyInfo (energy/collision/CollisionConstraintEnergyPool.hpp:9-30)
+struct Contact {
+    double k_start = 0, k_n = 0, k_t = 0, k_b = 0;
+    double lam_n = 0, lam_t = 0, lam_b = 0, cn_prev = 0;
+    V3 n, t, b;
+    bool use_static = false, unclamped = false;
+    double mu_s = 0, mu_k = 0;
+};
+struct Ground : Contact { unsigned p = 0; double cp_x = 0, cp_z = 0; };
+struct RGround : Contact { unsigned p = 0; V3 cp_local, cp_ground; int shape = 2; double radius = 0; };
+struct NH { unsigned idx[4]; double lambda, mu, kd; M3 Q; double V; M3 Eprev; };
+struct Rod { unsigned idx[2]; double K[6]; double L; V3 kappa0; };
+struct Joint {
+    unsigned p = 0;
+    double k[6], lam[6], cprev[6];
+    V3 pos_off; Q4 rot_off; V3 ref_p; Q4 ref_q;
+};
+struct Prim { uint8_t type; unsigned idx[3]; uint8_t np; unsigned object_id; double radius; };
+struct Entry { uint8_t type; unsigned idx; uint16_t local; };
+
+struct Ctx {
+    // SimulationParams / VBDSolver arguments
+    double dt = 1e-3, g = 9.81, margin = 1e-3;
+    unsigned iters = 1; double rho = 0.5;
+    double tol = 0; unsigned max_iters = 0;
+    int nthreads = 1;
+    Pool pool;
+    std::string err;
+
+    // ParticlePool (common/ParticlePool.hpp:76-111)
+    std::vector<V3> x, xb, y, xp, xl, xll, v, vp;
+    std::vector<double> m;
+    std::vector<uint8_t> fixed;
+    std::vector<unsigned> rot;              // rotation_idx, UINT_MAX if positional
+    // RotationPool (common/ParticlePool.hpp:7-68)
+    std::vector<Q4> q, qb, qy, qp, ql, qll;
+    std::vector<V3> w, wp, I;
+    std::vector<unsigned> scene_of;         // scene index of each particle
+    unsigned num_scenes = 1;
+
+    // energy pools
+    std::vector<NH> nh;
+    std::vector<Rod> rods;
+    std::vector<Ground> ground;
+    std::vector<RGround> rground;
+    std::vector<Joint> joints;
+    double joint_k_start = 1e4;
+
+    // static adjacency (common/StaticParticleAdjacency.hpp:17-34)
+    std::vector<unsigned> e_off;            // (np+1)*NTYPES, end of p = e_off[(p+1)*NTYPES]
+    std::vector<Entry> entries;
+    std::vector<unsigned> p_off, p_nbr;
+    // ColorList (common/ColorList.hpp:62-78)
+    std::vector<unsigned> color;
+    unsigned num_colors = 0;
+    std::vector<unsigned> color_offsets, work_list;
+
+    // collision
+    std::vector<Prim> prims;
+    std::vector<double> aabb;               // 6 per primitive
+    std::vector<uint64_t> morton;
+    std::vector<unsigned> sorted;
+    std::vector<unsigned> left, right, parent, subtree, leaf_count;
+    std::vector<double> nbounds;            // 6 per node
+    unsigned root = 0;
+    std::vector<std::pair<unsigned, unsigned>> pairs;
+
+    // statistics
+    double last_residual = -1;
+    unsigned long long iterations = 0;
+    bool finalized = false;
+
+    unsigned np() const { return (unsigned)x.size(); }
+    bool oriented(unsigned p) const { return rot[p] != UINT32_MAX; }
+};
+
+// -------------------------------------------------------------- energies
+// NeoHookeanEnergySolver::computeF (energy/elastic/NeoHookeanEnergySolver.hpp:96-109)
+static inline M3 computeF(V3 v1, V3 v2, V3 v3, V3 v4, const M3& Q) {
+    M3 X;
+    V3 c0 = v1 - v4, c1 = v2 - v4, c2 = v3 - v4;
+    for (int i = 0; i < 3; i++) { X.a[i][0] = c0[i]; X.a[i][1] = c1[i]; X.a[i][2] = c2[i]; }
+    return X * Q;
+}
+
+// NeoHookeanEnergySolver::energy (energy/elastic/NeoHookeanEnergySolver.hpp:20-53)
+static double nh_energy(const Ctx& c, const NH& e, double dt) {
+    M3 F = computeF(c.x[e.idx[0]], c.x[e.idx[1]], c.x[e.idx[2]], c.x[e.idx[3]], e.Q);
+    M3 FtF = F.T() * F;
+    M3 E = 0.5 * (FtF - M3::eye());
+    M3 Ed = (1 / dt) * (E - e.Eprev);
+    double sq = 0;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) sq += Ed.a[i][j] * Ed.a[i][j];
+    double damp = e.V * e.kd * sq;
+    double f = det(F) - e.mu / e.lambda - 1;
+    double hyd = 0.5 * e.lambda * e.V * f * f;
+    double dev = 0.5 * e.mu * e.V * (FtF.a[0][0] + FtF.a[1][1] + FtF.a[2][2] - 3);
+    return hyd + dev + damp;
+}
+
+// NeoHookeanEnergySolver::updateAfterTimeStep (energy/elastic/NeoHookeanEnergySolver.hpp:70-90)
+static void nh_after_step(Ctx& c, NH& e) {
+    M3 F = computeF(c.xp[e.idx[0]], c.xp[e.idx[1]], c.xp[e.idx[2]], c.xp[e.idx[3]], e.Q);
+    e.Eprev = 0.5 * (F.T() * F - M3::eye());
+}
+
+// NeoHookeanEnergySolver::accumulate (energy/elastic/NeoHookeanEnergySolver.hpp:121-227)
+static void nh_accumulate(const Ctx& c, const NH& e, unsigned local, double H[3][3], double G[3], double dt) {
+    M3 F = computeF(c.x[e.idx[0]], c.x[e.idx[1]], c.x[e.idx[2]], c.x[e.idx[3]], e.Q);
+    V3 c0 = cross(F.col(1), F.col(2));
+    V3 c1 = cross(F.col(2), F.col(0));
+    V3 c2 = cross(F.col(0), F.col(1));
+    double detF = dot(F.col(0), c0);
+    V3 qi; double sign;
+    if (local < 3) { qi = e.Q.row(local); sign = 1.0; }
+    else { qi = e.Q.row(0) + e.Q.row(1) + e.Q.row(2); sign = -1.0; }
+    V3 Fqi = F * qi;
+    V3 Fc = qi.x * c0 + qi.y * c1 + qi.z * c2;
+    double hyd = e.V * e.lambda * (detF - e.mu / e.lambda - 1);
+    double dev = e.V * e.mu;
+    M3 FtF = F.T() * F;
+    double qn2 = sqnorm(qi);
+    double damp = 2 / dt * e.V * e.kd;
+    V3 g = (sign * hyd) * Fc + (sign * dev) * Fqi;
+    M3 Ed = 0.5 * FtF;
+    for (int i = 0; i < 3; i++) Ed.a[i][i] -= 0.5;
+    Ed = (1 / dt) * (Ed - e.Eprev);
+    g += (sign * damp) * (F * (Ed * qi));
+    for (int i = 0; i < 3; i++) G[i] += g[i];
+    double qEq = dot(qi, Ed * qi);
+    M3 FFt = F * F.T();
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            double h = e.V * e.lambda * Fc[i] * Fc[j];
+            if (i == j) h += e.V * e.mu * qn2 + damp * qEq;
+            h += (0.5 * damp / dt) * (FFt.a[i][j] * qn2 + Fqi[i] * Fqi[j]);
+            H[i][j] += h;
+        }
+}
+
+// CosseratRodEnergySolver strain and Jacobians
+// (energy/elastic/CosseratRodEnergySolver.hpp:20-159)
+static void rod_strain(const Ctx& c, const Rod& e, double strain[6], Q4* qmid_out = nullptr, V3* qdiff_out = nullptr) {
+    Q4 q1 = c.q[c.rot[e.idx[0]]], q2 = c.q[c.rot[e.idx[1]]];
+    V3 p1 = c.x[e.idx[0]], p2 = c.x[e.idx[1]];
+    V3 qd = minus_s3(q2, q1);
+    Q4 qm = plus_s3(q1, 0.5 * qd);
+    double il = 1.0 / e.L;
+    V3 sh = il * qrot(qconj(qm), p2 - p1) - V3(0, 0, 1);
+    V3 be = il * qd - e.kappa0;
+    for (int i = 0; i < 3; i++) { strain[i] = sh[i]; strain[3 + i] = be[i]; }
+    if (qmid_out) *qmid_out = qm;
+    if (qdiff_out) *qdiff_out = qd;
+}
+
+static double rod_energy(const Ctx& c, const Rod& e) {
+    double s[6];
+    rod_strain(c, e, s);
+    double E = 0;
+    for (int i = 0; i < 6; i++) E += s[i] * e.K[i] * s[i];
+    return 0.5 * e.L * E;
+}
+
+static void rod_accumulate(const Ctx& c, const Rod& e, unsigned local, double H[6][6], double G[6]) {
+    double s[6]; Q4 qm; V3 qd;
+    rod_strain(c, e, s, &qm, &qd);
+    V3 p1 = c.x[e.idx[0]], p2 = c.x[e.idx[1]];
+    double il = 1.0 / e.L;
+    M3 gi = inv_right_jac(qd);
+    V3 th = 0.5 * qd;
+    M3 eth = exp_so3(th);
+    M3 gth = right_jac(th);
+    M3 R = qmat(qm);
+    V3 dpds = il * (p2 - p1);
+    M3 S = skew(R.T() * dpds);
+    double SG[6][6] = {};
+    M3 A, B, C;
+    if (local == 0) {
+        M3 dth = (-0.5) * gi.T();
+        M3 dthds = (-il) * gi.T();
+        A = (-il) * R.T();
+        B = S * (eth.T() + gth * dth);
+        C = dthds;
+    } else {
+        M3 dth = 0.5 * gi;
+        M3 dthds = il * gi;
+        A = il * R.T();
+        B = S * gth * dth;
+        C = dthds;
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) { SG[i][j] = A.a[i][j]; SG[i][3 + j] = B.a[i][j]; SG[3 + i][3 + j] = C.a[i][j]; }
+    for (int j = 0; j < 6; j++) {
+        double g = 0;
+        for (int i = 0; i < 6; i++) g += s[i] * e.K[i] * SG[i][j];
+        G[j] += e.L * g;
+    }
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) {
+            double h = 0;
+            for (int i = 0; i < 6; i++) h += SG[i][a] * e.K[i] * SG[i][b];
+            H[a][b] += e.L * h;
+        }
+}
+
+// GroundCollisionConstraintSolver::evaluateConstraint (energy/collision/GroundCollisionEnergySolver.hpp:14-25)
+static void ground_eval(const Ctx& c, const Ground& e, double& Cn, double& Ct, double& Cb) {
+    V3 p = c.x[e.p];
+    Cn = -p.y; Ct = p.x - e.cp_x; Cb = p.z - e.cp_z;
+}
+
+// RigidBodyGroundCollisionConstraintSolver::evaluateConstraint
+// (energy/collision/RigidBodyGroundCollisionEnergySolver.hpp:14-54)
+static void rground_eval(const Ctx& c, const RGround& e, double& Cn, double& Ct, double& Cb) {
+    V3 p = c.x[e.p];
+    Q4 q = c.q[c.rot[e.p]];
+    V3 cp_rb = p + qrot(q, e.cp_local);
+    V3 diff = e.cp_ground - cp_rb;
+    Ct = dot(e.t, diff); Cb = dot(e.b, diff);
+    if (e.shape == 2 || e.shape == 1) {
+        V3 cpg = p - V3(0, e.radius, 0);
+        Cn = dot(e.n, e.cp_ground - cpg);
+    } else {
+        Cn = dot(e.n, diff);
+    }
+}
+
+// CollisionConstraintEnergySolver::updateAfterIteration
+// (energy/collision/CollisionConstraintEnergySolver.hpp:60-134)
+static void contact_after_iter(Contact& e, double Cn, double Ct, double Cb) {
+    double cc = Cn - ALPHA * e.cn_prev;
+    double ln = e.k_n * cc + e.lam_n;
+    double lt = e.k_t * Ct + e.lam_t;
+    double lb = e.k_b * Cb + e.lam_b;
+    if (ln > 0) e.k_n += BETA * std::fabs(cc);
+    e.lam_n = std::max(0.0, ln);
+    double mag = std::sqrt(lt * lt + lb * lb);
+    double mu = e.use_static ? e.mu_s : e.mu_k;
+    double mx = mu * e.lam_n;
+    if (mag < mx) {
+        e.k_t += BETA * std::fabs(Ct);
+        e.k_b += BETA * std::fabs(Cb);
+        e.lam_t = lt; e.lam_b = lb;
+        e.unclamped = true;
+    } else {
+        if (e.use_static) { e.use_static = false; mx = e.mu_k * ln; }
+        e.lam_t = lt / (mag + 1e-8) * mx;
+        e.lam_b = lb / (mag + 1e-8) * mx;
+        e.unclamped = false;
+    }
+}
+
+// CollisionConstraintEnergySolver::updateAfterTimeStep
+// (energy/collision/CollisionConstraintEnergySolver.hpp:141-167)
+static void contact_after_step(Contact& e, double Cn_if_needed) {
+    if (e.lam_n > 0) e.cn_prev = Cn_if_needed;
+    if (e.unclamped && !e.use_static) e.use_static = true;
+    e.lam_n *= ALPHA * GAMMA;
+    e.lam_t *= GAMMA;
+    e.lam_b *= GAMMA;
+    e.k_n = std::max(GAMMA * e.k_n, e.k_start);
+    e.k_t = std::max(GAMMA * e.k_t, e.k_start);
+    e.k_b = std::max(GAMMA * e.k_b, e.k_start);
+}
+
+// CollisionConstraintEnergySolver::accumulate<DOF>
+// (energy/collision/CollisionConstraintEnergySolver.hpp:179-285).  gn/gt/gb are
+// the constraint gradients (DOF entries), hn/ht/hb the constraint Hessians.
+template <int DOF>
+static void contact_accumulate(const Contact& e, double Cn, double Ct, double Cb,
+                               const double* gn, const double* gt, const double* gb,
+                               const double (*hn)[DOF], const double (*ht)[DOF], const double (*hb)[DOF],
+                               double H[DOF][DOF], double G[DOF]) {
+    double cc = Cn - ALPHA * e.cn_prev;
+    double lnp = std::max(0.0, e.k_n * cc + e.lam_n);
+    double lt = e.k_t * Ct + e.lam_t, lb = e.k_b * Cb + e.lam_b;
+    double mag = std::sqrt(lt * lt + lb * lb);
+    double mu = e.use_static ? e.mu_s : e.mu_k;
+    double mx = mu * lnp;
+    if (mag > mx) {
+        double nn = std::sqrt(lt * lt + lb * lb);
+        lt = lt / (nn + 1e-8) * mx;
+        lb = lb / (nn + 1e-8) * mx;
+    }
+    double sn = e.k_n * cc + e.lam_n, st = e.k_t * Ct + e.lam_t, sb = e.k_b * Cb + e.lam_b;
+    for (int i = 0; i < DOF; i++) {
+        G[i] += lnp * gn[i] + lt * gt[i] + lb * gb[i];
+        for (int j = 0; j < DOF; j++) {
+            double h = 0;
+            h += sn * (hn ? hn[i][j] : 0.0) + e.k_n * gn[i] * gn[j];
+            h += st * (ht ? ht[i][j] : 0.0) + e.k_t * gt[i] * gt[j];
+            h += sb * (hb ? hb[i][j] : 0.0) + e.k_b * gb[i] * gb[j];
+            H[i][j] += h;
+        }
+    }
+}
+
+// GroundCollisionConstraintSolver::constraintGradientHessian
+// (energy/collision/GroundCollisionEnergySolver.hpp:27-60)
+template <int DOF>
+static void ground_accumulate(const Ctx& c, const Ground& e, double H[DOF][DOF], double G[DOF]) {
+    double Cn, Ct, Cb;
+    ground_eval(c, e, Cn, Ct, Cb);
+    double gn[DOF] = {}, gt[DOF] = {}, gb[DOF] = {};
+    gn[1] = -1; gt[0] = 1; gb[2] = 1;
+    contact_accumulate<DOF>(e, Cn, Ct, Cb, gn, gt, gb, nullptr, nullptr, nullptr, H, G);
+}
+
+// RigidBodyGroundCollisionConstraintSolver::constraintGradientHessian
+// (energy/collision/RigidBodyGroundCollisionEnergySolver.hpp:56-140)
+static void rground_accumulate(const Ctx& c, const RGround& e, double H[6][6], double G[6]) {
+    double Cn, Ct, Cb;
+    rground_eval(c, e, Cn, Ct, Cb);
+    Q4 q = c.q[c.rot[e.p]];
+    M3 R = qmat(q);
+    M3 S = skew(e.cp_local);
+    M3 RS = R * S;
+    double gn[6] = {}, gt[6] = {}, gb[6] = {};
+    double hn[6][6] = {}, ht[6][6] = {}, hb[6][6] = {};
+    auto rot_grad = [&](V3 d, double* g) {  // d^T (R S) as a column
+        for (int j = 0; j < 3; j++) g[3 + j] = d.x * RS.a[0][j] + d.y * RS.a[1][j] + d.z * RS.a[2][j];
+    };
+    auto rot_hess = [&](V3 d, double h[6][6]) {
+        M3 Hd = (-1.0) * (R.T() * skew(d) * R * S);
+        M3 Hs = 0.5 * (Hd + Hd.T());
+        for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) h[3 + i][3 + j] = Hs.a[i][j];
+    };
+    for (int i = 0; i < 3; i++) gn[i] = -e.n[i];
+    if (!(e.shape == 2 || e.shape == 1)) { rot_grad(e.n, gn); rot_hess(e.n, hn); }
+    for (int i = 0; i < 3; i++) { gt[i] = -e.t[i]; gb[i] = -e.b[i]; }
+    rot_grad(e.t, gt); rot_grad(e.b, gb);
+    rot_hess(e.t, ht); rot_hess(e.b, hb);
+    contact_accumulate<6>(e, Cn, Ct, Cb, gn, gt, gb, hn, ht, hb, H, G);
+}
+
+// OneSidedFixedJointConstraintSolver::evaluateConstraint
+// (energy/joint/OneSidedFixedJointEnergySolver.hpp:16-34)
+static void joint_eval(const Ctx& c, const Joint& e, double C[6]) {
+    V3 p = c.x[e.p];
+    Q4 q = c.q[c.rot[e.p]];
+    V3 jp = p + qrot(q, e.pos_off);
+    Q4 jq = qmul(q, e.rot_off);
+    V3 a = jp - e.ref_p;
+    V3 b = minus_s3(jq, e.ref_q);
+    for (int i = 0; i < 3; i++) { C[i] = a[i]; C[3 + i] = b[i]; }
+}
+
+// HardConstraintEnergySolver::energy (energy/HardConstraintEnergySolver.hpp:17-35)
+static double joint_energy(const Ctx& c, const Joint& e) {
+    double C[6]; joint_eval(c, e, C);
+    double E = 0;
+    for (int i = 0; i < 6; i++) E += 0.5 * e.k[i] * C[i] * C[i] + e.lam[i] * C[i];
+    return E;
+}
+
+// HardConstraintEnergySolver::accumulate<6> with
+// OneSidedFixedJointConstraintSolver::constraintGradientHessian
+// (energy/HardConstraintEnergySolver.hpp:100-155, energy/joint/OneSidedFixedJointEnergySolver.hpp:36-90)
+static void joint_accumulate(const Ctx& c, const Joint& e, double H[6][6], double G[6]) {
+    double Craw[6]; joint_eval(c, e, Craw);
+    Q4 q = c.q[c.rot[e.p]];
+    M3 R = qmat(q);
+    M3 dCp = (-1.0) * (R * skew(e.pos_off));
+    V3 th(Craw[3], Craw[4], Craw[5]);
+    M3 dCR = inv_right_jac(th) * qmat(e.rot_off).T();
+    double grad[6][6] = {};
+    for (int i = 0; i < 3; i++) {
+        grad[i][i] = 1;
+        for (int j = 0; j < 3; j++) { grad[i][3 + j] = dCp.a[i][j]; grad[3 + i][3 + j] = dCR.a[i][j]; }
+    }
+    const double lmin = std::numeric_limits<double>::lowest(), lmax = std::numeric_limits<double>::max();
+    for (int ci = 0; ci < 6; ci++) {
+        double C = Craw[ci] - ALPHA * e.cprev[ci];
+        double lu = e.k[ci] * C + e.lam[ci];
+        double lp = std::max(lmin, std::min(lmax, lu));
+        double ks = e.k[ci];
+        if (lu < lmin && std::fabs(C) > 1e-12) ks = std::fabs((lmin - e.lam[ci]) / C);
+        else if (lu > lmax && std::fabs(C) > 1e-12) ks = std::fabs((lmax - e.lam[ci]) / C);
+        for (int a = 0; a < 6; a++) {
+            G[a] += grad[ci][a] * lp;
+            for (int b = 0; b < 6; b++) H[a][b] += ks * grad[ci][a] * grad[ci][b];
+        }
+    }
+}
+
+// HardConstraintEnergySolver::updateAfterIteration (energy/HardConstraintEnergySolver.hpp:42-72)
+static void joint_after_iter(const Ctx& c, Joint& e) {
+    double C[6]; joint_eval(c, e, C);
+    const double lmin = std::numeric_limits<double>::lowest(), lmax = std::numeric_limits<double>::max();
+    for (int ci = 0; ci < 6; ci++) {
+        double cc = C[ci] - ALPHA * e.cprev[ci];
+        double lp = e.k[ci] * cc + e.lam[ci];
+        if (lp > lmin && lp < lmax) e.k[ci] += BETA * cc;
+        e.lam[ci] = std::max(lmin, std::min(lmax, lp));
+    }
+}
+
+// HardConstraintEnergySolver::updateAfterTimeStep (energy/HardConstraintEnergySolver.hpp:79-88)
+static void joint_after_step(const Ctx& c, Joint& e, double k_start) {
+    for (int i = 0; i < 6; i++) {
+        e.lam[i] = ALPHA * GAMMA * e.lam[i];
+        e.k[i] = std::max(k_start, GAMMA * e.k[i]);
+    }
+    joint_eval(c, e, e.cprev);
+}
+
+// ------------------------------------------------------- vertex block
+// Gradient / Hessian accumulation of VBDSolver::_solveParticle<DOF>
+// (simulation/VBDSolver.hpp:293-447): static energies in type order, each in
+// pool-slot order.
+template <int DOF>
+static void accumulate_block(const Ctx& c, unsigned p, double H[DOF][DOF], double G[DOF]) {
+    for (int i = 0; i < DOF; i++) { G[i] = 0; for (int j = 0; j < DOF; j++) H[i][j] = 0; }
+    unsigned beg = c.e_off[p * NTYPES], end = c.e_off[(p + 1) * NTYPES];
+    for (unsigned k = beg; k < end; k++) {
+        const Entry& en = c.entries[k];
+        switch (en.type) {
+            case NEO_HOOKEAN:
+                if (DOF == 3) nh_accumulate(c, c.nh[en.idx], en.local, (double(*)[3])H, G, c.dt);
+                break;
+            case COSSERAT_ROD:
+                if (DOF == 6) rod_accumulate(c, c.rods[en.idx], en.local, (double(*)[6])H, G);
+                break;
+            case GROUND:
+                ground_accumulate<DOF>(c, c.ground[en.idx], H, G);
+                break;
+            case RIGID_GROUND:
+                if (DOF == 6) rground_accumulate(c, c.rground[en.idx], (double(*)[6])H, G);
+                break;
+            case JOINT:
+                if (DOF == 6) joint_accumulate(c, c.joints[en.idx], (double(*)[6])H, G);
+                break;
+        }
+    }
+}
+
+// VBDSolver::_solveParticle<DOF> assembly and solve (simulation/VBDSolver.hpp:449-510)
+static void solve_particle(Ctx& c, unsigned p) {
+    if (c.fixed[p]) return;
+    double dt = c.dt;
+    if (c.oriented(p)) {
+        double H[6][6], G[6];
+        accumulate_block<6>(c, p, H, G);
+        unsigned r = c.rot[p];
+        double mass = c.m[p];
+        V3 Iv = c.I[r];
+        V3 a = (-1 / (dt * dt) * mass) * (c.x[p] - c.y[p]);
+        V3 ms = minus_s3(c.q[r], c.qy[r]);
+        double rhs[6];
+        for (int i = 0; i < 3; i++) { rhs[i] = a[i] - G[i]; rhs[3 + i] = -1 / (dt * dt) * (Iv[i] * ms[i]) - G[3 + i]; }
+        for (int i = 0; i < 3; i++) { H[i][i] += mass / (dt * dt); H[3 + i][3 + i] += Iv[i] / (dt * dt); }
+        double dx[6];
+        lu_solve<6>(H, rhs, dx);
+        c.x[p] += V3(dx[0], dx[1], dx[2]);
+        c.q[r] = plus_s3(c.q[r], V3(dx[3], dx[4], dx[5]));
+    } else {
+        double H[3][3], G[3];
+        accumulate_block<3>(c, p, H, G);
+        double mass = c.m[p];
+        V3 d = c.x[p] - c.y[p];
+        double rhs[3];
+        for (int i = 0; i < 3; i++) rhs[i] = -mass / (dt * dt) * d[i] - G[i];
+        for (int i = 0; i < 3; i++) H[i][i] += mass / (dt * dt);
+        double dx[3];
+        lu_solve<3>(H, rhs, dx);
+        c.x[p] += V3(dx[0], dx[1], dx[2]);
+    }
+}
+
+// Block residual r_p = |m/h^2 (x - y) + g_p| (the negated RHS of
+// simulation/VBDSolver.hpp:462-464,493) for the current iterate.
+static double block_residual_sq(const Ctx& c, unsigned p) {
+    double dt = c.dt;
+    if (c.oriented(p)) {
+        double H[6][6], G[6];
+        accumulate_block<6>(c, p, H, G);
+        unsigned r = c.rot[p];
+        V3 a = (c.m[p] / (dt * dt)) * (c.x[p] - c.y[p]);
+        V3 ms = minus_s3(c.q[r], c.qy[r]);
+        double s = 0;
+        for (int i = 0; i < 3; i++) {
+            double u = a[i] + G[i], w = c.I[r][i] / (dt * dt) * ms[i] + G[3 + i];
+            s += u * u + w * w;
+        }
+        return s;
+    }
+    double H[3][3], G[3];
+    accumulate_block<3>(c, p, H, G);
+    V3 a = (c.m[p] / (dt * dt)) * (c.x[p] - c.y[p]);
+    double s = 0;
+    for (int i = 0; i < 3; i++) { double u = a[i] + G[i]; s += u * u; }
+    return s;
+}
+
+static double residual(Ctx& c) {
+    double num = 0, den = 0;
+    for (unsigned p = 0; p < c.np(); p++) {
+        if (c.fixed[p]) continue;
+        num += block_residual_sq(c, p);
+        double mg = c.m[p] * c.g;
+        den += mg * mg;
+    }
+    return den > 0 ? std::sqrt(num) / std::sqrt(den) : std::sqrt(num);
+}
+
+// ----------------------------------------------------- step schedule
+// VBDSolver::_particleInertialUpdate (simulation/VBDSolver.hpp:208-248)
+static void inertial(Ctx& c, unsigned p) {
+    if (c.fixed[p]) return;
+    double dt = c.dt;
+    V3 aext(0, -c.g, 0);
+    V3 a = (c.v[p] - c.vp[p]) / dt;
+    V3 at;
+    double an = norm(aext);
+    if (an > 1e-12) {
+        double al = dot(a, aext) / an;
+        double t;
+        if (al > an) t = 1;
+        else if (al < 0) t = 0;
+        else t = al / an;
+        at = t * aext;
+    }
+    c.y[p] = c.x[p] + dt * c.v[p] + (dt * dt) * aext;
+    c.x[p] += dt * c.v[p] + (dt * dt) * at;
+    c.xl[p] = c.x[p];
+    c.xll[p] = c.x[p];
+    if (c.oriented(p)) {
+        // VBDSolver::_particleRotationInertialUpdate (simulation/VBDSolver.hpp:253-283)
+        unsigned r = c.rot[p];
+        V3 w = c.w[r], Iv = c.I[r];
+        V3 Iw(Iv.x * w.x, Iv.y * w.y, Iv.z * w.z);
+        V3 wx = cross(w, Iw);
+        V3 acc(-(1 / Iv.x) * wx.x, -(1 / Iv.y) * wx.y, -(1 / Iv.z) * wx.z);
+        V3 dqi = dt * w + (dt * dt) * acc;
+        c.qy[r] = plus_s3(c.q[r], dqi);
+        c.q[r] = plus_s3(c.q[r], dt * w);
+        c.ql[r] = c.q[r];
+        c.qll[r] = c.q[r];
+    }
+}
+
+// VBDSolver::_particleChebyshevAcceleration (simulation/VBDSolver.hpp:513-536)
+static void chebyshev(Ctx& c, unsigned p, double omega) {
+    c.x[p] = omega * (c.x[p] - c.xll[p]) + c.xll[p];
+    if (c.oriented(p)) {
+        unsigned r = c.rot[p];
+        c.q[r] = plus_s3(c.qll[r], omega * minus_s3(c.q[r], c.qll[r]));
+    }
+    c.xll[p] = c.xl[p];
+    c.xl[p] = c.x[p];
+    if (c.oriented(p)) {
+        unsigned r = c.rot[p];
+        c.qll[r] = c.ql[r];
+        c.ql[r] = c.q[r];
+    }
+}
+
+// VBDSolver::_particleVelocityUpdate (simulation/VBDSolver.hpp:538-566)
+static void velocity(Ctx& c, unsigned p) {
+    double dt = c.dt;
+    c.vp[p] = c.v[p];
+    c.v[p] = (c.x[p] - c.xp[p]) / dt;
+    c.xp[p] = c.x[p];
+    if (c.oriented(p)) {
+        unsigned r = c.rot[p];
+        c.wp[r] = c.w[r];
+        c.w[r] = minus_s3(c.q[r], c.qp[r]) / dt;
+        c.qp[r] = c.q[r];
+    }
+}
+
+// Energy hooks run at the start of each step, in EnergyRegistry order
+// (energy/EnergyRegistry.hpp:100-109, simulation/VBDSolver.hpp:54-58).
+static void after_time_step(Ctx& c) {
+    c.pool.parallel_for(0, (long)c.nh.size(), [&](long e) { nh_after_step(c, c.nh[e]); });
+    // GroundCollisionEnergySolver::updateContactPoints + updateAfterTimeStep
+    // (energy/collision/GroundCollisionEnergySolver.hpp:81-91)
+    c.pool.parallel_for(0, (long)c.ground.size(), [&](long i) {
+        Ground& e = c.ground[i];
+        e.cp_x = c.x[e.p].x;
+        e.cp_z = c.x[e.p].z;
+        double Cn, Ct, Cb;
+        ground_eval(c, e, Cn, Ct, Cb);
+        contact_after_step(e, Cn);
+    });
+    // RigidBodyGroundCollisionEnergySolver::updateContactPoints
+    // (energy/collision/RigidBodyGroundCollisionEnergySolver.hpp:161-183)
+    for (auto& e : c.rground) {
+        e.cp_ground.x = c.x[e.p].x;
+        e.cp_ground.z = c.x[e.p].z;
+        if (e.shape == 2 || e.shape == 1)
+            e.cp_local = qrot(qconj(c.q[c.rot[e.p]]), V3(0, -e.radius, 0));
+        double Cn, Ct, Cb;
+        rground_eval(c, e, Cn, Ct, Cb);
+        contact_after_step(e, Cn);
+    }
+    for (auto& e : c.joints) joint_after_step(c, e, c.joint_k_start);
+}
+
+static void after_iteration(Ctx& c) {
+    c.pool.parallel_for(0, (long)c.ground.size(), [&](long i) {
+        double Cn, Ct, Cb;
+        ground_eval(c, c.ground[i], Cn, Ct, Cb);
+        contact_after_iter(c.ground[i], Cn, Ct, Cb);
+    });
+    for (auto& e : c.rground) {
+        double Cn, Ct, Cb;
+        rground_eval(c, e, Cn, Ct, Cb);
+        contact_after_iter(e, Cn, Ct, Cb);
+    }
+    for (auto& e : c.joints) joint_after_iter(c, e);
+}
+
+static void collision_stage(Ctx& c);
+
+// VBDSolver::solve_Parallel (simulation/VBDSolver.hpp:48-103) preceded by the
+// collision stage of SimulationExecutor::_workerTimeStep
+// (simulation/SimulationExecutor.hpp:142-156).
+static void time_step(Ctx& c) {
+    if (!c.prims.empty()) collision_stage(c);
+    after_time_step(c);
+    long n = (long)c.np();
+    c.pool.parallel_for(0, n, [&](long p) { inertial(c, (unsigned)p); });
+    double omega = 1;
+    unsigned max_it = c.tol > 0 ? c.max_iters : c.iters;
+    unsigned it = 0;
+    for (; it < max_it; it++) {
+        if (it > 2) omega = 4 / (4 - c.rho * c.rho * omega);
+        else if (it == 2) omega = 2 / (2 - c.rho * c.rho);
+        else omega = 1;
+        for (unsigned col = 0; col < c.num_colors; col++) {
+            c.pool.parallel_for(c.color_offsets[col], c.color_offsets[col + 1],
+                                [&](long k) { solve_particle(c, c.work_list[k]); });
+        }
+        c.pool.parallel_for(0, n, [&](long p) { chebyshev(c, (unsigned)p, omega); });
+        after_iteration(c);
+        if (c.tol > 0) {
+            c.last_residual = residual(c);
+            if (c.last_residual <= c.tol) { it++; break; }
+        }
+    }
+    c.iterations += it;
+    c.pool.parallel_for(0, n, [&](long p) { velocity(c, (unsigned)p); });
+}
+
+// ------------------------------------------------- adjacency / coloring
+// StaticParticleAdjacency::buildAdjacency (common/StaticParticleAdjacency.hpp:42-133):
+// entries grouped per particle by type, then by pool slot; neighbour sets are
+// the distinct other particles of every shared static energy.
+static void build_adjacency(Ctx& c) {
+    unsigned n = c.np();
+    std::vector<unsigned> val((size_t)n * NTYPES, 0);
+    std::vector<std::vector<unsigned>> nb(n);
+    auto visit = [&](uint8_t type, const unsigned* idx, int k) {
+        for (int a = 0; a < k; a++) {
+            val[(size_t)idx[a] * NTYPES + type]++;
+            for (int b = 0; b < k; b++) if (a != b) nb[idx[a]].push_back(idx[b]);
+        }
+    };
+    for (auto& e : c.nh) visit(NEO_HOOKEAN, e.idx, 4);
+    for (auto& e : c.rods) visit(COSSERAT_ROD, e.idx, 2);
+    for (auto& e : c.ground) visit(GROUND, &e.p, 1);
+    for (auto& e : c.rground) visit(RIGID_GROUND, &e.p, 1);
+    for (auto& e : c.joints) visit(JOINT, &e.p, 1);
+    c.e_off.assign((size_t)(n + 1) * NTYPES, 0);
+    unsigned run = 0;
+    for (unsigned p = 0; p < n; p++)
+        for (int t = 0; t < NTYPES; t++) { c.e_off[(size_t)p * NTYPES + t] = run; run += val[(size_t)p * NTYPES + t]; }
+    for (int t = 0; t < NTYPES; t++) c.e_off[(size_t)n * NTYPES + t] = run;
+    c.entries.assign(run, Entry{});
+    std::vector<unsigned> cur(c.e_off.begin(), c.e_off.end());
+    auto scatter = [&](uint8_t type, const unsigned* idx, int k, unsigned slot) {
+        for (int a = 0; a < k; a++) c.entries[cur[(size_t)idx[a] * NTYPES + type]++] = Entry{type, slot, (uint16_t)a};
+    };
+    for (unsigned s = 0; s < c.nh.size(); s++) scatter(NEO_HOOKEAN, c.nh[s].idx, 4, s);
+    for (unsigned s = 0; s < c.rods.size(); s++) scatter(COSSERAT_ROD, c.rods[s].idx, 2, s);
+    for (unsigned s = 0; s < c.ground.size(); s++) scatter(GROUND, &c.ground[s].p, 1, s);
+    for (unsigned s = 0; s < c.rground.size(); s++) scatter(RIGID_GROUND, &c.rground[s].p, 1, s);
+    for (unsigned s = 0; s < c.joints.size(); s++) scatter(JOINT, &c.joints[s].p, 1, s);
+    c.p_off.assign(n + 1, 0);
+    c.p_nbr.clear();
+    for (unsigned p = 0; p < n; p++) {
+        auto& v = nb[p];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        c.p_off[p + 1] = c.p_off[p] + (unsigned)v.size();
+        c.p_nbr.insert(c.p_nbr.end(), v.begin(), v.end());
+    }
+}
+
+// ColorList::greedyColor2 -- DSATUR, verbatim O(V^2) selection
+// (common/ColorList.hpp:149-241).
+static void dsatur_reference(Ctx& c) {
+    unsigned n = c.np();
+    const unsigned UNC = UINT32_MAX;
+    c.color.assign(n, UNC);
+    std::vector<unsigned> sat(n, 0);
+    unsigned ncol = 0;
+    std::vector<char> used;
+    for (unsigned it = 0; it < n; it++) {
+        unsigned best = UNC;
+        for (unsigned j = 0; j < n; j++) {
+            if (c.color[j] != UNC) continue;
+            if (best == UNC) best = j;
+            unsigned db = c.p_off[best + 1] - c.p_off[best];
+            unsigned dj = c.p_off[j + 1] - c.p_off[j];
+            if (sat[j] > sat[best]) best = j;
+            else if (sat[j] == sat[best] && dj > db) best = j;
+        }
+        used.assign(ncol + 1, 0);
+        for (unsigned e = c.p_off[best]; e < c.p_off[best + 1]; e++) {
+            unsigned nbh = c.p_nbr[e];
+            if (c.color[nbh] != UNC) used[c.color[nbh]] = 1;
+        }
+        unsigned col = 0;
+        while (col < used.size() && used[col]) col++;
+        c.color[best] = col;
+        ncol = std::max(ncol, col + 1);
+        for (unsigned e = c.p_off[best]; e < c.p_off[best + 1]; e++) {
+            unsigned u = c.p_nbr[e];
+            if (c.color[u] != UNC) continue;
+            std::vector<char> seen(ncol, 0);
+            unsigned cnt = 0;
+            for (unsigned k = c.p_off[u]; k < c.p_off[u + 1]; k++) {
+                unsigned w = c.p_nbr[k];
+                if (c.color[w] != UNC && !seen[c.color[w]]) { seen[c.color[w]] = 1; cnt++; }
+            }
+            sat[u] = cnt;
+        }
+    }
+    c.num_colors = ncol;
+}
+
+// Same selection rule as dsatur_reference -- maximise (saturation, degree),
+// ties to the lowest index -- kept in a lazy max-heap so that large scenes
+// finish in O((V+E) log V).  Produces the identical coloring.
+static void dsatur_fast(Ctx& c) {
+    unsigned n = c.np();
+    const unsigned UNC = UINT32_MAX;
+    c.color.assign(n, UNC);
+    std::vector<unsigned> sat(n, 0);
+    std::vector<std::array<uint64_t, 4>> seen(n, {0, 0, 0, 0});
+    std::priority_queue<std::tuple<unsigned, unsigned, unsigned>> pq;  // (sat, deg, ~idx)
+    for (unsigned p = 0; p < n; p++) pq.push({0u, c.p_off[p + 1] - c.p_off[p], ~p});
+    unsigned ncol = 0;
+    while (!pq.empty()) {
+        auto [s, d, ni] = pq.top();
+        pq.pop();
+        unsigned v = ~ni;
+        if (c.color[v] != UNC || s != sat[v]) continue;
+        uint64_t used[5] = {0, 0, 0, 0, 0};
+        for (unsigned e = c.p_off[v]; e < c.p_off[v + 1]; e++) {
+            unsigned w = c.p_nbr[e];
+            if (c.color[w] != UNC) used[c.color[w] >> 6] |= 1ull << (c.color[w] & 63);
+        }
+        unsigned col = 0;
+        while (col < 320 && (used[col >> 6] >> (col & 63) & 1)) col++;
+        if (col >= 256) throw std::runtime_error("Ran out of colors!");
+        c.color[v] = col;
+        ncol = std::max(ncol, col + 1);
+        for (unsigned e = c.p_off[v]; e < c.p_off[v + 1]; e++) {
+            unsigned u = c.p_nbr[e];
+            if (c.color[u] != UNC) continue;
+            uint64_t& word = seen[u][col >> 6];
+            if (!(word >> (col & 63) & 1)) {
+                word |= 1ull << (col & 63);
+                sat[u]++;
+                pq.push({sat[u], c.p_off[u + 1] - c.p_off[u], ~u});
+            }
+        }
+    }
+    c.num_colors = ncol;
+}
+
+// ColorList::rebuildWorkList (common/ColorList.hpp:345-363)
+static void rebuild_work_list(Ctx& c) {
+    unsigned n = c.np();
+    std::vector<unsigned> cnt(c.num_colors, 0);
+    for (unsigned p = 0; p < n; p++) cnt[c.color[p]]++;
+    c.color_offsets.assign(c.num_colors + 1, 0);
+    for (unsigned k = 0; k < c.num_colors; k++) c.color_offsets[k + 1] = c.color_offsets[k] + cnt[k];
+    c.work_list.assign(n, 0);
+    std::vector<unsigned> cur(c.color_offsets.begin(), c.color_offsets.end() - 1);
+    for (unsigned p = 0; p < n; p++) c.work_list[cur[c.color[p]]++] = p;
+}
+
+// ----------------------------------------------------------------- LBVH
+static inline double dmin_(double a, double b) { return (b < a) ? b : a; }  // std::min
+static inline double dmax_(double a, double b) { return (a < b) ? b : a; }  // std::max
+
+// CollisionPrimitivePool::speculativeGlobalBounds (collision/CollisionPrimitivePool.hpp:160-236)
+static void spec_bounds(const Ctx& c, const Prim& pr, double* bx) {
+    double mn[3] = {std::numeric_limits<double>::max(), std::numeric_limits<double>::max(), std::numeric_limits<double>::max()};
+    double mx[3] = {std::numeric_limits<double>::lowest(), std::numeric_limits<double>::lowest(), std::numeric_limits<double>::lowest()};
+    auto expand = [&](V3 p) { for (int i = 0; i < 3; i++) { mn[i] = dmin_(mn[i], p[i]); mx[i] = dmax_(mx[i], p[i]); } };
+    const double dt = c.dt;
+    if (pr.type == 0) {
+        for (int k = 0; k < 3; k++) {
+            V3 p = c.x[pr.idx[k]];
+            expand(p);
+            V3 dv = dt * c.v[pr.idx[k]];
+            expand(p + dv);
+        }
+    } else if (pr.type == 1) {
+        V3 p1 = c.x[pr.idx[0]], p2 = c.x[pr.idx[1]];
+        double r = pr.radius;
+        for (int i = 0; i < 3; i++) { mn[i] = dmin_(p1[i], p2[i]) - r; mx[i] = dmax_(p1[i], p2[i]) + r; }
+        V3 n1 = p1 + dt * c.v[pr.idx[0]], n2 = p2 + dt * c.v[pr.idx[1]];
+        for (int i = 0; i < 3; i++) { mn[i] = dmin_(mn[i], dmin_(n1[i], n2[i]) - r); mx[i] = dmax_(mx[i], dmax_(n1[i], n2[i]) + r); }
+    } else {
+        // sphere: local bounds [-r, r]^3 centred on the particle (collision/SDF.hpp)
+        unsigned op = pr.idx[0];
+        double r = pr.radius;
+        V3 lmin(-r, -r, -r), lmax(r, r, r);
+        V3 ctr = 0.5 * (lmin + lmax);
+        V3 he = 0.5 * (lmax - lmin);
+        Q4 q = c.q[c.rot[op]];
+        V3 wc = qrot(q, ctr) + c.x[op];
+        M3 R = qmat(q);
+        M3 A; for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) A.a[i][j] = std::fabs(R.a[i][j]);
+        V3 we = A * he;
+        for (int i = 0; i < 3; i++) { mn[i] = wc[i] - we[i]; mx[i] = wc[i] + we[i]; }
+        Q4 nq = plus_s3(q, dt * c.w[c.rot[op]]);
+        V3 nwc = qrot(nq, ctr) + c.x[op] + dt * c.v[op];
+        M3 NR = qmat(nq);
+        for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) A.a[i][j] = std::fabs(NR.a[i][j]);
+        V3 nwe = A * he;
+        for (int i = 0; i < 3; i++) { mn[i] = dmin_(mn[i], nwc[i] - nwe[i]); mx[i] = dmax_(mx[i], nwc[i] + nwe[i]); }
+    }
+    for (int i = 0; i < 3; i++) { bx[i] = mn[i]; bx[3 + i] = mx[i]; }
+}
+
+// LBVHBuilder::expandBits21 / morton3D_64 (collision/LBVHBuilder.hpp:65-85)
+static inline uint64_t expand21(uint64_t v) {
+    v &= 0x1FFFFFull;
+    v = (v | (v << 32)) & 0x1F00000000FFFFull;
+    v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+static inline uint64_t morton64(double nx, double ny, double nz) {
+    double x = std::clamp(nx * 2097152.0, 0.0, 2097151.0);
+    double y = std::clamp(ny * 2097152.0, 0.0, 2097151.0);
+    double z = std::clamp(nz * 2097152.0, 0.0, 2097151.0);
+    return expand21((uint64_t)x) | (expand21((uint64_t)y) << 1) | (expand21((uint64_t)z) << 2);
+}
+
+// LBVHBuilder::constructTree (collision/LBVHBuilder.cpp:181-286)
+static void construct_tree(Ctx& c, unsigned nprim) {
+    int n = (int)nprim;
+    unsigned nn = 2 * nprim - 1;
+    const unsigned INV = UINT32_MAX;
+    c.left.assign(nn, INV); c.right.assign(nn, INV); c.parent.assign(nn, INV);
+    c.leaf_count.assign(nn, 0); c.subtree.assign(nn, 0);
+    // LBVHBuilder::commonPrefixLen (collision/LBVHBuilder.hpp:33-41): equal
+    // codes fall back to the primitive indices
+    auto delta = [&](int i, int j) -> int {
+        if (j < 0 || j >= n) return -1;
+        unsigned si = c.sorted[i], sj = c.sorted[j];
+        uint64_t a = c.morton[si], b = c.morton[sj];
+        if (a == b) {
+            uint64_t x = (uint64_t)si ^ (uint64_t)sj;
+            return 64 + (x ? __builtin_clzll(x) : 64);
+        }
+        return __builtin_clzll(a ^ b);
+    };
+    for (int i = 0; i < n - 1; i++) {
+        int d = (delta(i, i + 1) - delta(i, i - 1) >= 0) ? 1 : -1;
+        int dmin = delta(i, i - d);
+        int lmax = 128;
+        while (delta(i, i + lmax * d) > dmin) lmax *= 4;
+        int l = 0;
+        for (unsigned t = lmax; t >= 1; t /= 2)
+            if (delta(i, i + (l + (int)t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = delta(i, j);
+        int s = 0;
+        for (int t = (l + 1) / 2; t >= 1; t = (t == 1 ? 0 : (t + 1) / 2)) {
+            int ns = s + t;
+            if (ns < l && delta(i, i + ns * d) > dnode) s = ns;
+        }
+        int gamma = i + s * d + std::min(d, 0);
+        unsigned g = (unsigned)(i + n);
+        if (std::min(i, j) == gamma) { c.left[g] = gamma; c.parent[gamma] = g; }
+        else { c.left[g] = n + gamma; c.parent[n + gamma] = g; }
+        if (std::max(i, j) == gamma + 1) { c.right[g] = gamma + 1; c.parent[gamma + 1] = g; }
+        else { c.right[g] = n + gamma + 1; c.parent[n + gamma + 1] = g; }
+    }
+    unsigned node = 0;
+    while (c.parent[node] != INV) node = c.parent[node];
+    c.root = node;
+    for (int l = 0; l < n; l++) { c.leaf_count[l] = 1; c.subtree[l] = 1; }
+}
+
+// LBVHBuilder::assembleBVH, serial refit (collision/LBVHBuilder.cpp:410-453)
+static void refit(Ctx& c, unsigned n) {
+    unsigned nn = 2 * n - 1;
+    c.nbounds.assign((size_t)nn * 6, 0);
+    std::vector<uint8_t> visited(nn, 0);
+    for (unsigned l = 0; l < n; l++) {
+        const double* b = &c.aabb[(size_t)c.sorted[l] * 6];
+        for (int k = 0; k < 6; k++) c.nbounds[(size_t)l * 6 + k] = b[k];
+        unsigned node = c.parent[l];
+        while (node != UINT32_MAX) {
+            if (visited[node]++ == 0) break;
+            unsigned a = c.left[node], bb = c.right[node];
+            for (int k = 0; k < 3; k++) {
+                c.nbounds[(size_t)node * 6 + k] = dmin_(c.nbounds[(size_t)a * 6 + k], c.nbounds[(size_t)bb * 6 + k]);
+                c.nbounds[(size_t)node * 6 + 3 + k] = dmax_(c.nbounds[(size_t)a * 6 + 3 + k], c.nbounds[(size_t)bb * 6 + 3 + k]);
+            }
+            c.subtree[node] = c.subtree[a] + c.subtree[bb];
+            node = c.parent[node];
+        }
+    }
+}
+
+// LBVHTraversal::traverseSelfIterative (collision/LBVHTraversal.hpp:30-88)
+static void traverse(Ctx& c) {
+    c.pairs.clear();
+    std::vector<std::pair<unsigned, unsigned>> st;
+    st.push_back({c.root, c.root});
+    auto ov = [&](unsigned a, unsigned b) {
+        const double* A = &c.nbounds[(size_t)a * 6];
+        const double* B = &c.nbounds[(size_t)b * 6];
+        return A[0] <= B[3] && A[1] <= B[4] && A[2] <= B[5] && A[3] >= B[0] && A[4] >= B[1] && A[5] >= B[2];
+    };
+    while (!st.empty()) {
+        auto [a, b] = st.back();
+        st.pop_back();
+        if (!ov(a, b)) continue;
+        bool la = c.leaf_count[a] > 0, lb = c.leaf_count[b] > 0;
+        if (la && lb) { if (a < b) c.pairs.push_back({a, b}); continue; }
+        if (a == b) {
+            unsigned l = c.left[a], r = c.right[a];
+            st.push_back({l, l}); st.push_back({r, r}); st.push_back({l, r});
+            continue;
+        }
+        if (la || (!lb && c.subtree[b] > c.subtree[a])) {
+            st.push_back({a, c.left[b]}); st.push_back({a, c.right[b]});
+        } else {
+            st.push_back({c.left[a], b}); st.push_back({c.right[a], b});
+        }
+    }
+    std::sort(c.pairs.begin(), c.pairs.end());
+}
+
+// LBVHBuilder::buildBVH + broad phase (collision/LBVHBuilder.cpp:13-25,
+// collision/CollisionDetector.cpp:24-55).  Narrow phase: triangle-triangle and
+// rod-rod are no-ops in the reference (CollisionDetector.cpp:589-599,668-676);
+// sphere-sphere and sphere-rod throw there (CollisionDetector.cpp:180-213,678-687).
+static void collision_stage(Ctx& c) {
+    unsigned n = (unsigned)c.prims.size();
+    if (n == 0) { c.pairs.clear(); return; }
+    c.aabb.assign((size_t)n * 6, 0);
+    double smin[3] = {std::numeric_limits<double>::max(), std::numeric_limits<double>::max(), std::numeric_limits<double>::max()};
+    double smax[3] = {std::numeric_limits<double>::lowest(), std::numeric_limits<double>::lowest(), std::numeric_limits<double>::lowest()};
+    std::vector<double> cen((size_t)n * 3);
+    for (unsigned p = 0; p < n; p++) {
+        double* b = &c.aabb[(size_t)p * 6];
+        spec_bounds(c, c.prims[p], b);
+        for (int i = 0; i < 3; i++) {
+            cen[(size_t)p * 3 + i] = (b[i] + b[3 + i]) * 0.5;
+            smin[i] = dmin_(smin[i], b[i]);
+            smax[i] = dmax_(smax[i], b[3 + i]);
+        }
+    }
+    double ext[3];
+    for (int i = 0; i < 3; i++) ext[i] = dmax_(smax[i] - smin[i], 1e-6);
+    c.morton.assign(n, 0);
+    for (unsigned p = 0; p < n; p++) {
+        double nc[3];
+        for (int i = 0; i < 3; i++) nc[i] = (cen[(size_t)p * 3 + i] - smin[i]) / ext[i];
+        c.morton[p] = morton64(nc[0], nc[1], nc[2]);
+    }
+    // Algorithm::radixSort: stable LSD, 8 passes of 8 bits (common/Algorithm.hpp:22-56)
+    c.sorted.resize(n);
+    std::iota(c.sorted.begin(), c.sorted.end(), 0u);
+    std::vector<unsigned> tmp(n);
+    for (int sh = 0; sh < 64; sh += 8) {
+        size_t cnt[256] = {};
+        for (unsigned i : c.sorted) cnt[(c.morton[i] >> sh) & 255]++;
+        size_t s = 0;
+        for (int b = 0; b < 256; b++) { size_t t = cnt[b]; cnt[b] = s; s += t; }
+        for (unsigned i : c.sorted) tmp[cnt[(c.morton[i] >> sh) & 255]++] = i;
+        c.sorted.swap(tmp);
+    }
+    construct_tree(c, n);
+    refit(c, n);
+    traverse(c);
+}
+
+}  // namespace orc
+
+// =================================================================== C API
+using namespace orc;
+
+static thread_local std::string g_err;
+
+#define ORC_TRY(body) try { body; return 0; } catch (const std::exception& ex) { g_err = ex.what(); return 2; }
+
+extern "C" {
+
+const char* orc_last_error(void) { return g_err.c_str(); }
+
+void* orc_create(void) { return new Ctx(); }
+void orc_destroy(void* h) { delete (Ctx*)h; }
+
+void orc_set_params(void* h, double dt, double g, double margin) {
+    Ctx& c = *(Ctx*)h; c.dt = dt; c.g = g; c.margin = margin;
+}
+void orc_set_solver(void* h, unsigned iters, double rho, double tol, unsigned max_iters) {
+    Ctx& c = *(Ctx*)h; c.iters = iters; c.rho = rho; c.tol = tol; c.max_iters = max_iters;
+}
+void orc_set_threads(void* h, int n) {
+    Ctx& c = *(Ctx*)h;
+    c.nthreads = n < 1 ? 1 : n;
+    c.pool.start(c.nthreads);
+}
+
+// Scenes are disjoint components; DSATUR over disjoint components colors each
+// component exactly as a separate context would, so no bookkeeping is needed.
+void orc_begin_scene(void* h) { ((Ctx*)h)->num_scenes++; }
+
+// ParticlePool::addParticle (common/ParticlePool.hpp:217-240)
+unsigned orc_particles_add(void* h, unsigned n, const double* pos, const double* mass) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = c.np();
+    bool first_scene = c.x.empty();
+    for (unsigned i = 0; i < n; i++) {
+        V3 p(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        c.x.push_back(p); c.xb.push_back(p); c.y.push_back(p); c.xp.push_back(p); c.xl.push_back(p); c.xll.push_back(p);
+        c.v.push_back(V3()); c.vp.push_back(V3());
+        c.m.push_back(mass[i]); c.fixed.push_back(0); c.rot.push_back(UINT32_MAX);
+        c.scene_of.push_back(first_scene ? 0 : c.num_scenes - 1);
+    }
+    return first;
+}
+// ParticlePool::addOrientedParticle (common/ParticlePool.hpp:257-263)
+unsigned orc_particles_add_oriented(void* h, unsigned n, const double* pos, const double* quat,
+                                    const double* mass, const double* inertia) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = orc_particles_add(h, n, pos, mass);
+    for (unsigned i = 0; i < n; i++) {
+        Q4 q{quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3]};
+        c.rot[first + i] = (unsigned)c.q.size();
+        c.q.push_back(q); c.qb.push_back(q); c.qy.push_back(q); c.qp.push_back(q); c.ql.push_back(q); c.qll.push_back(q);
+        c.w.push_back(V3()); c.wp.push_back(V3());
+        c.I.push_back(V3(inertia[3 * i], inertia[3 * i + 1], inertia[3 * i + 2]));
+    }
+    return first;
+}
+void orc_set_fixed(void* h, unsigned n, const unsigned* idx, const uint8_t* f) {
+    Ctx& c = *(Ctx*)h; for (unsigned i = 0; i < n; i++) c.fixed[idx[i]] = f[i];
+}
+void orc_set_velocities(void* h, unsigned first, unsigned n, const double* v, const double* vp) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < n; i++) {
+        c.v[first + i] = V3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        const double* s = vp ? vp : v;
+        c.vp[first + i] = V3(s[3 * i], s[3 * i + 1], s[3 * i + 2]);
+    }
+}
+void orc_set_positions_raw(void* h, unsigned first, unsigned n, const double* x) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < n; i++) c.x[first + i] = V3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+}
+void orc_set_rotations_raw(void* h, unsigned first, unsigned n, const double* q) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < n; i++) c.q[c.rot[first + i]] = Q4{q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
+}
+void orc_get_positions(void* h, double* out) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < c.np(); i++) { out[3 * i] = c.x[i].x; out[3 * i + 1] = c.x[i].y; out[3 * i + 2] = c.x[i].z; }
+}
+void orc_get_velocities(void* h, double* out) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < c.np(); i++) { out[3 * i] = c.v[i].x; out[3 * i + 1] = c.v[i].y; out[3 * i + 2] = c.v[i].z; }
+}
+void orc_get_rotations(void* h, double* out) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < c.np(); i++) {
+        Q4 q = c.oriented(i) ? c.q[c.rot[i]] : Q4();
+        out[4 * i] = q.w; out[4 * i + 1] = q.x; out[4 * i + 2] = q.y; out[4 * i + 3] = q.z;
+    }
+}
+unsigned orc_num_particles(void* h) { return ((Ctx*)h)->np(); }
+
+unsigned orc_neo_hookean_add(void* h, unsigned n, const unsigned* idx, const double* lam, const double* mu,
+                             const double* kd, const double* Q, const double* V) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.nh.size();
+    for (unsigned i = 0; i < n; i++) {
+        NH e;
+        for (int k = 0; k < 4; k++) e.idx[k] = idx[4 * i + k];
+        e.lambda = lam[i]; e.mu = mu[i]; e.kd = kd[i]; e.V = V[i];
+        for (int r = 0; r < 3; r++) for (int s = 0; s < 3; s++) e.Q.a[r][s] = Q[9 * i + 3 * r + s];
+        c.nh.push_back(e);
+    }
+    return first;
+}
+unsigned orc_cosserat_rod_add(void* h, unsigned n, const unsigned* idx, const double* K, const double* L,
+                              const double* kappa) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.rods.size();
+    for (unsigned i = 0; i < n; i++) {
+        Rod e;
+        e.idx[0] = idx[2 * i]; e.idx[1] = idx[2 * i + 1];
+        for (int k = 0; k < 6; k++) e.K[k] = K[6 * i + k];
+        e.L = L[i];
+        e.kappa0 = V3(kappa[3 * i], kappa[3 * i + 1], kappa[3 * i + 2]);
+        c.rods.push_back(e);
+    }
+    return first;
+}
+// CollisionConstraintEnergyPool::addEnergy (energy/collision/CollisionConstraintEnergyPool.hpp:48-69)
+static void init_contact(Contact& e, double ks, double ms, double mk) {
+    e.lam_n = e.lam_t = e.lam_b = 0;
+    e.k_start = e.k_n = e.k_t = e.k_b = ks;
+    e.cn_prev = 0; e.mu_s = ms; e.mu_k = mk; e.use_static = false; e.unclamped = false;
+}
+unsigned orc_ground_add(void* h, unsigned n, const unsigned* p, const double* ks, const double* ms, const double* mk) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.ground.size();
+    for (unsigned i = 0; i < n; i++) {
+        Ground e; init_contact(e, ks[i], ms[i], mk[i]); e.p = p[i]; e.cp_x = e.cp_z = 0;
+        c.ground.push_back(e);
+    }
+    return first;
+}
+unsigned orc_rigid_ground_add(void* h, unsigned n, const unsigned* p, const uint8_t* shape, const double* radius,
+                              const double* cpl, const double* ks, const double* ms, const double* mk) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.rground.size();
+    for (unsigned i = 0; i < n; i++) {
+        RGround e; init_contact(e, ks[i], ms[i], mk[i]);
+        e.p = p[i]; e.shape = shape[i]; e.radius = radius[i];
+        e.cp_local = V3(cpl[3 * i], cpl[3 * i + 1], cpl[3 * i + 2]);
+        e.cp_ground = V3();
+        e.n = V3(0, 1, 0); e.t = V3(1, 0, 0); e.b = V3(0, 0, 1);
+        c.rground.push_back(e);
+    }
+    return first;
+}
+unsigned orc_joint_add(void* h, unsigned n, const unsigned* p, const double* po, const double* ro,
+                       const double* rp, const double* rq) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.joints.size();
+    for (unsigned i = 0; i < n; i++) {
+        Joint e;
+        e.p = p[i];
+        for (int k = 0; k < 6; k++) { e.k[k] = c.joint_k_start; e.lam[k] = 0; e.cprev[k] = 0; }
+        e.pos_off = V3(po[3 * i], po[3 * i + 1], po[3 * i + 2]);
+        e.rot_off = Q4{ro[4 * i], ro[4 * i + 1], ro[4 * i + 2], ro[4 * i + 3]};
+        e.ref_p = V3(rp[3 * i], rp[3 * i + 1], rp[3 * i + 2]);
+        e.ref_q = Q4{rq[4 * i], rq[4 * i + 1], rq[4 * i + 2], rq[4 * i + 3]};
+        c.joints.push_back(e);
+    }
+    return first;
+}
+unsigned orc_add_triangles(void* h, unsigned n, const unsigned* idx, unsigned obj) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.prims.size();
+    for (unsigned i = 0; i < n; i++) c.prims.push_back(Prim{0, {idx[3 * i], idx[3 * i + 1], idx[3 * i + 2]}, 3, obj, 0});
+    return first;
+}
+unsigned orc_add_rod_segments(void* h, unsigned n, const unsigned* idx, double radius, unsigned obj) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.prims.size();
+    for (unsigned i = 0; i < n; i++) c.prims.push_back(Prim{1, {idx[2 * i], idx[2 * i + 1], 0}, 2, obj, radius});
+    return first;
+}
+unsigned orc_add_spheres(void* h, unsigned n, const unsigned* p, const double* r, const unsigned* obj) {
+    Ctx& c = *(Ctx*)h;
+    unsigned first = (unsigned)c.prims.size();
+    for (unsigned i = 0; i < n; i++) c.prims.push_back(Prim{2, {p[i], 0, 0}, 1, obj[i], r[i]});
+    return first;
+}
+
+// 0 = heap DSATUR, 1 = verbatim O(V^2) DSATUR
+int orc_finalize(void* h, int reference_dsatur) {
+    Ctx& c = *(Ctx*)h;
+    ORC_TRY({
+        build_adjacency(c);
+        if (reference_dsatur) dsatur_reference(c); else dsatur_fast(c);
+        if (c.num_colors > 256) throw std::runtime_error("Ran out of colors!");
+        rebuild_work_list(c);
+        c.finalized = true;
+    });
+}
+
+int orc_step(void* h, unsigned n) {
+    Ctx& c = *(Ctx*)h;
+    if (!c.finalized) { g_err = "finalize first"; return 8; }
+    ORC_TRY({ for (unsigned s = 0; s < n; s++) time_step(c); });
+}
+
+// Wall time (seconds) of n steps, the CPU-baseline measurement.
+double orc_time_steps(void* h, unsigned n) {
+    Ctx& c = *(Ctx*)h;
+    auto t0 = std::chrono::steady_clock::now();
+    for (unsigned s = 0; s < n; s++) time_step(c);
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+int orc_collision_stage(void* h) { ORC_TRY(collision_stage(*(Ctx*)h)); }
+void orc_after_time_step(void* h) { after_time_step(*(Ctx*)h); }
+
+void orc_get_coloring(void* h, unsigned* colors, unsigned* num_colors) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < c.np(); i++) colors[i] = c.color[i];
+    *num_colors = c.num_colors;
+}
+unsigned orc_num_entries(void* h) { return (unsigned)((Ctx*)h)->entries.size(); }
+void orc_get_adjacency(void* h, unsigned* e_off, uint8_t* type, unsigned* idx, uint16_t* local,
+                       unsigned* p_off, unsigned* p_nbr) {
+    Ctx& c = *(Ctx*)h;
+    if (e_off) std::copy(c.e_off.begin(), c.e_off.end(), e_off);
+    for (size_t k = 0; k < c.entries.size(); k++) {
+        if (type) type[k] = c.entries[k].type;
+        if (idx) idx[k] = c.entries[k].idx;
+        if (local) local[k] = c.entries[k].local;
+    }
+    if (p_off) std::copy(c.p_off.begin(), c.p_off.end(), p_off);
+    if (p_nbr) std::copy(c.p_nbr.begin(), c.p_nbr.end(), p_nbr);
+}
+unsigned orc_num_neighbors(void* h) { return (unsigned)((Ctx*)h)->p_nbr.size(); }
+
+unsigned orc_num_pairs(void* h) { return (unsigned)((Ctx*)h)->pairs.size(); }
+void orc_get_lbvh(void* h, uint64_t* morton, unsigned* sorted, unsigned* left, unsigned* right, unsigned* parent,
+                  unsigned* subtree, double* bounds, unsigned* root, unsigned* pairs) {
+    Ctx& c = *(Ctx*)h;
+    unsigned n = (unsigned)c.prims.size();
+    if (morton) std::copy(c.morton.begin(), c.morton.end(), morton);
+    if (sorted) std::copy(c.sorted.begin(), c.sorted.end(), sorted);
+    if (n == 0) return;
+    if (left) std::copy(c.left.begin(), c.left.end(), left);
+    if (right) std::copy(c.right.begin(), c.right.end(), right);
+    if (parent) std::copy(c.parent.begin(), c.parent.end(), parent);
+    if (subtree) std::copy(c.subtree.begin(), c.subtree.end(), subtree);
+    if (bounds) std::copy(c.nbounds.begin(), c.nbounds.end(), bounds);
+    if (root) *root = c.root;
+    if (pairs) for (size_t k = 0; k < c.pairs.size(); k++) { pairs[2 * k] = c.pairs[k].first; pairs[2 * k + 1] = c.pairs[k].second; }
+}
+
+// Karras tree + refit + traversal on caller-provided codes and boxes
+// (the inputs of test/test_lbvh.cpp:31-70 and :168-301).
+int orc_lbvh_from_codes(void* h, unsigned n, const uint64_t* codes, const double* boxes) {
+    Ctx& c = *(Ctx*)h;
+    if (n == 0) { c.pairs.clear(); return 0; }
+    ORC_TRY({
+        c.prims.assign(n, Prim{0, {0, 0, 0}, 0, 0, 0});
+        c.morton.assign(codes, codes + n);
+        c.aabb.assign((size_t)n * 6, 0);
+        if (boxes) std::copy(boxes, boxes + (size_t)n * 6, c.aabb.begin());
+        c.sorted.resize(n);
+        std::iota(c.sorted.begin(), c.sorted.end(), 0u);
+        std::stable_sort(c.sorted.begin(), c.sorted.end(), [&](unsigned a, unsigned b) { return c.morton[a] < c.morton[b]; });
+        construct_tree(c, n);
+        refit(c, n);
+        traverse(c);
+    });
+}
+
+int orc_debug_block(void* h, unsigned p, double* G, double* H, int* dof) {
+    Ctx& c = *(Ctx*)h;
+    if (c.oriented(p)) {
+        double HH[6][6], GG[6];
+        accumulate_block<6>(c, p, HH, GG);
+        for (int i = 0; i < 6; i++) { G[i] = GG[i]; for (int j = 0; j < 6; j++) H[6 * i + j] = HH[i][j]; }
+        *dof = 6;
+    } else {
+        double HH[3][3], GG[3];
+        accumulate_block<3>(c, p, HH, GG);
+        for (int i = 0; i < 3; i++) { G[i] = GG[i]; for (int j = 0; j < 3; j++) H[3 * i + j] = HH[i][j]; }
+        *dof = 3;
+    }
+    return 0;
+}
+
+// Per-element energies (NeoHookeanEnergySolver::energy, CosseratRodEnergySolver::energy,
+// HardConstraintEnergySolver::energy) for the finite-difference checks.
+double orc_energy(void* h, int type, unsigned slot) {
+    Ctx& c = *(Ctx*)h;
+    switch (type) {
+        case NEO_HOOKEAN: return nh_energy(c, c.nh[slot], c.dt);
+        case COSSERAT_ROD: return rod_energy(c, c.rods[slot]);
+        case JOINT: return joint_energy(c, c.joints[slot]);
+    }
+    return 0;
+}
+// Single-element accumulate for the finite-difference checks (no adjacency needed).
+void orc_element_accumulate(void* h, int type, unsigned slot, unsigned local, double* G, double* H) {
+    Ctx& c = *(Ctx*)h;
+    if (type == NEO_HOOKEAN) {
+        double HH[3][3] = {}, GG[3] = {};
+        nh_accumulate(c, c.nh[slot], local, HH, GG, c.dt);
+        for (int i = 0; i < 3; i++) { G[i] = GG[i]; for (int j = 0; j < 3; j++) H[3 * i + j] = HH[i][j]; }
+    } else {
+        double HH[6][6] = {}, GG[6] = {};
+        if (type == COSSERAT_ROD) rod_accumulate(c, c.rods[slot], local, HH, GG);
+        else if (type == JOINT) joint_accumulate(c, c.joints[slot], HH, GG);
+        for (int i = 0; i < 6; i++) { G[i] = GG[i]; for (int j = 0; j < 6; j++) H[6 * i + j] = HH[i][j]; }
+    }
+}
+
+double orc_residual(void* h) { return residual(*(Ctx*)h); }
+double orc_last_residual(void* h) { return ((Ctx*)h)->last_residual; }
+unsigned long long orc_iterations(void* h) { return ((Ctx*)h)->iterations; }
+
+// Math::Exp_s3 / Log_S3 / QuaternionFromXYZEulerAngles for test inputs
+void orc_exp_s3(const double* v, double* q) {
+    Q4 r = exp_s3(V3(v[0], v[1], v[2])); q[0] = r.w; q[1] = r.x; q[2] = r.y; q[3] = r.z;
+}
+void orc_quat_from_xyz_euler(const double* e, double* q) {  // common/Math.hpp:298-318
+    double x = e[0] * M_PI / 180.0, y = e[1] * M_PI / 180.0, z = e[2] * M_PI / 180.0;
+    Q4 qx{std::cos(x * 0.5), std::sin(x * 0.5), 0, 0};
+    Q4 qy{std::cos(y * 0.5), 0, std::sin(y * 0.5), 0};
+    Q4 qz{std::cos(z * 0.5), 0, 0, std::sin(z * 0.5)};
+    Q4 r = qmul(qmul(qz, qy), qx);
+    q[0] = r.w; q[1] = r.x; q[2] = r.y; q[3] = r.z;
+}
+void orc_plus_s3(const double* q, const double* v, double* out) {
+    Q4 r = plus_s3(Q4{q[0], q[1], q[2], q[3]}, V3(v[0], v[1], v[2]));
+    out[0] = r.w; out[1] = r.x; out[2] = r.y; out[3] = r.z;
+}
+
+}  // extern "C"

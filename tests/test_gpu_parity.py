@@ -1,0 +1,139 @@
+"""Parity of the engine (through its C-ABI) with the FP64 oracle.
+
+Tolerances (max vertex position error relative to the scene's bounding-box
+diagonal):
+  * FP64 engine vs oracle: 1e-9 -- same algorithm, only the summation order and
+    the block-solve factorisation differ;
+  * FP32 engine vs oracle: 1e-5 -- FP32 accumulation with the FP64 fallback of
+    ill-conditioned blocks.
+Integer outputs (coloring) are compared bit for bit.
+"""
+import numpy as np
+import pytest
+
+from avbd_b200 import Context, scenes
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-9
+TOL32 = 1e-5
+
+
+def pair(sc, oracle_lib, precision="fp32", **kw):
+    e = Context()
+    sc.load(e, precision=precision, **kw)
+    e.finalize()
+    o = oracle_lib.Oracle()
+    sc.load(o, **kw)
+    o.finalize()
+    return e, o
+
+
+def rel_err(e, o, sc):
+    return np.abs(e.positions() - o.positions()).max() / sc.bbox_diagonal()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_cube_fixed_bottom_100_steps(oracle_lib, precision, tol):
+    sc = scenes.cube_fixed_bottom(8)
+    e, o = pair(sc, oracle_lib, precision)
+    ce, nce = e.coloring()
+    co, nco = o.coloring()
+    assert nce == nco and (ce == co).all()
+    x0 = o.positions()
+    for _ in range(10):
+        e.step(10)
+        o.step(10)
+        assert rel_err(e, o, sc) < tol
+    assert np.abs(o.positions() - x0).max() > 1e-3  # the cube moved
+    np.testing.assert_allclose(e.velocities(), o.velocities(), atol=tol * sc.bbox_diagonal() * 60 * 10)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL64), ("fp32", TOL32)])
+def test_cube_drop_ground_contact(oracle_lib, precision, tol):
+    sc = scenes.cube_drop(n=6, iters=20, surface=True)
+    e, o = pair(sc, oracle_lib, precision)
+    for _ in range(6):
+        e.step(10)
+        o.step(10)
+    err = rel_err(e, o, sc)
+    assert o.positions()[:, 1].min() < 0.05  # it reached the ground
+    assert err < (tol if precision == "fp64" else 1e-4), err
+
+
+def test_damping_fp64(oracle_lib):
+    sc = scenes.Scene(name="damped", dt=1 / 60, solver_iters=10, iter_acceleration=0.5)
+    scenes.add_tet_cube(sc, 4, E=1e5, nu=0.4, kd=10.0, fix_bottom=True)
+    e, o = pair(sc, oracle_lib, "fp64")
+    e.step(30)
+    o.step(30)
+    assert rel_err(e, o, sc) < TOL64
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_block_gradient_hessian(oracle_lib, precision):
+    """avbd_debug_block vs the oracle's accumulate at a perturbed state (the
+    scalar-vs-AVX comparison of test/test_neohookean_accumulate.cpp:51-84)."""
+    sc = scenes.cube_drop(n=4, surface=False)
+    e, o = pair(sc, oracle_lib, precision)
+    rng = np.random.default_rng(0)
+    X = o.positions() + rng.uniform(-0.02, 0.02, size=(o.num_particles, 3))
+    if precision == "fp32":
+        X = X.astype(np.float32).astype(np.float64)
+    e.set_positions(0, X)
+    o.set_positions_raw(0, X)
+    rtol = 1e-10 if precision == "fp64" else 2e-4
+    for p in rng.choice(o.num_particles, 12, replace=False):
+        Ge, He = e.debug_block(int(p))
+        Go, Ho = o.debug_block(int(p))
+        scale_g = np.abs(Go).max() + 1e-12
+        scale_h = np.abs(Ho).max()
+        assert np.abs(Ge - Go).max() <= rtol * max(scale_g, scale_h * 1e-2) + 1e-9, (p, Ge, Go)
+        assert np.abs(He - Ho).max() <= rtol * scale_h, (p, He, Ho)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL64), ("fp32", TOL32 * 10)])
+def test_batched_scenes(oracle_lib, precision, tol):
+    sc = scenes.batched_cubes(num_scenes=7, seed=3, n_min=2, n_max=5, iters=15)
+    e, o = pair(sc, oracle_lib, precision)
+    ce, nce = e.coloring()
+    co, nco = o.coloring()
+    assert nce == nco and (ce == co).all()
+    e.step(20)
+    o.step(20)
+    assert rel_err(e, o, sc) < tol
+
+
+def test_coloring_bit_exact_large(oracle_lib):
+    sc = scenes.cube_drop(n=16, surface=False)
+    e, o = pair(sc, oracle_lib, "fp32")
+    ce, nce = e.coloring()
+    co, nco = o.coloring()
+    assert nce == nco and (ce == co).all()
+
+
+def test_residual_matches_oracle(oracle_lib):
+    sc = scenes.cube_drop(n=4, surface=False)
+    e, o = pair(sc, oracle_lib, "fp64")
+    e.step(3)
+    o.step(3)
+    assert abs(e.residual() - o.residual()) <= 1e-8 * max(1.0, o.residual())
+
+
+def test_run_to_tolerance(oracle_lib):
+    sc = scenes.cube_fixed_bottom(6)
+    e, o = pair(sc, oracle_lib, "fp64", residual_tolerance=1e-4, max_iters=500)
+    e.step(5)
+    o.step(5)
+    st = e.stats()
+    assert st["last_residual"] <= 1e-4
+    assert st["iterations"] == o.iterations
+    assert rel_err(e, o, sc) < 1e-7
+
+
+def test_stats_and_no_fallback_on_c1(oracle_lib):
+    sc = scenes.cube_fixed_bottom(8)
+    e, _ = pair(sc, oracle_lib, "fp32")
+    e.step(5)
+    st = e.stats()
+    assert st["iterations"] == 50 and st["kernel_launches"] > 0 and st["num_colors"] >= 4

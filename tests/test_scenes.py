@@ -1,0 +1,59 @@
+"""Scene builders reproduce the workload sizes and the set-up math of the
+reference's TetMeshObject::setup (simobject/TetMeshObject.cpp:21-113)."""
+import numpy as np
+
+from avbd_b200 import scenes
+
+
+class Recorder:
+    def __init__(self):
+        self.calls = {}
+
+    def __getattr__(self, name):
+        def f(*a, **k):
+            self.calls.setdefault(name, []).append(a)
+        return f
+
+
+def test_cube_fixed_bottom_sizes():
+    sc = scenes.cube_fixed_bottom(8)
+    assert sc.num_particles == 729 and sc.num_tets == 3072
+    r = Recorder()
+    sc.load(r)
+    (X, m), = r.calls["add_particles"]
+    assert np.isclose(m.sum(), 1000.0)  # 1 m^3 at 1000 kg/m^3
+    (slots, fl), = r.calls["set_fixed"]
+    assert len(slots) == 81 and np.allclose(X[slots, 1], 0.0)
+
+
+def test_cube_drop_sizes():
+    sc = scenes.cube_drop(32)
+    assert sc.num_particles == 35937 and sc.num_tets == 196608 and sc.num_primitives == 12288
+    r = Recorder()
+    sc.load(r)
+    (X, m), = r.calls["add_particles"]
+    assert X[:, 1].min() > 0.5 - 0.2 / 32 - 1e-12
+    (p, ks, mus, muk), = r.calls["add_ground_collision"]
+    assert np.allclose(ks, m / sc.dt ** 2) and np.allclose(mus, 0.4) and np.allclose(muk, 0.2)
+
+
+def test_tet_volumes_and_Q():
+    sc = scenes.cube_drop(4, seed=2)
+    r = Recorder()
+    sc.load(r)
+    (X, m), = r.calls["add_particles"]
+    (idx, lam, mu, kd, Q, V), = r.calls["add_neo_hookean"]
+    assert np.isclose(V.sum(), 1.0, rtol=0.05)  # perturbed 1 m cube
+    T = X[idx]
+    Xm = np.stack([T[:, 0] - T[:, 3], T[:, 1] - T[:, 3], T[:, 2] - T[:, 3]], axis=2)
+    assert np.allclose(np.einsum("nij,njk->nik", Xm, Q.reshape(-1, 3, 3)), np.eye(3), atol=1e-9)
+    E, nu = 1e6, 0.49
+    assert np.allclose(mu, E / (2 * (1 + nu))) and np.allclose(lam, E * nu / ((1 + nu) * (1 - 2 * nu)))
+
+
+def test_batched_scene_count():
+    sc = scenes.batched_cubes(num_scenes=5, seed=0, n_min=2, n_max=4)
+    r = Recorder()
+    sc.load(r)
+    assert len(r.calls["begin_scene"]) == 4
+    assert len(r.calls["add_particles"]) == 5
