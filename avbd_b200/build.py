@@ -21,6 +21,7 @@ LIB = os.path.join(HERE, "libavbd_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+                  "-Werror", "cross-execution-space-call",
                   "-Xcompiler", "-fvisibility=hidden", "-I" + os.path.join(ROOT, "include")]
 
 

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <thread>
@@ -24,6 +25,13 @@ static thread_local std::string g_err;
 static int fail(int code, const std::string& msg) {
     g_err = msg;
     return code;
+}
+
+// AVBD_TRACE=1 prints the set-up stages to stderr.
+static void trace(const char* what) {
+    static int on = -1;
+    if (on < 0) on = getenv("AVBD_TRACE") != nullptr;
+    if (on) fprintf(stderr, "[avbd] %s\n", what);
 }
 
 #define CUDA_OR_FAIL(x)                                                                      \
@@ -600,7 +608,9 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
 
     // coloring
     std::vector<unsigned> p_off, p_nbr;
+    trace("finalize: adjacency");
     build_neighbors(c, inc_off, inc_tet, p_off, p_nbr);
+    trace("finalize: dsatur");
     for (unsigned p = 0; p < n; p++)
         if (p_off[p + 1] - p_off[p] > 0xFFFFu) return fail(AVBD_ERR_UNSUPPORTED, "vertex degree above 65535");
     {
@@ -609,6 +619,7 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
         if (rc) return fail(rc, err);
     }
 
+    trace("finalize: permutation");
     // color-major permutation: [solved positional | oriented | fixed] per color
     const unsigned nc = c->num_colors;
     std::vector<unsigned> cnt(3ull * nc, 0);
@@ -637,6 +648,7 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
         c->inv[e] = i;
     }
 
+    trace("finalize: device buffers");
     // device buffers
     int rc;
     if ((rc = dalloc(c, &c->d_counters, 4)) || (rc = dalloc(c, &c->d_residual, 4)) ||
@@ -649,6 +661,7 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     rc = use64(c) ? upload_state<double>(c, c->d, inc_off, inc_tet, inc_local, ground_of)
                   : upload_state<float>(c, c->f, inc_off, inc_tet, inc_local, ground_of);
     if (rc) return rc;
+    trace("finalize: lbvh");
     if (!c->prims.empty()) {
         std::string err;
         if (int r2 = lbvh_allocate(c, err)) return fail(r2, err);

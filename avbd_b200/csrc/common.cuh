@@ -43,7 +43,7 @@ template <typename R> AVBD_HD V3<R> cross3(V3<R> a, V3<R> b) {
 template <typename V> AVBD_D auto xyz(const V& v) -> V3<decltype(v.x)> { return {v.x, v.y, v.z}; }
 
 template <typename R>
-AVBD_D typename Vec4Of<R>::T make4(V3<R> v, R w) {
+AVBD_HD typename Vec4Of<R>::T make4(V3<R> v, R w) {
     typename Vec4Of<R>::T r;
     r.x = v.x; r.y = v.y; r.z = v.z; r.w = w;
     return r;
