@@ -198,9 +198,9 @@ class Context:
         check(self.L.avbd_get_positions(self.h, 0, n, _dp(out)))
         return out
 
-    def velocities(self):
+    def velocities(self, out=None):
         n = self.num_particles
-        out = np.empty((n, 3))
+        out = np.empty((n, 3)) if out is None else out
         check(self.L.avbd_get_velocities(self.h, 0, n, _dp(out)))
         return out
 
@@ -246,6 +246,13 @@ class Context:
         r = C.c_double(0)
         check(self.L.avbd_residual(self.h, C.byref(r)))
         return r.value
+
+    def profile_solve(self, iterations=2):
+        """Kernel time (ms) and algorithmic bytes of the per-color solve launches
+        of `iterations` further iterations (advances the state)."""
+        ms, b, nl = C.c_double(0), C.c_double(0), C.c_uint(0)
+        check(self.L.avbd_profile_solve(self.h, iterations, C.byref(ms), C.byref(b), C.byref(nl)))
+        return ms.value, b.value, nl.value
 
     def stats(self):
         s = Stats()

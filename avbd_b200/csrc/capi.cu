@@ -438,6 +438,20 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
         begin[i + 1] = begin[i] + (solved ? inc_off[e + 1] - inc_off[e] : 0);
     }
     const size_t nrec = begin[n];
+    // algorithmic bytes of each color's solve launch
+    c->color_bytes.assign(c->num_colors, 0.0);
+    {
+        const double V4B = sizeof(V4), RECB = sizeof(IncRec<R>);
+        const double ground_b = c->ground.empty() ? 0.0 : 3 * V4B + 1;
+        for (unsigned col = 0; col < c->num_colors; col++) {
+            double b = 0;
+            for (unsigned i = c->color_begin[col]; i < c->color_begin[col] + c->color_solve[col]; i++) {
+                b += 3 * V4B + 2 * sizeof(uint32_t) + 1 + RECB * (begin[i + 1] - begin[i]);
+                if (flags[i] & VF_GROUND) b += ground_b;
+            }
+            c->color_bytes[col] = b;
+        }
+    }
     std::vector<IncRec<R>> rec(nrec);
     {
         unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
@@ -971,6 +985,47 @@ int avbd_debug_block(avbd_ctx* c, unsigned p, double* G, double* H, int* dof) {
     for (int i = 0; i < 9; i++) H[i] = h[3 + i];
     if (dof) *dof = 3;
     return AVBD_OK;
+}
+
+int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, double* solve_bytes,
+                       unsigned* launches) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    StepConsts k = consts(c);
+    const unsigned nc = c->num_colors;
+    std::vector<cudaEvent_t> ev(2ull * nc * iterations);
+    for (auto& e : ev) CUDA_OR_FAIL(cudaEventCreate(&e));
+    double bytes = 0;
+    unsigned nl = 0;
+    double omega = 1;
+    for (unsigned it = 0; it < iterations; it++) {
+        omega = omega_at(it, c->solver.iter_acceleration, omega);
+        for (unsigned col = 0; col < nc; col++) {
+            cudaEvent_t a = ev[2ull * (it * nc + col)], b = ev[2ull * (it * nc + col) + 1];
+            CUDA_OR_FAIL(cudaEventRecord(a, c->stream));
+            if (c->color_solve[col]) {
+                if (use64(c)) launch_solve_color<double>(c, c->d, k, c->color_begin[col], c->color_solve[col], c->stream);
+                else launch_solve_color<float>(c, c->f, k, c->color_begin[col], c->color_solve[col], c->stream);
+                bytes += c->color_bytes[col];
+                nl++;
+            }
+            CUDA_OR_FAIL(cudaEventRecord(b, c->stream));
+        }
+        if (use64(c)) launch_chebyshev_dual<double>(c, c->d, k, omega, c->stream);
+        else launch_chebyshev_dual<float>(c, c->f, k, omega, c->stream);
+    }
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    double ms = 0;
+    for (size_t i = 0; i < ev.size(); i += 2) {
+        float t = 0;
+        CUDA_OR_FAIL(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+        ms += t;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (solve_ms) *solve_ms = ms;
+    if (solve_bytes) *solve_bytes = bytes;
+    if (launches) *launches = nl;
+    return device_error(c);
 }
 
 int avbd_residual(avbd_ctx* c, double* residual) {

@@ -145,6 +145,7 @@ struct avbd_ctx {
     std::vector<unsigned> inv;          // external -> internal
     std::vector<unsigned> color_begin;  // internal offset of each color slab
     std::vector<unsigned> color_solve;  // vertices of the slab that run the 3-DOF solve
+    std::vector<double> color_bytes;    // algorithmic bytes of each color's solve launch
     unsigned max_color_solve = 0;
 
     avbd::DevState<float> f;

@@ -96,12 +96,14 @@ def tet_setup(X: np.ndarray, tets: np.ndarray, E, nu, density):
     """Q, rest volume and lumped masses of TetMeshObject::setup
     (simobject/TetMeshObject.cpp:62-97)."""
     v1, v2, v3, v4 = (X[tets[:, k]] for k in range(4))
-    Xm = np.stack([v1 - v4, v2 - v4, v3 - v4], axis=2)  # columns
-    Q = np.linalg.inv(Xm)
-    V = np.abs(np.linalg.det(Xm) / 6.0)
+    a, b, c = v1 - v4, v2 - v4, v3 - v4  # columns of X
+    # X^-1 rows are the cross products of the columns over det X
+    r0, r1, r2 = np.cross(b, c), np.cross(c, a), np.cross(a, b)
+    det = np.einsum("ij,ij->i", a, r0)
+    Q = np.stack([r0, r1, r2], axis=1) / det[:, None, None]
+    V = np.abs(det / 6.0)
     lam, mu = lame(E, nu)
-    masses = np.zeros(len(X))
-    np.add.at(masses, tets.ravel(), np.repeat(0.25 * V * density, 4))
+    masses = np.bincount(tets.ravel(), weights=np.repeat(0.25 * V * density, 4), minlength=len(X))
     return Q, V, lam, mu, masses
 
 
@@ -189,25 +191,36 @@ def cube_drop(n: int = 32, seed: int = 0, iters: int = 20, rho: float = 0.5, dt:
     return sc
 
 
+def batched_cube_params(seed: int, s: int, n_min: int = 4, n_max: int = 24):
+    """Parameters of scene s of a batch: drawn from a generator seeded by
+    (seed, s), so any subset of a batch is reproduced exactly."""
+    rng = np.random.default_rng([seed, s])
+    n = int(rng.integers(n_min, n_max + 1))
+    E = float(10 ** rng.uniform(4, 7))
+    nu = float(rng.uniform(0.3, 0.49))
+    R = random_rotation(rng)
+    return n, E, nu, R
+
+
 def batched_cubes(num_scenes: int = 1024, seed: int = 0, n_min: int = 4, n_max: int = 24, iters: int = 15,
-                  rho: float = 0.5, dt: float = 1.0 / 60.0, spacing: float = 2.0) -> Scene:
+                  rho: float = 0.5, dt: float = 1.0 / 60.0, spacing: float = 2.0, scene_ids=None) -> Scene:
     """Many independent cubes of uneven size advanced together: cell counts
     n ~ U{n_min..n_max} per side (6 n^3 tets), E log-uniform in [1e4, 1e7],
     nu ~ U(0.3, 0.49), random initial rotation, per-vertex ground contact,
-    15 iterations per step.  Each cube is its own scene (own coloring)."""
-    rng = np.random.default_rng(seed)
+    15 iterations per step.  Each cube is its own scene (own coloring).
+    scene_ids selects a subset of the batch (same cubes, same placement)."""
+    ids = list(range(num_scenes)) if scene_ids is None else list(scene_ids)
     sc = Scene(name=f"batch{num_scenes}", dt=dt, solver_iters=iters, iter_acceleration=rho)
     side = int(np.ceil(np.sqrt(num_scenes)))
-    ns = rng.integers(n_min, n_max + 1, size=num_scenes)
-    Es = 10 ** rng.uniform(4, 7, size=num_scenes)
-    nus = rng.uniform(0.3, 0.49, size=num_scenes)
-    for s in range(num_scenes):
-        if s > 0:
+    cells = []
+    for k, s in enumerate(ids):
+        if k > 0:
             sc.record("begin_scene")
-        R = random_rotation(rng)
+        n, E, nu, R = batched_cube_params(seed, s, n_min, n_max)
+        cells.append(n)
         ox, oz = (s % side) * spacing, (s // side) * spacing
-        add_tet_cube(sc, int(ns[s]), size=1.0, origin=(ox, 0.0, oz), E=float(Es[s]), nu=float(nus[s]),
-                     density=1000.0, rotation=R, ground=True, bottom_at=0.3)
-    sc.num_scenes = num_scenes
-    sc.meta["cells"] = ns.tolist()
+        add_tet_cube(sc, n, size=1.0, origin=(ox, 0.0, oz), E=E, nu=nu, density=1000.0, rotation=R, ground=True,
+                     bottom_at=0.3)
+    sc.num_scenes = len(ids)
+    sc.meta["cells"] = cells
     return sc

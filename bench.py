@@ -1,0 +1,279 @@
+#!/usr/bin/env python
+"""Benchmark: batched AVBD steps to residual 1e-4 on B200.
+
+Workload (default): 1024 independent NeoHookean cubes of uneven size
+(n ~ U{4..24} cells per side, 6 n^3 tets, E log-uniform 1e4..1e7,
+nu ~ U(0.3, 0.49), random rotation, ground contact), all advanced together;
+every step runs AVBD iterations until the residual R <= 1e-4 (at most
+--max-iters).  One step of the batch counts as `scenes` scene-steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line.  `value` is scene-steps/s over all ranks with the state
+resident in HBM; `e2e` repeats the measurement through the C-ABI with the
+state uploaded from pinned host memory and the positions read back every
+step; `roofline` reports the per-color vertex-solve kernel against the
+measured HBM bandwidth; `cpu_baseline` times the FP64 oracle port on the
+host cores on a sample of the same batch.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/s to residual 1e-4: learned+batched vs plain AVBD, same B200"
+UNIT = "scene-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--scenes", type=int, default=1024)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--tol", type=float, default=1e-4)
+    p.add_argument("--max-iters", type=int, default=100)
+    p.add_argument("--cpu-sample-scenes", type=int, default=2)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def traffic_for(workload: str):
+    """Per-launch DRAM bytes of the solve kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "solve_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+def cpu_sample(args, seed, threads):
+    """FP64 oracle port on the first S scenes of the same batch: scene-steps/s."""
+    from avbd_b200 import scenes
+    from oracle.oracle import Oracle
+    S = args.cpu_sample_scenes
+    sc = scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=range(S))
+    o = Oracle(threads=threads)
+    sc.load(o, residual_tolerance=args.tol, max_iters=args.max_iters)
+    o.finalize()
+    o.step(1)  # warm-up (first contact step)
+    steps, t = 0, 0.0
+    while t < args.cpu_seconds and steps < 200:
+        t += o.time_steps(1)
+        steps += 1
+    return S * steps / t, S, steps, t
+
+
+def run_reference(args):
+    from avbd_b200 import dist
+    rank, world, _ = dist.env()
+    if rank != 0:
+        return
+    threads = min(os.cpu_count() or 1, 32)
+    from avbd_b200 import scenes
+    from oracle.oracle import Oracle
+    S = args.cpu_sample_scenes
+    sc = scenes.batched_cubes(num_scenes=args.scenes, seed=args.seed, scene_ids=range(S))
+    o = Oracle(threads=threads)
+    sc.load(o, residual_tolerance=args.tol, max_iters=args.max_iters)
+    o.finalize()
+    for _ in range(args.warmup):
+        o.step(1)
+    t = o.time_steps(args.steps)
+    v = S * args.steps / t
+    sample = f"{S} of {args.scenes} scenes of the batch, {args.steps} steps, FP64 oracle port, {threads} threads"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"batch{args.scenes}_cubes", "scenes_timed": S,
+                       "residual_tolerance": args.tol, "max_iters": args.max_iters},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args):
+    import numpy as np
+    import torch
+
+    from avbd_b200 import Context, dist, scenes
+
+    rank, world, local = dist.env()
+    torch.cuda.set_device(local)
+    dist.init("nccl")
+    seed = dist.shard_seed(args.seed, rank)
+
+    t0 = time.time()
+    sc = scenes.batched_cubes(num_scenes=args.scenes, seed=seed)
+    e = Context(device=local)
+    stream = torch.cuda.Stream(device=local)
+    e.set_stream(stream.cuda_stream)
+    sc.load(e, residual_tolerance=args.tol, max_iters=args.max_iters)
+    e.finalize()
+    setup_s = time.time() - t0
+    n = sc.num_particles
+
+    # warm-up
+    e.step(args.warmup)
+    e.synchronize()
+
+    # ---- device-resident timing
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    st0 = e.stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    e.step(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    st1 = e.stats()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = st1["kernel_launches"] - st0["kernel_launches"]
+    iters = (st1["iterations"] - st0["iterations"]) / args.steps
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    x_host = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    v_host = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    x_host[:] = e.positions()
+    v_host[:] = e.velocities()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e.set_state(x_host, v_host)
+        e.step(1)
+        e.positions(out=x_host)
+        e.velocities(out=v_host)
+    e1.record(stream)
+    e1.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    dist.barrier()
+
+    # ---- per-kernel roofline of the vertex solve
+    solve_ms, solve_bytes, solve_launches = e.profile_solve(2)
+    e.synchronize()
+
+    ms_max, ms_e2e_max = dist.reduce([ms, ms_e2e], "max", device=torch.device("cuda", local))
+    value = args.scenes * world * args.steps / (ms_max / 1e3)
+    value_e2e = args.scenes * world * args.steps / (ms_e2e_max / 1e3)
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        per_launch_ms = solve_ms / max(1, solve_launches)
+        per_launch_bytes = solve_bytes / max(1, solve_launches)
+        achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
+        workload = f"batch{args.scenes}_cubes"
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic_for(workload), "kernel": "k_solve_tet (per-color vertex block solve)",
+                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "peak_source": peak_kind}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = min(os.cpu_count() or 1, 32)
+            v_cpu, S, steps, t = cpu_sample(args, seed, threads)
+            cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{S} of {args.scenes} scenes of the same batch, {steps} steps in {t:.1f} s, "
+                             f"FP64 oracle port"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "scenes_per_gpu": args.scenes, "vertices_per_gpu": n,
+                       "tets_per_gpu": sc.num_tets, "residual_tolerance": args.tol, "max_iters": args.max_iters,
+                       "iterations_per_step": iters, "method": "plain AVBD (no warm start)",
+                       "l2": f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration",
+                       "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
+            "clocks": clk, "gpu_launches": launches,
+            "e2e": {"value": value_e2e, "unit": UNIT, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n},
+            "roofline": roof, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    e.close()
+    dist.shutdown()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

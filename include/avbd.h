@@ -256,6 +256,16 @@ AVBD_API int avbd_debug_block(avbd_ctx* ctx, unsigned p, double* G, double* H, i
  * sqrt(sum_v |m g|^2)), FP64 reduction on the device. */
 AVBD_API int avbd_residual(avbd_ctx* ctx, double* residual);
 
+/* Measurement entry point (no counterpart in the reference): runs `iterations`
+ * further solver iterations on the current state without the CUDA graph,
+ * bracketing every per-color vertex-solve launch with CUDA events on the
+ * context's stream.  Returns the summed kernel time, the algorithmic bytes
+ * those launches had to move (per solved vertex: x read + y read + x write,
+ * its two incidence offsets and flags, contact state when present, and one
+ * incidence record per incident tet) and the number of launches. */
+AVBD_API int avbd_profile_solve(avbd_ctx* ctx, unsigned iterations, double* solve_ms, double* solve_bytes,
+                                unsigned* launches);
+
 AVBD_API const char* avbd_last_error_string(void);
 AVBD_API const char* avbd_version(void);
 
