@@ -20,6 +20,7 @@ ERRORS = {
 }
 PRECISION_FP32 = 0
 PRECISION_FP64 = 1
+PRECISION_MIXED = 2
 SHAPE_TRIANGLE, SHAPE_ROD_SEGMENT, SHAPE_SPHERE = 0, 1, 2
 
 

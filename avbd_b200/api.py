@@ -62,7 +62,8 @@ class Context:
         check(self.L.avbd_set_params(self.h, C.byref(self._params)))
 
     def set_solver(self, solver_iters, iter_acceleration, residual_tolerance=0.0, max_iters=0, precision=None):
-        prec = self._solver.precision if precision is None else (1 if precision in (1, "fp64") else 0)
+        codes = {"fp32": 0, "fp64": 1, "mixed": 2, 0: 0, 1: 1, 2: 2}
+        prec = self._solver.precision if precision is None else codes[precision]
         self._solver = SolverParams(int(solver_iters), float(iter_acceleration), float(residual_tolerance),
                                     int(max_iters), prec)
         check(self.L.avbd_set_solver(self.h, C.byref(self._solver)))

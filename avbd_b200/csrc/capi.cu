@@ -15,6 +15,7 @@
 #include <cstring>
 #include <numeric>
 #include <thread>
+#include <type_traits>
 
 #include "engine.h"
 
@@ -44,7 +45,8 @@ namespace avbd {
 void count_launch(avbd_ctx* c, unsigned k) { c->stats.kernel_launches += k; }
 }
 
-static bool use64(const avbd_ctx* c) { return c->solver.precision == AVBD_PRECISION_FP64; }
+// FP64 and mixed keep the particle state in double precision.
+static bool use64(const avbd_ctx* c) { return c->solver.precision != AVBD_PRECISION_FP32; }
 
 template <typename T>
 static int dalloc(avbd_ctx* c, T** p, size_t count) {
@@ -148,7 +150,8 @@ int avbd_set_params(avbd_ctx* c, const avbd_params* p) {
 int avbd_set_solver(avbd_ctx* c, const avbd_solver_params* s) {
     if (int r = check_ctx(c)) return r;
     if (!s) return fail(AVBD_ERR_INVALID_ARG, "null solver params");
-    if (s->precision != AVBD_PRECISION_FP32 && s->precision != AVBD_PRECISION_FP64)
+    if (s->precision != AVBD_PRECISION_FP32 && s->precision != AVBD_PRECISION_FP64 &&
+        s->precision != AVBD_PRECISION_MIXED)
         return fail(AVBD_ERR_INVALID_ARG, "unknown precision");
     if (c->finalized && s->precision != c->solver.precision) free_device(c);
     c->solver = *s;
@@ -408,7 +411,7 @@ void build_neighbors(avbd_ctx* c, const std::vector<unsigned>& inc_off, const st
     }
 }
 
-template <typename R>
+template <typename R, typename RS>
 int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_off,
                  const std::vector<uint32_t>& inc_tet, const std::vector<uint16_t>& inc_local,
                  const std::vector<int>& ground_of) {
@@ -441,7 +444,7 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
     // algorithmic bytes of each color's solve launch
     c->color_bytes.assign(c->num_colors, 0.0);
     {
-        const double V4B = sizeof(V4), RECB = sizeof(IncRec<R>);
+        const double V4B = sizeof(V4), RECB = sizeof(IncRec<RS>);
         const double ground_b = c->ground.empty() ? 0.0 : 3 * V4B + 1;
         for (unsigned col = 0; col < c->num_colors; col++) {
             double b = 0;
@@ -452,7 +455,7 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
             c->color_bytes[col] = b;
         }
     }
-    std::vector<IncRec<R>> rec(nrec);
+    std::vector<IncRec<RS>> rec(nrec);
     {
         unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
         if (n < 20000) nt = 1;
@@ -472,20 +475,20 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
                         D[2][j] = h.Q[2 * 3 + j];
                         D[3][j] = -(h.Q[j] + h.Q[3 + j] + h.Q[6 + j]);
                     }
-                    IncRec<R>& r = rec[w];
+                    IncRec<RS>& r = rec[w];
                     int o = 0;
                     for (int j = 0; j < 4; j++) {
                         if ((unsigned)j == loc) continue;
                         r.o[o] = c->inv[h.idx[j]];
-                        r.d[3 * o] = (R)D[j][0];
-                        r.d[3 * o + 1] = (R)D[j][1];
-                        r.d[3 * o + 2] = (R)D[j][2];
+                        r.d[3 * o] = (RS)D[j][0];
+                        r.d[3 * o + 1] = (RS)D[j][1];
+                        r.d[3 * o + 2] = (RS)D[j][2];
                         o++;
                     }
                     r.tet = inc_tet[k];
-                    r.vlam = (R)(h.V * h.lambda);
-                    r.vmu = (R)(h.V * h.mu);
-                    r.shift = (R)(h.mu / h.lambda + 1.0);
+                    r.vlam = (RS)(h.V * h.lambda);
+                    r.vmu = (RS)(h.V * h.mu);
+                    r.mol = (RS)(h.mu / h.lambda);
                 }
             }
         };
@@ -499,9 +502,12 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
     int rc;
     if ((rc = dalloc(c, &s.x, n)) || (rc = dalloc(c, &s.y, n)) || (rc = dalloc(c, &s.xp, n)) ||
         (rc = dalloc(c, &s.xl, n)) || (rc = dalloc(c, &s.xll, n)) || (rc = dalloc(c, &s.v, n)) ||
-        (rc = dalloc(c, &s.vp, n)) || (rc = dalloc(c, &s.flags, n)) || (rc = dalloc(c, &s.inc, nrec)) ||
-        (rc = dalloc(c, &s.inc_begin, n + 1)))
+        (rc = dalloc(c, &s.vp, n)) || (rc = dalloc(c, &s.flags, n)) || (rc = dalloc(c, &s.inc_begin, n + 1)))
         return rc;
+    IncRec<RS>* d_rec = nullptr;
+    if ((rc = dalloc(c, &d_rec, nrec))) return rc;
+    if constexpr (std::is_same<R, RS>::value) s.inc = d_rec;
+    else s.inc32 = d_rec;
     cudaStream_t st = c->stream;
     CUDA_OR_FAIL(cudaMemcpyAsync(s.x, x.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
     CUDA_OR_FAIL(cudaMemcpyAsync(s.y, y.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
@@ -511,7 +517,7 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
     CUDA_OR_FAIL(cudaMemcpyAsync(s.v, v.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
     CUDA_OR_FAIL(cudaMemcpyAsync(s.vp, vp.data(), sizeof(V4) * n, cudaMemcpyHostToDevice, st));
     CUDA_OR_FAIL(cudaMemcpyAsync(s.flags, flags.data(), n, cudaMemcpyHostToDevice, st));
-    if (nrec) CUDA_OR_FAIL(cudaMemcpyAsync(s.inc, rec.data(), sizeof(IncRec<R>) * nrec, cudaMemcpyHostToDevice, st));
+    if (nrec) CUDA_OR_FAIL(cudaMemcpyAsync(d_rec, rec.data(), sizeof(IncRec<RS>) * nrec, cudaMemcpyHostToDevice, st));
     CUDA_OR_FAIL(cudaMemcpyAsync(s.inc_begin, begin.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));
 
     // ground contact, one record per particle (internal order)
@@ -672,8 +678,12 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     CUDA_OR_FAIL(cudaMemsetAsync(c->d_error, 0, sizeof(int), c->stream));
     CUDA_OR_FAIL(cudaMemcpyAsync(c->d_perm, c->perm.data(), sizeof(unsigned) * n, cudaMemcpyHostToDevice, c->stream));
     CUDA_OR_FAIL(cudaMemcpyAsync(c->d_inv, c->inv.data(), sizeof(unsigned) * n, cudaMemcpyHostToDevice, c->stream));
-    rc = use64(c) ? upload_state<double>(c, c->d, inc_off, inc_tet, inc_local, ground_of)
-                  : upload_state<float>(c, c->f, inc_off, inc_tet, inc_local, ground_of);
+    if (c->solver.precision == AVBD_PRECISION_MIXED)
+        rc = upload_state<double, float>(c, c->d, inc_off, inc_tet, inc_local, ground_of);
+    else if (use64(c))
+        rc = upload_state<double, double>(c, c->d, inc_off, inc_tet, inc_local, ground_of);
+    else
+        rc = upload_state<float, float>(c, c->f, inc_off, inc_tet, inc_local, ground_of);
     if (rc) return rc;
     trace("finalize: lbvh");
     if (!c->prims.empty()) {

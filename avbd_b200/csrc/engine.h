@@ -27,13 +27,13 @@ template <> struct alignas(16) IncRec<float> {
     uint32_t o[3];
     uint32_t tet;
     float d[9];
-    float vlam, vmu, shift;  // V*lambda, V*mu, mu/lambda + 1
+    float vlam, vmu, mol;  // V*lambda, V*mu, mu/lambda
 };
 template <> struct alignas(16) IncRec<double> {
     uint32_t o[3];
     uint32_t tet;
     double d[9];
-    double vlam, vmu, shift;
+    double vlam, vmu, mol;
 };
 static_assert(sizeof(IncRec<float>) == 64, "FP32 incidence record must be 64 B");
 static_assert(sizeof(IncRec<double>) == 112, "FP64 incidence record must be 112 B");
@@ -50,6 +50,7 @@ struct DevState {
     V4 *x = nullptr, *y = nullptr, *xp = nullptr, *xl = nullptr, *xll = nullptr, *v = nullptr, *vp = nullptr;
     uint8_t* flags = nullptr;
     IncRec<R>* inc = nullptr;
+    IncRec<float>* inc32 = nullptr;   // FP32 records of the mixed mode (double state)
     uint32_t* inc_begin = nullptr;
     // per-tet data (damping path only)
     unsigned ntets = 0;

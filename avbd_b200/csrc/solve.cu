@@ -126,7 +126,7 @@ AVBD_D IncRec<float> load_rec<float>(const IncRec<float>* p) {
     r.tet = __float_as_uint(a.w);
     r.d[0] = b.x; r.d[1] = b.y; r.d[2] = b.z; r.d[3] = b.w;
     r.d[4] = c.x; r.d[5] = c.y; r.d[6] = c.z; r.d[7] = c.w;
-    r.d[8] = d.x; r.vlam = d.y; r.vmu = d.z; r.shift = d.w;
+    r.d[8] = d.x; r.vlam = d.y; r.vmu = d.z; r.mol = d.w;
     return r;
 }
 template <>
@@ -141,82 +141,90 @@ AVBD_D IncRec<double> load_rec<double>(const IncRec<double>* p) {
     v = __ldcs(q + 3); r.d[4] = v.x; r.d[5] = v.y;
     v = __ldcs(q + 4); r.d[6] = v.x; r.d[7] = v.y;
     v = __ldcs(q + 5); r.d[8] = v.x; r.vlam = v.y;
-    v = __ldcs(q + 6); r.vmu = v.x; r.shift = v.y;
+    v = __ldcs(q + 6); r.vmu = v.x; r.mol = v.y;
     return r;
 }
 
-template <typename R>
+// Accumulated block: gradient in the state precision P, Hessian in HT.  The
+// Hessian only shapes the Newton step, never the converged state, so the
+// mixed mode keeps it in FP32 while the gradient (which the residual
+// measures) is formed in FP64.
+template <typename P, typename HT>
 struct Block3 {
-    R g0 = 0, g1 = 0, g2 = 0;
-    R h00 = 0, h11 = 0, h22 = 0, h01 = 0, h02 = 0, h12 = 0;
+    P g0 = 0, g1 = 0, g2 = 0;
+    HT h00 = 0, h11 = 0, h22 = 0, h01 = 0, h02 = 0, h12 = 0;
 };
 
 // One NeoHookean incidence: NeoHookeanEnergySolver::accumulate with the tet
-// restated relative to the solved vertex (see IncRec).
-template <typename R, bool DAMP>
-AVBD_D void accumulate_tet(const DevState<R>& s, const IncRec<R>& r, V3<R> xi, R dt, Block3<R>& B) {
-    V3<R> e1 = xyz(ld_ro(s.x + r.o[0])) - xi;
-    V3<R> e2 = xyz(ld_ro(s.x + r.o[1])) - xi;
-    V3<R> e3 = xyz(ld_ro(s.x + r.o[2])) - xi;
-    V3<R> d1 = mk3(r.d[0], r.d[1], r.d[2]);
-    V3<R> d2 = mk3(r.d[3], r.d[4], r.d[5]);
-    V3<R> d3 = mk3(r.d[6], r.d[7], r.d[8]);
-    V3<R> dw = mk3(-(d1.x + d2.x + d3.x), -(d1.y + d2.y + d3.y), -(d1.z + d2.z + d3.z));
+// restated relative to the solved vertex (see IncRec).  P is the precision of
+// positions and gradient, RS the stored record scalar, HT the Hessian type.
+template <typename P, typename RS, typename HT, bool DAMP>
+AVBD_D void accumulate_tet(const DevState<P>& s, const IncRec<RS>& r, V3<P> xi, P dt, Block3<P, HT>& B) {
+    V3<P> e1 = xyz(ld_ro(s.x + r.o[0])) - xi;
+    V3<P> e2 = xyz(ld_ro(s.x + r.o[1])) - xi;
+    V3<P> e3 = xyz(ld_ro(s.x + r.o[2])) - xi;
+    V3<P> d1 = mk3<P>(r.d[0], r.d[1], r.d[2]);
+    V3<P> d2 = mk3<P>(r.d[3], r.d[4], r.d[5]);
+    V3<P> d3 = mk3<P>(r.d[6], r.d[7], r.d[8]);
+    V3<P> dw = mk3<P>(-(d1.x + d2.x + d3.x), -(d1.y + d2.y + d3.y), -(d1.z + d2.z + d3.z));
     // columns of F
-    V3<R> F0 = d1.x * e1 + d2.x * e2 + d3.x * e3;
-    V3<R> F1 = d1.y * e1 + d2.y * e2 + d3.y * e3;
-    V3<R> F2 = d1.z * e1 + d2.z * e2 + d3.z * e3;
-    V3<R> c0 = cross3(F1, F2), c1 = cross3(F2, F0), c2 = cross3(F0, F1);
-    R J = dot3(F0, c0);
-    V3<R> Fc = dw.x * c0 + dw.y * c1 + dw.z * c2;   // cof(F) d
-    V3<R> Fd = dw.x * F0 + dw.y * F1 + dw.z * F2;   // F d
-    R hyd = r.vlam * (J - r.shift);
-    R dev = r.vmu;
-    R qn2 = dot3(dw, dw);
+    V3<P> F0 = d1.x * e1 + d2.x * e2 + d3.x * e3;
+    V3<P> F1 = d1.y * e1 + d2.y * e2 + d3.y * e3;
+    V3<P> F2 = d1.z * e1 + d2.z * e2 + d3.z * e3;
+    V3<P> c0 = cross3(F1, F2), c1 = cross3(F2, F0), c2 = cross3(F0, F1);
+    P J = dot3(F0, c0);
+    V3<P> Fc = dw.x * c0 + dw.y * c1 + dw.z * c2;   // cof(F) d
+    V3<P> Fd = dw.x * F0 + dw.y * F1 + dw.z * F2;   // F d
+    P hyd = (P)r.vlam * ((J - P(1)) - (P)r.mol);     // V lambda (J - mu/lambda - 1)
+    P dev = (P)r.vmu;
+    P qn2 = dot3(dw, dw);
     B.g0 += hyd * Fc.x + dev * Fd.x;
     B.g1 += hyd * Fc.y + dev * Fd.y;
     B.g2 += hyd * Fc.z + dev * Fd.z;
-    R dg = dev * qn2;
-    B.h00 += r.vlam * Fc.x * Fc.x + dg;
-    B.h11 += r.vlam * Fc.y * Fc.y + dg;
-    B.h22 += r.vlam * Fc.z * Fc.z + dg;
-    B.h01 += r.vlam * Fc.x * Fc.y;
-    B.h02 += r.vlam * Fc.x * Fc.z;
-    B.h12 += r.vlam * Fc.y * Fc.z;
+    const HT vl = (HT)r.vlam, fx = (HT)Fc.x, fy = (HT)Fc.y, fz = (HT)Fc.z;
+    const HT dg = (HT)(dev * qn2);
+    B.h00 += vl * fx * fx + dg;
+    B.h11 += vl * fy * fy + dg;
+    B.h22 += vl * fz * fz + dg;
+    B.h01 += vl * fx * fy;
+    B.h02 += vl * fx * fz;
+    B.h12 += vl * fy * fz;
     if constexpr (DAMP) {
-        typename Vec4Of<R>::T e0 = s.tet_e[2 * r.tet], e1v = s.tet_e[2 * r.tet + 1];
-        R vkd = e1v.z;
-        if (vkd != R(0)) {
-            R idt = R(1) / dt;
+        typename Vec4Of<P>::T e0 = s.tet_e[2 * r.tet], e1v = s.tet_e[2 * r.tet + 1];
+        P vkd = e1v.z;
+        if (vkd != P(0)) {
+            P idt = P(1) / dt;
             // Edot = (1/2 (F^T F - I) - E_prev) / dt
-            R E00 = (R(0.5) * (dot3(F0, F0) - R(1)) - e0.x) * idt;
-            R E11 = (R(0.5) * (dot3(F1, F1) - R(1)) - e0.y) * idt;
-            R E22 = (R(0.5) * (dot3(F2, F2) - R(1)) - e0.z) * idt;
-            R E01 = (R(0.5) * dot3(F0, F1) - e0.w) * idt;
-            R E02 = (R(0.5) * dot3(F0, F2) - e1v.x) * idt;
-            R E12 = (R(0.5) * dot3(F1, F2) - e1v.y) * idt;
-            V3<R> Ed = mk3(E00 * dw.x + E01 * dw.y + E02 * dw.z, E01 * dw.x + E11 * dw.y + E12 * dw.z,
-                           E02 * dw.x + E12 * dw.y + E22 * dw.z);
-            R damp = R(2) * idt * vkd;
-            V3<R> FEd = Ed.x * F0 + Ed.y * F1 + Ed.z * F2;
+            P E00 = (P(0.5) * (dot3(F0, F0) - P(1)) - e0.x) * idt;
+            P E11 = (P(0.5) * (dot3(F1, F1) - P(1)) - e0.y) * idt;
+            P E22 = (P(0.5) * (dot3(F2, F2) - P(1)) - e0.z) * idt;
+            P E01 = (P(0.5) * dot3(F0, F1) - e0.w) * idt;
+            P E02 = (P(0.5) * dot3(F0, F2) - e1v.x) * idt;
+            P E12 = (P(0.5) * dot3(F1, F2) - e1v.y) * idt;
+            V3<P> Ed = mk3<P>(E00 * dw.x + E01 * dw.y + E02 * dw.z, E01 * dw.x + E11 * dw.y + E12 * dw.z,
+                              E02 * dw.x + E12 * dw.y + E22 * dw.z);
+            P damp = P(2) * idt * vkd;
+            V3<P> FEd = Ed.x * F0 + Ed.y * F1 + Ed.z * F2;
             B.g0 += damp * FEd.x;
             B.g1 += damp * FEd.y;
             B.g2 += damp * FEd.z;
-            R diag = damp * dot3(dw, Ed);
-            R al = R(0.5) * damp * idt;
+            HT diag = (HT)(damp * dot3(dw, Ed));
+            HT al = (HT)(P(0.5) * damp * idt);
+            HT q2 = (HT)qn2;
             // F F^T = sum_c F_c F_c^T
-            R f00 = F0.x * F0.x + F1.x * F1.x + F2.x * F2.x;
-            R f11 = F0.y * F0.y + F1.y * F1.y + F2.y * F2.y;
-            R f22 = F0.z * F0.z + F1.z * F1.z + F2.z * F2.z;
-            R f01 = F0.x * F0.y + F1.x * F1.y + F2.x * F2.y;
-            R f02 = F0.x * F0.z + F1.x * F1.z + F2.x * F2.z;
-            R f12 = F0.y * F0.z + F1.y * F1.z + F2.y * F2.z;
-            B.h00 += diag + al * (f00 * qn2 + Fd.x * Fd.x);
-            B.h11 += diag + al * (f11 * qn2 + Fd.y * Fd.y);
-            B.h22 += diag + al * (f22 * qn2 + Fd.z * Fd.z);
-            B.h01 += al * (f01 * qn2 + Fd.x * Fd.y);
-            B.h02 += al * (f02 * qn2 + Fd.x * Fd.z);
-            B.h12 += al * (f12 * qn2 + Fd.y * Fd.z);
+            HT f00 = (HT)(F0.x * F0.x + F1.x * F1.x + F2.x * F2.x);
+            HT f11 = (HT)(F0.y * F0.y + F1.y * F1.y + F2.y * F2.y);
+            HT f22 = (HT)(F0.z * F0.z + F1.z * F1.z + F2.z * F2.z);
+            HT f01 = (HT)(F0.x * F0.y + F1.x * F1.y + F2.x * F2.y);
+            HT f02 = (HT)(F0.x * F0.z + F1.x * F1.z + F2.x * F2.z);
+            HT f12 = (HT)(F0.y * F0.z + F1.y * F1.z + F2.y * F2.z);
+            HT dx = (HT)Fd.x, dy = (HT)Fd.y, dz = (HT)Fd.z;
+            B.h00 += diag + al * (f00 * q2 + dx * dx);
+            B.h11 += diag + al * (f11 * q2 + dy * dy);
+            B.h22 += diag + al * (f22 * q2 + dz * dz);
+            B.h01 += al * (f01 * q2 + dx * dy);
+            B.h02 += al * (f02 * q2 + dx * dz);
+            B.h12 += al * (f12 * q2 + dy * dz);
         }
     }
 }
@@ -224,33 +232,33 @@ AVBD_D void accumulate_tet(const DevState<R>& s, const IncRec<R>& r, V3<R> xi, R
 // Ground contact term of the block (CollisionConstraintEnergySolver::accumulate<3>
 // with GroundCollisionConstraintSolver): the Hessian k grad C grad C^T is always
 // added, the gradient is gated by the clamped multipliers.
-template <typename R>
-AVBD_D void accumulate_ground(const DevState<R>& s, unsigned p, V3<R> xi, Block3<R>& B) {
-    typename Vec4Of<R>::T k = s.gk[p], lam = s.glam[p], cp = s.gcp[p];
+template <typename P, typename HT>
+AVBD_D void accumulate_ground(const DevState<P>& s, unsigned p, V3<P> xi, Block3<P, HT>& B) {
+    typename Vec4Of<P>::T k = s.gk[p], lam = s.glam[p], cp = s.gcp[p];
     uint8_t gf = s.gflag[p];
-    R Cn = -xi.y, Ct = xi.x - cp.x, Cb = xi.z - cp.y;
-    R cc = Cn - R(AVBD_ALPHA) * lam.w;
-    R ln = k.x * cc + lam.x;
-    R lnp = ln > R(0) ? ln : R(0);
-    R lt = k.y * Ct + lam.y, lb = k.z * Cb + lam.z;
-    R mag = sqrt(lt * lt + lb * lb);
-    R mu = (gf & GF_USE_STATIC) ? cp.z : cp.w;
-    R mx = mu * lnp;
+    P Cn = -xi.y, Ct = xi.x - cp.x, Cb = xi.z - cp.y;
+    P cc = Cn - P(AVBD_ALPHA) * lam.w;
+    P ln = k.x * cc + lam.x;
+    P lnp = ln > P(0) ? ln : P(0);
+    P lt = k.y * Ct + lam.y, lb = k.z * Cb + lam.z;
+    P mag = sqrt(lt * lt + lb * lb);
+    P mu = (gf & GF_USE_STATIC) ? cp.z : cp.w;
+    P mx = mu * lnp;
     if (mag > mx) {
-        R sc = mx / (mag + R(1e-8));
+        P sc = mx / (mag + P(1e-8));
         lt = lt * sc;
         lb = lb * sc;
     }
     B.g0 += lt;
     B.g1 += -lnp;
     B.g2 += lb;
-    B.h00 += k.y;
-    B.h11 += k.x;
-    B.h22 += k.z;
+    B.h00 += (HT)k.y;
+    B.h11 += (HT)k.x;
+    B.h22 += (HT)k.z;
 }
 
-template <typename R, int LANES>
-AVBD_D void reduce_block(Block3<R>& B) {
+template <int LANES, typename P, typename HT>
+AVBD_D void reduce_block(Block3<P, HT>& B) {
 #pragma unroll
     for (int m = LANES / 2; m >= 1; m >>= 1) {
         B.g0 += shfl_xor(B.g0, m);
@@ -272,8 +280,9 @@ enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2 };
 // reduction and the 3x3 solve by the group's first lane.  MODE_RESIDUAL
 // evaluates |m/h^2 (x-y) + grad| instead of updating; MODE_DEBUG exports the
 // accumulated block.
-template <typename R, int LANES, bool DAMP, bool GROUND, int MODE>
-__global__ void __launch_bounds__(256) k_solve_tet(DevState<R> s, unsigned begin, unsigned count, Consts<R> c,
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE>
+__global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
+                                                   unsigned begin, unsigned count, Consts<P> c,
                                                    unsigned long long* counters, double* out) {
     unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned gi = tid / LANES;
@@ -282,17 +291,17 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<R> s, unsigned begin
     unsigned p = begin + (active ? gi : 0);
     uint8_t fl = active ? s.flags[p] : 0;
     if (MODE != MODE_SOLVE && (fl & (VF_FIXED | VF_ORIENTED))) active = false;
-    Block3<R> B;
-    V3<R> xi = mk3<R>(0, 0, 0);
+    Block3<P, HT> B;
+    V3<P> xi = mk3<P>(0, 0, 0);
     if (active) {
         xi = xyz(s.x[p]);
         unsigned b = s.inc_begin[p], e = s.inc_begin[p + 1];
         for (unsigned k = b + lane; k < e; k += LANES) {
-            IncRec<R> r = load_rec<R>(s.inc + k);
-            accumulate_tet<R, DAMP>(s, r, xi, c.dt, B);
+            IncRec<RS> r = load_rec<RS>(inc + k);
+            accumulate_tet<P, RS, HT, DAMP>(s, r, xi, c.dt, B);
         }
     }
-    reduce_block<R, LANES>(B);
+    reduce_block<LANES>(B);
     if (!active || lane != 0) {
         if constexpr (MODE == MODE_RESIDUAL) {
             // keep the warp reduction below well defined
@@ -302,26 +311,26 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<R> s, unsigned begin
     }
     double r2 = 0.0, mg2 = 0.0;
     if (active && lane == 0) {
-        if (GROUND && (fl & VF_GROUND)) accumulate_ground<R>(s, p, xi, B);
-        typename Vec4Of<R>::T y4 = s.y[p];
-        R m = y4.w;
-        R cm = m * c.inv_dt2;
-        V3<R> d = xi - xyz(y4);
+        if (GROUND && (fl & VF_GROUND)) accumulate_ground<P, HT>(s, p, xi, B);
+        typename Vec4Of<P>::T y4 = s.y[p];
+        P m = y4.w;
+        P cm = m * c.inv_dt2;
+        V3<P> d = xi - xyz(y4);
         if constexpr (MODE == MODE_SOLVE) {
-            Sym3<R> A{cm + B.h00, cm + B.h11, cm + B.h22, B.h01, B.h02, B.h12};
-            V3<R> rhs = mk3(-cm * d.x - B.g0, -cm * d.y - B.g1, -cm * d.z - B.g2);
-            V3<R> dx;
-            R kappa = solve_sym3<R>(A, rhs, dx);
+            Sym3<P> A{cm + (P)B.h00, cm + (P)B.h11, cm + (P)B.h22, (P)B.h01, (P)B.h02, (P)B.h12};
+            V3<P> rhs = mk3<P>(-cm * d.x - B.g0, -cm * d.y - B.g1, -cm * d.z - B.g2);
+            V3<P> dx;
+            P kappa = solve_sym3<P>(A, rhs, dx);
             if (!(kappa <= c.kappa_max)) {
                 double M[3][3] = {{(double)A.a00, (double)A.a01, (double)A.a02},
                                   {(double)A.a01, (double)A.a11, (double)A.a12},
                                   {(double)A.a02, (double)A.a12, (double)A.a22}};
                 double bb[3] = {(double)rhs.x, (double)rhs.y, (double)rhs.z}, xx[3];
                 lu_solve_d<3>(M, bb, xx);
-                dx = mk3<R>((R)xx[0], (R)xx[1], (R)xx[2]);
+                dx = mk3<P>((P)xx[0], (P)xx[1], (P)xx[2]);
                 atomicAdd(counters, 1ull);
             }
-            typename Vec4Of<R>::T o = make4<R>(xi + dx, R(0));
+            typename Vec4Of<P>::T o = make4<P>(xi + dx, P(0));
             s.x[p] = o;
         } else if constexpr (MODE == MODE_RESIDUAL) {
             double u0 = (double)cm * (double)d.x + (double)B.g0;
@@ -472,40 +481,56 @@ void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStre
     count_launch(c);
 }
 
-template <typename R, int LANES, int MODE>
-static void solve_dispatch(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                           cudaStream_t st, double* out) {
+template <typename P, typename RS, typename HT, int LANES, int MODE>
+static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
+                           unsigned count, cudaStream_t st, double* out) {
     unsigned threads = count * LANES;
     unsigned blocks = nblocks(threads, 256);
     if (blocks == 0) return;
     bool damp = c->damping, ground = !c->ground.empty();
-    auto kc = mkc<R>(k);
+    auto kc = mkc<P>(k);
     if (damp && ground)
-        k_solve_tet<R, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
     else if (damp)
-        k_solve_tet<R, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
     else if (ground)
-        k_solve_tet<R, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
     else
-        k_solve_tet<R, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
     count_launch(c);
 }
 
-template <typename R, int MODE>
-static void solve_lanes(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out) {
+template <typename P, typename RS, typename HT, int MODE>
+static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
+                          unsigned count, cudaStream_t st, double* out) {
     switch (c->lanes) {
-        case 4: solve_dispatch<R, 4, MODE>(c, s, k, begin, count, st, out); break;
-        case 16: solve_dispatch<R, 16, MODE>(c, s, k, begin, count, st, out); break;
-        case 32: solve_dispatch<R, 32, MODE>(c, s, k, begin, count, st, out); break;
-        default: solve_dispatch<R, 8, MODE>(c, s, k, begin, count, st, out); break;
+        case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, begin, count, st, out); break;
+        case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, begin, count, st, out); break;
+        case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, begin, count, st, out); break;
+        default: solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out); break;
     }
+}
+
+// FP32: everything in float.  FP64: everything in double.  Mixed: double
+// state and gradient, float records and Hessian.
+template <int MODE>
+static void solve_lanes(avbd_ctx* c, DevState<float>& s, const StepConsts& k, unsigned begin, unsigned count,
+                        cudaStream_t st, double* out) {
+    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out);
+}
+template <int MODE>
+static void solve_lanes(avbd_ctx* c, DevState<double>& s, const StepConsts& k, unsigned begin, unsigned count,
+                        cudaStream_t st, double* out) {
+    if (c->solver.precision == AVBD_PRECISION_MIXED)
+        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out);
+    else
+        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out);
 }
 
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
                         cudaStream_t st) {
-    solve_lanes<R, MODE_SOLVE>(c, s, k, begin, count, st, nullptr);
+    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr);
 }
 
 template <typename R>
@@ -524,12 +549,12 @@ void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStrea
 template <typename R>
 void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st) {
     cudaMemsetAsync(out2, 0, 2 * sizeof(double), st);
-    solve_lanes<R, MODE_RESIDUAL>(c, s, k, 0, s.n, st, out2);
+    solve_lanes<MODE_RESIDUAL>(c, s, k, 0, s.n, st, out2);
 }
 
 template <typename R>
 void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st) {
-    solve_lanes<R, MODE_DEBUG>(c, s, k, p, 1, st, out);
+    solve_lanes<MODE_DEBUG>(c, s, k, p, 1, st, out);
 }
 
 template <typename R>

@@ -32,6 +32,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "steps/s to residual 1e-4: learned+batched vs plain AVBD, same B200"
 UNIT = "scene-steps/s"
+DTYPES = {"fp32": "f32", "fp64": "f64", "mixed": "f64 state+gradient / f32 element records+Hessian"}
 
 
 def parse():
@@ -47,6 +48,7 @@ def parse():
     p.add_argument("--cpu-sample-scenes", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
     return p.parse_args()
 
 
@@ -178,7 +180,7 @@ def run_engine(args):
     e = Context(device=local)
     stream = torch.cuda.Stream(device=local)
     e.set_stream(stream.cuda_stream)
-    sc.load(e, residual_tolerance=args.tol, max_iters=args.max_iters)
+    sc.load(e, residual_tolerance=args.tol, max_iters=args.max_iters, precision=args.precision)
     e.finalize()
     setup_s = time.time() - t0
     n = sc.num_particles
@@ -252,10 +254,11 @@ def run_engine(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
             "config": {"workload": workload, "scenes_per_gpu": args.scenes, "vertices_per_gpu": n,
                        "tets_per_gpu": sc.num_tets, "residual_tolerance": args.tol, "max_iters": args.max_iters,
                        "iterations_per_step": iters, "method": "plain AVBD (no warm start)",
+                       "precision": args.precision,
                        "l2": f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration",
                        "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
             "clocks": clk, "gpu_launches": launches,

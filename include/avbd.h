@@ -57,11 +57,18 @@ extern "C" {
 #define AVBD_SHAPE_ROD_SEGMENT  1
 #define AVBD_SHAPE_SPHERE       2
 
-/* Arithmetic of the solve.  FP32 is the production path (FP32 accumulation,
- * FP64 block inverse on ill-conditioned blocks, FP64 residual reduction);
- * FP64 runs every kernel in double precision and is the parity/debug path. */
+/* Arithmetic of the solve.
+ *  FP32:  FP32 state, element records, accumulation and updates; FP64 block
+ *         inverse on ill-conditioned blocks; FP64 residual reduction.  Its
+ *         residual floor grows with stiffness (FP32 position quantisation and
+ *         gradient cancellation), so it suits fixed-iteration stepping.
+ *  FP64:  every kernel in double precision (parity/debug path).
+ *  MIXED: FP64 state and gradient, FP32 element records and Hessian: the same
+ *         HBM record traffic as FP32 with an FP64-accurate residual; the mode
+ *         for run-to-tolerance stepping of stiff scenes. */
 #define AVBD_PRECISION_FP32 0
 #define AVBD_PRECISION_FP64 1
+#define AVBD_PRECISION_MIXED 2
 
 typedef struct avbd_ctx avbd_ctx;
 

@@ -161,6 +161,33 @@ def test_run_to_tolerance(oracle_lib):
     assert rel_err(e, o, sc) < 1e-7
 
 
+@pytest.mark.parametrize("n", [4, 8])
+def test_mixed_precision_tracks_oracle(oracle_lib, n):
+    """Mixed mode (FP64 state and gradient, FP32 records and Hessian): the FP32
+    rounding of the element data perturbs the model by ~1e-7 relative."""
+    sc = scenes.cube_fixed_bottom(n)
+    e, o = pair(sc, oracle_lib, "mixed")
+    e.step(50)
+    o.step(50)
+    assert rel_err(e, o, sc) < 1e-6
+
+
+def test_mixed_run_to_tolerance_on_stiff_batch(oracle_lib):
+    """Stiff scenes reach R <= 1e-4 in the mixed mode with about the oracle's
+    iteration count, while FP32 stalls on its rounding floor."""
+    sc = scenes.batched_cubes(num_scenes=4, seed=5, n_min=5, n_max=8)
+    e, o = pair(sc, oracle_lib, "mixed", residual_tolerance=1e-4, max_iters=300)
+    e.step(4)
+    o.step(4)
+    it0e, it0o = e.stats()["iterations"], o.iterations
+    e.step(3)
+    o.step(3)
+    ie = e.stats()["iterations"] - it0e
+    io = o.iterations - it0o
+    assert e.stats()["last_residual"] <= 1e-4
+    assert abs(ie - io) <= max(2, 0.2 * io), (ie, io)
+
+
 def test_stats_and_no_fallback_on_c1(oracle_lib):
     sc = scenes.cube_fixed_bottom(8)
     e, _ = pair(sc, oracle_lib, "fp32")
