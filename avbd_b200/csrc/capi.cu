@@ -75,6 +75,14 @@ static void free_device(avbd_ctx* c) {
     c->d_perm = nullptr;
     c->d_inv = nullptr;
     c->d_error = nullptr;
+    c->d_scene = nullptr;
+    c->d_scene_active = nullptr;
+    c->d_scene_cand = nullptr;
+    c->d_scene_r2 = nullptr;
+    c->d_scene_ex = nullptr;
+    c->d_scene_mg2 = nullptr;
+    c->d_scene_iters = nullptr;
+    c->d_tol_count = nullptr;
     c->finalized = false;
     c->graph_dirty = true;
 }
@@ -685,6 +693,26 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     else
         rc = upload_state<float, float>(c, c->f, inc_off, inc_tet, inc_local, ground_of);
     if (rc) return rc;
+    // per-scene run-to-tolerance state
+    {
+        const unsigned S = (unsigned)sb.size() - 1;
+        c->num_scenes = S;
+        std::vector<uint32_t> sid(n);
+        for (unsigned i = 0; i < n; i++) sid[i] = scene_of[c->perm[i]];
+        std::vector<double> mg2(S, 0.0);
+        for (unsigned e = 0; e < n; e++)
+            if (!c->fixed[e]) {
+                mg2[scene_of[e]] += c->mass[e] * c->mass[e];  // sum of m^2; g^2 is applied per step
+            }
+        if ((rc = dalloc(c, &c->d_scene, n)) || (rc = dalloc(c, &c->d_scene_active, S)) ||
+            (rc = dalloc(c, &c->d_scene_cand, S)) || (rc = dalloc(c, &c->d_scene_r2, S)) ||
+            (rc = dalloc(c, &c->d_scene_ex, S)) || (rc = dalloc(c, &c->d_scene_mg2, S)) ||
+            (rc = dalloc(c, &c->d_scene_iters, S)) || (rc = dalloc(c, &c->d_tol_count, 1)))
+            return rc;
+        CUDA_OR_FAIL(cudaMemcpyAsync(c->d_scene, sid.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+        CUDA_OR_FAIL(cudaMemcpyAsync(c->d_scene_mg2, mg2.data(), sizeof(double) * S, cudaMemcpyHostToDevice, c->stream));
+        CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    }
     trace("finalize: lbvh");
     if (!c->prims.empty()) {
         std::string err;
@@ -735,29 +763,40 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
     StepConsts k = consts(c);
     cudaStream_t st = c->stream;
     if (c->solver.residual_tolerance > 0) {
-        // run-to-tolerance: the residual is checked on the host after every sweep
-        unsigned max_it = c->solver.max_iters ? c->solver.max_iters : 1000;
+        // Run-to-tolerance, scene by scene: a scene iterates until its own
+        // residual R_s <= tol (or max_iters), exactly as it would alone in a
+        // context.  The in-sweep residual the solve accumulates for free marks
+        // candidate scenes; only those pay for the exact post-iteration
+        // residual that decides the stop.  Converged scenes are skipped by the
+        // solve, Chebyshev and dual kernels.  One host read per iteration (the
+        // count of scenes still iterating) ends the loop.
+        const unsigned max_it = c->solver.max_iters ? c->solver.max_iters : 1000;
+        const double tol = c->solver.residual_tolerance;
+        SceneTol solveT{c->d_scene, c->d_scene_active, nullptr, c->d_scene_r2, nullptr};
+        SceneTol resT{c->d_scene, nullptr, c->d_scene_cand, nullptr, c->d_scene_ex};
         for (unsigned t = 0; t < n_steps; t++) {
             if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
             if (c->damping) launch_tet_eprev<R>(c, s, k, st);
             launch_begin_step<R>(c, s, k, st);
+            launch_tol_init(c, st);
             double omega = 1;
-            unsigned it = 0;
-            for (; it < max_it;) {
+            for (unsigned it = 0; it < max_it; it++) {
                 omega = omega_at(it, c->solver.iter_acceleration, omega);
-                enqueue_iteration<R>(c, s, k, omega, st);
-                it++;
-                launch_residual<R>(c, s, k, c->d_residual, st);
-                double h[2];
-                CUDA_OR_FAIL(cudaMemcpyAsync(h, c->d_residual, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+                for (unsigned col = 0; col < c->num_colors; col++)
+                    if (c->color_solve[col])
+                        launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st, solveT);
+                launch_chebyshev_dual<R>(c, s, k, omega, st, solveT);
+                launch_tol_decide_a(c, tol, st);
+                launch_residual<R>(c, s, k, nullptr, st, resT);
+                launch_tol_decide_b(c, tol, max_it, st);
+                int n_active = 0;
+                CUDA_OR_FAIL(cudaMemcpyAsync(&n_active, c->d_tol_count, sizeof(int), cudaMemcpyDeviceToHost, st));
                 CUDA_OR_FAIL(cudaStreamSynchronize(st));
-                double R2 = h[1] > 0 ? std::sqrt(h[0]) / std::sqrt(h[1]) : std::sqrt(h[0]);
-                c->stats.last_residual = R2;
-                if (R2 <= c->solver.residual_tolerance) break;
+                if (n_active == 0) break;
             }
-            c->stats.iterations += it;
             launch_velocity<R>(c, s, k, st);
         }
+        CUDA_OR_FAIL(cudaGetLastError());
         return AVBD_OK;
     }
     bool capturable = c->use_graph && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
@@ -786,7 +825,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         } else {
             enqueue_step_fixed<R>(c, s, k, st);
         }
-        c->stats.iterations += c->solver.solver_iters;
+        c->host_iterations += (unsigned long long)c->solver.solver_iters * c->num_scenes;
     }
     CUDA_OR_FAIL(cudaGetLastError());
     return AVBD_OK;
@@ -844,6 +883,15 @@ int avbd_get_stats(avbd_ctx* c, avbd_stats* out) {
         }
         CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
         c->stats.fp64_fallbacks = h[0];
+        c->stats.iterations = c->host_iterations + h[1];
+        if (c->solver.residual_tolerance > 0 && h[2]) {
+            // largest confirmed per-scene residual of the last step (order-preserving encoding)
+            unsigned long long u = h[2];
+            u = (u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u;
+            double r;
+            std::memcpy(&r, &u, sizeof(r));
+            c->stats.last_residual = r;
+        }
     }
     *out = c->stats;
     return AVBD_OK;

@@ -65,6 +65,16 @@ struct DevState {
     int* err = nullptr;    // device-side status (AVBD_ERR_*), 0 when healthy
 };
 
+// Per-scene run-to-tolerance state passed to the solve, Chebyshev and residual
+// kernels.  Null pointers disable the corresponding behaviour.
+struct SceneTol {
+    const uint32_t* scene = nullptr;  // scene of each internal vertex
+    const uint8_t* active = nullptr;  // solve / update only vertices of these scenes
+    const uint8_t* cand = nullptr;    // exact residual only for these scenes
+    double* r2 = nullptr;             // per-scene sum of in-sweep block residuals^2
+    double* ex = nullptr;             // per-scene sum of exact block residuals^2
+};
+
 // Scalar arguments of a step.
 struct StepConsts {
     double dt;
@@ -160,6 +170,17 @@ struct avbd_ctx {
     uint32_t* d_inv = nullptr;          // external -> internal
     int* d_error = nullptr;             // device-side status
     unsigned long long launches_per_step = 0;
+    // per-scene run-to-tolerance state (num_scenes entries, scene ids per vertex)
+    unsigned num_scenes = 1;
+    uint32_t* d_scene = nullptr;
+    uint8_t* d_scene_active = nullptr;
+    uint8_t* d_scene_cand = nullptr;
+    double* d_scene_r2 = nullptr;
+    double* d_scene_ex = nullptr;
+    double* d_scene_mg2 = nullptr;
+    uint32_t* d_scene_iters = nullptr;
+    int* d_tol_count = nullptr;
+    unsigned long long host_iterations = 0;  // scene-iterations of fixed-iteration steps
 
     // CUDA graph of one full step (fixed-iteration mode)
     cudaGraphExec_t graph = nullptr;
@@ -181,13 +202,19 @@ template <typename R>
 void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st);
+                        cudaStream_t st, const SceneTol& T = SceneTol());
 template <typename R>
-void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st);
+void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+                           const SceneTol& T = SceneTol());
 template <typename R>
 void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
 template <typename R>
-void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st);
+void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st,
+                     const SceneTol& T = SceneTol());
+// per-scene tolerance bookkeeping kernels
+void launch_tol_init(avbd_ctx* c, cudaStream_t st);
+void launch_tol_decide_a(avbd_ctx* c, double tol, cudaStream_t st);
+void launch_tol_decide_b(avbd_ctx* c, double tol, unsigned max_it, cudaStream_t st);
 template <typename R>
 void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st);
 template <typename R>

@@ -283,7 +283,7 @@ enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2 };
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE>
 __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
-                                                   unsigned long long* counters, double* out) {
+                                                   unsigned long long* counters, double* out, SceneTol T) {
     unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned gi = tid / LANES;
     unsigned lane = tid % LANES;
@@ -291,6 +291,9 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
     unsigned p = begin + (active ? gi : 0);
     uint8_t fl = active ? s.flags[p] : 0;
     if (MODE != MODE_SOLVE && (fl & (VF_FIXED | VF_ORIENTED))) active = false;
+    // per-scene run-to-tolerance: converged scenes are skipped before any record is read
+    if (MODE == MODE_SOLVE && T.active && active && !T.active[T.scene[p]]) active = false;
+    if (MODE == MODE_RESIDUAL && T.cand && active && !T.cand[T.scene[p]]) active = false;
     Block3<P, HT> B;
     V3<P> xi = mk3<P>(0, 0, 0);
     if (active) {
@@ -319,6 +322,11 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
         if constexpr (MODE == MODE_SOLVE) {
             Sym3<P> A{cm + (P)B.h00, cm + (P)B.h11, cm + (P)B.h22, (P)B.h01, (P)B.h02, (P)B.h12};
             V3<P> rhs = mk3<P>(-cm * d.x - B.g0, -cm * d.y - B.g1, -cm * d.z - B.g2);
+            if (T.r2) {  // in-sweep residual: the block RHS just before this vertex's update
+                double q = (double)rhs.x * (double)rhs.x + (double)rhs.y * (double)rhs.y +
+                           (double)rhs.z * (double)rhs.z;
+                atomicAdd(T.r2 + T.scene[p], q);
+            }
             V3<P> dx;
             P kappa = solve_sym3<P>(A, rhs, dx);
             if (!(kappa <= c.kappa_max)) {
@@ -347,6 +355,10 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
         }
     }
     if constexpr (MODE == MODE_RESIDUAL) {
+        if (T.ex) {  // per-scene sums
+            if (active && lane == 0) atomicAdd(T.ex + T.scene[p], r2);
+            return;
+        }
         // FP64 reduction: warp, then one atomic per warp
 #pragma unroll
         for (int m = 16; m >= 1; m >>= 1) {
@@ -364,11 +376,12 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
 // update that follows it (CollisionConstraintEnergySolver::updateAfterIteration);
 // a ground energy reads only its own particle, so the fusion is exact.
 template <typename R>
-__global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega) {
+__global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega, SceneTol T) {
     unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= s.n) return;
     uint8_t fl = s.flags[p];
     if (fl & VF_ORIENTED) return;
+    if (T.active && !T.active[T.scene[p]]) return;
     typename Vec4Of<R>::T x4 = s.x[p], l4 = s.xl[p], ll4 = s.xll[p];
     V3<R> x = xyz(x4), ll = xyz(ll4);
     V3<R> xn = omega * (x - ll) + ll;
@@ -483,31 +496,37 @@ void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStre
 
 template <typename P, typename RS, typename HT, int LANES, int MODE>
 static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
-                           unsigned count, cudaStream_t st, double* out) {
+                           unsigned count, cudaStream_t st, double* out, const SceneTol& T) {
     unsigned threads = count * LANES;
     unsigned blocks = nblocks(threads, 256);
     if (blocks == 0) return;
     bool damp = c->damping, ground = !c->ground.empty();
     auto kc = mkc<P>(k);
+    auto* ctr = c->d_counters;
     if (damp && ground)
-        k_solve_tet<P, RS, HT, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
     else if (damp)
-        k_solve_tet<P, RS, HT, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
     else if (ground)
-        k_solve_tet<P, RS, HT, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
     else
-        k_solve_tet<P, RS, HT, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, c->d_counters, out);
+        k_solve_tet<P, RS, HT, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
     count_launch(c);
 }
 
+// The solve runs with the context's lane count; residual and debug passes use 8.
 template <typename P, typename RS, typename HT, int MODE>
 static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
-                          unsigned count, cudaStream_t st, double* out) {
-    switch (c->lanes) {
-        case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, begin, count, st, out); break;
-        case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, begin, count, st, out); break;
-        case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, begin, count, st, out); break;
-        default: solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out); break;
+                          unsigned count, cudaStream_t st, double* out, const SceneTol& T) {
+    if constexpr (MODE != MODE_SOLVE) {
+        solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T);
+    } else {
+        switch (c->lanes) {
+            case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, begin, count, st, out, T); break;
+            case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, begin, count, st, out, T); break;
+            case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, begin, count, st, out, T); break;
+            default: solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T); break;
+        }
     }
 }
 
@@ -515,28 +534,29 @@ static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, co
 // state and gradient, float records and Hessian.
 template <int MODE>
 static void solve_lanes(avbd_ctx* c, DevState<float>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out) {
-    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out);
+                        cudaStream_t st, double* out, const SceneTol& T) {
+    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out, T);
 }
 template <int MODE>
 static void solve_lanes(avbd_ctx* c, DevState<double>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out) {
+                        cudaStream_t st, double* out, const SceneTol& T) {
     if (c->solver.precision == AVBD_PRECISION_MIXED)
-        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out);
+        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out, T);
     else
-        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out);
+        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out, T);
 }
 
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st) {
-    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr);
+                        cudaStream_t st, const SceneTol& T) {
+    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr, T);
 }
 
 template <typename R>
-void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st) {
+void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+                           const SceneTol& T) {
     (void)k;
-    k_chebyshev_dual<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)omega);
+    k_chebyshev_dual<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)omega, T);
     count_launch(c);
 }
 
@@ -547,14 +567,95 @@ void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStrea
 }
 
 template <typename R>
-void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st) {
-    cudaMemsetAsync(out2, 0, 2 * sizeof(double), st);
-    solve_lanes<MODE_RESIDUAL>(c, s, k, 0, s.n, st, out2);
+void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st,
+                     const SceneTol& T) {
+    if (out2) cudaMemsetAsync(out2, 0, 2 * sizeof(double), st);
+    solve_lanes<MODE_RESIDUAL>(c, s, k, 0, s.n, st, out2, T);
+}
+
+// ------------------------------------------- per-scene run-to-tolerance
+__global__ void k_tol_init(uint8_t* active, uint8_t* cand, double* r2, double* ex, uint32_t* iters, unsigned S,
+                           unsigned long long* maxr) {
+    unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) *maxr = 0ull;
+    if (s >= S) return;
+    active[s] = 1;
+    cand[s] = 0;
+    r2[s] = 0;
+    ex[s] = 0;
+    iters[s] = 0;
+}
+
+AVBD_D double scene_R(double r2, double mg2) { return mg2 > 0 ? sqrt(r2) / sqrt(mg2) : sqrt(r2); }
+
+// After a sweep: every active scene counts the iteration and becomes a
+// candidate when its in-sweep residual is at the tolerance.
+__global__ void k_tol_decide_a(uint8_t* active, uint8_t* cand, double* r2, const double* m2, uint32_t* iters,
+                               unsigned S, double tol, double g2, unsigned long long* scene_iterations) {
+    unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    cand[s] = 0;
+    if (active[s]) {
+        iters[s]++;
+        atomicAdd(scene_iterations, 1ull);
+        cand[s] = scene_R(r2[s], m2[s] * g2) <= tol;
+    }
+    r2[s] = 0;
+}
+
+AVBD_D unsigned long long ord_enc64(double d) {
+    unsigned long long u = (unsigned long long)__double_as_longlong(d);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+// Candidates whose exact residual is at the tolerance stop; so does every
+// scene at the iteration cap.  Counts the scenes still iterating.
+__global__ void k_tol_decide_b(uint8_t* active, uint8_t* cand, double* ex, const double* m2, const uint32_t* iters,
+                               unsigned S, double tol, double g2, unsigned max_it, int* n_active,
+                               unsigned long long* maxr) {
+    unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    if (active[s]) {
+        if (cand[s]) {
+            double R = scene_R(ex[s], m2[s] * g2);
+            atomicMax(maxr, ord_enc64(R));
+            if (R <= tol) active[s] = 0;
+        }
+        if (iters[s] >= max_it) active[s] = 0;
+        if (active[s]) atomicAdd(n_active, 1);
+    }
+    cand[s] = 0;
+    ex[s] = 0;
+}
+
+void launch_tol_init(avbd_ctx* c, cudaStream_t st) {
+    unsigned S = c->num_scenes;
+    k_tol_init<<<nblocks(S, 256), 256, 0, st>>>(c->d_scene_active, c->d_scene_cand, c->d_scene_r2, c->d_scene_ex,
+                                                c->d_scene_iters, S, c->d_counters + 2);
+    count_launch(c);
+}
+
+void launch_tol_decide_a(avbd_ctx* c, double tol, cudaStream_t st) {
+    unsigned S = c->num_scenes;
+    k_tol_decide_a<<<nblocks(S, 256), 256, 0, st>>>(c->d_scene_active, c->d_scene_cand, c->d_scene_r2,
+                                                    c->d_scene_mg2, c->d_scene_iters, S, tol,
+                                                    c->params.g_accel * c->params.g_accel, c->d_counters + 1);
+    count_launch(c);
+}
+
+void launch_tol_decide_b(avbd_ctx* c, double tol, unsigned max_it, cudaStream_t st) {
+    unsigned S = c->num_scenes;
+    cudaMemsetAsync(c->d_tol_count, 0, sizeof(int), st);
+    k_tol_decide_b<<<nblocks(S, 256), 256, 0, st>>>(c->d_scene_active, c->d_scene_cand, c->d_scene_ex,
+                                                    c->d_scene_mg2, c->d_scene_iters, S, tol,
+                                                    c->params.g_accel * c->params.g_accel, max_it, c->d_tol_count,
+                                                    c->d_counters + 2);
+    count_launch(c);
 }
 
 template <typename R>
 void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st) {
-    solve_lanes<MODE_DEBUG>(c, s, k, p, 1, st, out);
+    solve_lanes<MODE_DEBUG>(c, s, k, p, 1, st, out, SceneTol());
 }
 
 template <typename R>
@@ -575,10 +676,12 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
     template void launch_begin_step<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);               \
     template void launch_tet_eprev<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                \
     template void launch_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,         \
-                                        cudaStream_t);                                                          \
-    template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t);   \
+                                        cudaStream_t, const SceneTol&);                                         \
+    template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t,    \
+                                           const SceneTol&);                                                    \
     template void launch_velocity<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                 \
-    template void launch_residual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double*, cudaStream_t);        \
+    template void launch_residual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double*, cudaStream_t,         \
+                                     const SceneTol&);                                                          \
     template void launch_debug_block<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, double*,          \
                                         cudaStream_t);                                                          \
     template void launch_load_positions<R>(DevState<R>&, const double*, const uint32_t*, unsigned, unsigned, int, \

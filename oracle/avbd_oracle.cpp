@@ -326,6 +326,12 @@ struct Ctx {
     std::vector<V3> w, wp, I;
     std::vector<unsigned> scene_of;         // scene index of each particle
     unsigned num_scenes = 1;
+    // run-to-tolerance bookkeeping: every scene iterates until its own residual
+    // reaches the tolerance, as it would in a context of its own
+    std::vector<double> sweep_r2;           // in-sweep block residual of each particle
+    std::vector<uint8_t> scene_active;
+    std::vector<double> scene_mg2;
+    std::vector<unsigned> scene_iters;      // iterations of the last step, per scene
 
     // energy pools
     std::vector<NH> nh;
@@ -726,6 +732,7 @@ static void accumulate_block(const Ctx& c, unsigned p, double H[DOF][DOF], doubl
 // VBDSolver::_solveParticle<DOF> assembly and solve (simulation/VBDSolver.hpp:449-510)
 static void solve_particle(Ctx& c, unsigned p) {
     if (c.fixed[p]) return;
+    if (!c.scene_active.empty() && !c.scene_active[c.scene_of[p]]) return;
     double dt = c.dt;
     if (c.oriented(p)) {
         double H[6][6], G[6];
@@ -738,6 +745,11 @@ static void solve_particle(Ctx& c, unsigned p) {
         double rhs[6];
         for (int i = 0; i < 3; i++) { rhs[i] = a[i] - G[i]; rhs[3 + i] = -1 / (dt * dt) * (Iv[i] * ms[i]) - G[3 + i]; }
         for (int i = 0; i < 3; i++) { H[i][i] += mass / (dt * dt); H[3 + i][3 + i] += Iv[i] / (dt * dt); }
+        if (!c.sweep_r2.empty()) {
+            double s = 0;
+            for (int i = 0; i < 6; i++) s += rhs[i] * rhs[i];
+            c.sweep_r2[p] = s;
+        }
         double dx[6];
         lu_solve<6>(H, rhs, dx);
         c.x[p] += V3(dx[0], dx[1], dx[2]);
@@ -750,6 +762,7 @@ static void solve_particle(Ctx& c, unsigned p) {
         double rhs[3];
         for (int i = 0; i < 3; i++) rhs[i] = -mass / (dt * dt) * d[i] - G[i];
         for (int i = 0; i < 3; i++) H[i][i] += mass / (dt * dt);
+        if (!c.sweep_r2.empty()) c.sweep_r2[p] = rhs[0] * rhs[0] + rhs[1] * rhs[1] + rhs[2] * rhs[2];
         double dx[3];
         lu_solve<3>(H, rhs, dx);
         c.x[p] += V3(dx[0], dx[1], dx[2]);
@@ -886,18 +899,25 @@ static void after_time_step(Ctx& c) {
     for (auto& e : c.joints) joint_after_step(c, e, c.joint_k_start);
 }
 
+static inline bool scene_on(const Ctx& c, unsigned p) {
+    return c.scene_active.empty() || c.scene_active[c.scene_of[p]];
+}
+
 static void after_iteration(Ctx& c) {
     c.pool.parallel_for(0, (long)c.ground.size(), [&](long i) {
+        if (!scene_on(c, c.ground[i].p)) return;
         double Cn, Ct, Cb;
         ground_eval(c, c.ground[i], Cn, Ct, Cb);
         contact_after_iter(c.ground[i], Cn, Ct, Cb);
     });
     for (auto& e : c.rground) {
+        if (!scene_on(c, e.p)) continue;
         double Cn, Ct, Cb;
         rground_eval(c, e, Cn, Ct, Cb);
         contact_after_iter(e, Cn, Ct, Cb);
     }
-    for (auto& e : c.joints) joint_after_iter(c, e);
+    for (auto& e : c.joints)
+        if (scene_on(c, e.p)) joint_after_iter(c, e);
 }
 
 static void collision_stage(Ctx& c);
@@ -911,24 +931,70 @@ static void time_step(Ctx& c) {
     long n = (long)c.np();
     c.pool.parallel_for(0, n, [&](long p) { inertial(c, (unsigned)p); });
     double omega = 1;
-    unsigned max_it = c.tol > 0 ? c.max_iters : c.iters;
+    const bool tol_mode = c.tol > 0;
+    unsigned max_it = tol_mode ? c.max_iters : c.iters;
+    const unsigned S = c.num_scenes;
+    if (tol_mode) {
+        // Each scene iterates until its own residual R_s <= tol (or max_iters).
+        // The in-sweep residual (every block's RHS just before its update) is
+        // the trigger; the exact post-iteration residual confirms the stop.
+        c.scene_active.assign(S, 1);
+        c.scene_iters.assign(S, 0);
+        c.sweep_r2.assign(c.np(), 0.0);
+        c.scene_mg2.assign(S, 0.0);
+        for (unsigned p = 0; p < c.np(); p++)
+            if (!c.fixed[p]) c.scene_mg2[c.scene_of[p]] += (c.m[p] * c.g) * (c.m[p] * c.g);
+    }
     unsigned it = 0;
     for (; it < max_it; it++) {
         if (it > 2) omega = 4 / (4 - c.rho * c.rho * omega);
         else if (it == 2) omega = 2 / (2 - c.rho * c.rho);
         else omega = 1;
+        if (tol_mode) {
+            bool any = false;
+            for (unsigned s = 0; s < S; s++) any |= c.scene_active[s] != 0;
+            if (!any) break;
+        }
         for (unsigned col = 0; col < c.num_colors; col++) {
             c.pool.parallel_for(c.color_offsets[col], c.color_offsets[col + 1],
                                 [&](long k) { solve_particle(c, c.work_list[k]); });
         }
-        c.pool.parallel_for(0, n, [&](long p) { chebyshev(c, (unsigned)p, omega); });
+        c.pool.parallel_for(0, n, [&](long p) {
+            if (scene_on(c, (unsigned)p)) chebyshev(c, (unsigned)p, omega);
+        });
         after_iteration(c);
-        if (c.tol > 0) {
-            c.last_residual = residual(c);
-            if (c.last_residual <= c.tol) { it++; break; }
+        if (tol_mode) {
+            std::vector<double> r2(S, 0.0), ex(S, 0.0);
+            for (unsigned p = 0; p < c.np(); p++)
+                if (!c.fixed[p] && c.scene_active[c.scene_of[p]]) r2[c.scene_of[p]] += c.sweep_r2[p];
+            std::vector<uint8_t> cand(S, 0);
+            for (unsigned s = 0; s < S; s++) {
+                if (!c.scene_active[s]) continue;
+                c.scene_iters[s]++;
+                double R = c.scene_mg2[s] > 0 ? std::sqrt(r2[s]) / std::sqrt(c.scene_mg2[s]) : std::sqrt(r2[s]);
+                cand[s] = R <= c.tol;
+            }
+            for (unsigned p = 0; p < c.np(); p++)
+                if (!c.fixed[p] && cand[c.scene_of[p]]) ex[c.scene_of[p]] += block_residual_sq(c, p);
+            c.last_residual = 0;
+            for (unsigned s = 0; s < S; s++) {
+                if (!c.scene_active[s]) continue;
+                if (cand[s]) {
+                    double R = c.scene_mg2[s] > 0 ? std::sqrt(ex[s]) / std::sqrt(c.scene_mg2[s]) : std::sqrt(ex[s]);
+                    if (R <= c.tol) c.scene_active[s] = 0;
+                    c.last_residual = std::max(c.last_residual, R);
+                }
+                if (c.scene_iters[s] >= max_it) c.scene_active[s] = 0;
+            }
         }
     }
-    c.iterations += it;
+    if (tol_mode) {
+        for (unsigned s = 0; s < S; s++) c.iterations += c.scene_iters[s];
+        c.scene_active.clear();
+        c.sweep_r2.clear();
+    } else {
+        c.iterations += (unsigned long long)it * S;
+    }
     c.pool.parallel_for(0, n, [&](long p) { velocity(c, (unsigned)p); });
 }
 

@@ -188,6 +188,19 @@ def test_mixed_run_to_tolerance_on_stiff_batch(oracle_lib):
     assert abs(ie - io) <= max(2, 0.2 * io), (ie, io)
 
 
+def test_per_scene_tolerance_batch_fp64(oracle_lib):
+    """Every scene of a batch iterates to its own residual: the FP64 engine
+    spends the oracle's scene-iterations and ends in the oracle's state."""
+    sc = scenes.batched_cubes(num_scenes=6, seed=2, n_min=3, n_max=6)
+    e, o = pair(sc, oracle_lib, "fp64", residual_tolerance=1e-4, max_iters=200)
+    for _ in range(5):
+        e.step(1)
+        o.step(1)
+    st = e.stats()
+    assert abs(st["iterations"] - o.iterations) <= 2, (st["iterations"], o.iterations)
+    assert rel_err(e, o, sc) < 1e-7
+
+
 def test_stats_and_no_fallback_on_c1(oracle_lib):
     sc = scenes.cube_fixed_bottom(8)
     e, _ = pair(sc, oracle_lib, "fp32")
