@@ -582,6 +582,8 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
 
 }  // namespace
 
+static int autotune(avbd_ctx* c);
+
 extern "C" int avbd_finalize(avbd_ctx* c) {
     if (int r = check_ctx(c)) return r;
     CUDA_OR_FAIL(cudaSetDevice(c->device));
@@ -673,8 +675,18 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     for (unsigned e = 0; e < n; e++) {
         unsigned i = cur[3ull * c->color[e] + cls(e)]++;
         c->perm[i] = e;
-        c->inv[e] = i;
     }
+    // within a slab: scene by scene (locality of the neighbour gathers), and
+    // inside a scene by descending incidence count (threads of a warp then run
+    // loops of similar length)
+    for (unsigned k = 0; k < nc; k++) {
+        auto first = c->perm.begin() + c->color_begin[k];
+        std::stable_sort(first, first + c->color_solve[k], [&](unsigned a, unsigned b) {
+            if (scene_of[a] != scene_of[b]) return scene_of[a] < scene_of[b];
+            return inc_off[a + 1] - inc_off[a] > inc_off[b + 1] - inc_off[b];
+        });
+    }
+    for (unsigned i = 0; i < n; i++) c->inv[c->perm[i]] = i;
 
     trace("finalize: device buffers");
     // device buffers
@@ -720,6 +732,8 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     }
     c->stats.num_colors = nc;
     c->stats.num_scenes = (unsigned)sb.size() - 1;
+    trace("finalize: autotune");
+    if (int r3 = autotune(c)) return r3;
     c->finalized = true;
     c->graph_dirty = true;
     return AVBD_OK;
@@ -757,6 +771,62 @@ void enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaSt
 }
 
 StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_accel, c->kappa_max}; }
+
+// Picks the threads-per-vertex of the tet solve (1, 2, 4, 8, 16 or 32) by timing one
+// sweep of every color slab with each choice on the context's own data.
+// Positions are snapshotted and restored, so the state is untouched.
+// AVBD_LANES=<n> in the environment forces a choice.
+template <typename R>
+int autotune_impl(avbd_ctx* c, DevState<R>& s) {
+    const char* env = getenv("AVBD_LANES");
+    if (env) {
+        int l = atoi(env);
+        if (l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32) c->lanes = l;
+        return AVBD_OK;
+    }
+    unsigned long long solved = 0;
+    for (unsigned v : c->color_solve) solved += v;
+    c->lanes = 8;
+    if (solved < 50000) return AVBD_OK;
+    using V4 = typename Vec4Of<R>::T;
+    V4* snap = nullptr;
+    CUDA_OR_FAIL(cudaMalloc(&snap, sizeof(V4) * s.n));
+    cudaStream_t st = c->stream;
+    CUDA_OR_FAIL(cudaMemcpyAsync(snap, s.x, sizeof(V4) * s.n, cudaMemcpyDeviceToDevice, st));
+    StepConsts k = consts(c);
+    cudaEvent_t a, b;
+    CUDA_OR_FAIL(cudaEventCreate(&a));
+    CUDA_OR_FAIL(cudaEventCreate(&b));
+    const unsigned long long launches0 = c->stats.kernel_launches;
+    int best = 8;
+    float best_ms = 1e30f;
+    for (int l : {1, 2, 4, 8, 16}) {
+        c->lanes = l;
+        for (int rep = 0; rep < 2; rep++) {  // rep 0 warms up, rep 1 is timed
+            if (rep == 1) CUDA_OR_FAIL(cudaEventRecord(a, st));
+            for (unsigned col = 0; col < c->num_colors; col++)
+                if (c->color_solve[col]) launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st);
+            if (rep == 1) CUDA_OR_FAIL(cudaEventRecord(b, st));
+        }
+        CUDA_OR_FAIL(cudaEventSynchronize(b));
+        float ms = 0;
+        CUDA_OR_FAIL(cudaEventElapsedTime(&ms, a, b));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = l;
+        }
+        CUDA_OR_FAIL(cudaMemcpyAsync(s.x, snap, sizeof(V4) * s.n, cudaMemcpyDeviceToDevice, st));
+    }
+    CUDA_OR_FAIL(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long), st));
+    CUDA_OR_FAIL(cudaStreamSynchronize(st));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(snap);
+    c->lanes = best;
+    c->stats.kernel_launches = launches0;
+    if (getenv("AVBD_TRACE")) fprintf(stderr, "[avbd] autotune: %d threads per vertex (%.3f ms per sweep)\n", best, best_ms);
+    return AVBD_OK;
+}
 
 template <typename R>
 int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
@@ -830,6 +900,14 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
     CUDA_OR_FAIL(cudaGetLastError());
     return AVBD_OK;
 }
+
+}  // namespace
+
+static int autotune(avbd_ctx* c) {
+    return use64(c) ? autotune_impl<double>(c, c->d) : autotune_impl<float>(c, c->f);
+}
+
+namespace {
 
 int device_error(avbd_ctx* c) {
     int h = 0;

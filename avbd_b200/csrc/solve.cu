@@ -299,9 +299,17 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
     if (active) {
         xi = xyz(s.x[p]);
         unsigned b = s.inc_begin[p], e = s.inc_begin[p + 1];
-        for (unsigned k = b + lane; k < e; k += LANES) {
-            IncRec<RS> r = load_rec<RS>(inc + k);
+        // software pipeline: the next record streams in while this one is processed
+        unsigned k = b + lane;
+        IncRec<RS> r;
+        if (k < e) r = load_rec<RS>(inc + k);
+        while (k < e) {
+            const unsigned kn = k + LANES;
+            IncRec<RS> rn;
+            if (kn < e) rn = load_rec<RS>(inc + kn);
             accumulate_tet<P, RS, HT, DAMP>(s, r, xi, c.dt, B);
+            r = rn;
+            k = kn;
         }
     }
     reduce_block<LANES>(B);
@@ -522,6 +530,8 @@ static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, co
         solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T);
     } else {
         switch (c->lanes) {
+            case 1: solve_dispatch<P, RS, HT, 1, MODE>(c, s, inc, k, begin, count, st, out, T); break;
+            case 2: solve_dispatch<P, RS, HT, 2, MODE>(c, s, inc, k, begin, count, st, out, T); break;
             case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, begin, count, st, out, T); break;
             case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, begin, count, st, out, T); break;
             case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, begin, count, st, out, T); break;
