@@ -89,6 +89,7 @@ SIGNATURES = {
     "avbd_debug_block": [_vp, C.c_uint, _dp, _dp, C.POINTER(C.c_int)],
     "avbd_residual": [_vp, _dp],
     "avbd_profile_solve": [_vp, C.c_uint, _dp, _dp, _up],
+    "avbd_lbvh_morton_sort_noalloc": [_vp, C.c_uint, _vp, _vp, _vp],
     "avbd_last_error_string": [],
     "avbd_version": [],
 }

@@ -19,6 +19,7 @@
 // disjoint, which implies all leaf pairs below are disjoint too.  The same set
 // is produced here by one thread per leaf a walking the tree for leaves b > a.
 #include <algorithm>
+#include <mutex>
 
 #include "engine.h"
 
@@ -501,4 +502,133 @@ extern "C" int avbd_get_candidate_pairs(avbd_ctx* c, unsigned capacity, unsigned
         pairs2[2 * k + 1] = h[k].y;
     }
     return AVBD_OK;
+}
+
+// ======================================================= no-alloc variant
+//
+// Morton codes + stable radix sort of caller-provided primitive boxes, with
+// every scratch buffer in file-scope device arrays instead of cudaMalloc.  For
+// callers that must not allocate device memory while they run: a host loop
+// being recorded into a CUDA graph, a real-time loop with a fixed memory
+// budget, or an application whose device memory belongs to another
+// framework's allocator.  The arrays are sized for AVBD_NOALLOC_MAX_PRIMITIVES
+// primitives (about 4 MB) and stay resident on every GPU that loads the
+// library until the process exits.
+
+namespace {
+
+constexpr unsigned kNoAllocMax = AVBD_NOALLOC_MAX_PRIMITIVES;
+constexpr unsigned kNoAllocBlocks = (kNoAllocMax + RB - 1) / RB;
+
+static __device__ __align__(256) uint64_t g_na_keys_a[kNoAllocMax];  // sorted keys end here
+static __device__ __align__(256) uint64_t g_na_keys_b[kNoAllocMax];
+static __device__ __align__(256) uint32_t g_na_vals_b[kNoAllocMax];
+static __device__ __align__(256) uint32_t g_na_hist[256 * kNoAllocBlocks];
+static __device__ __align__(256) unsigned long long g_na_box[8];
+
+struct NoAllocScratch {
+    uint64_t* keys_a = nullptr;
+    uint64_t* keys_b = nullptr;
+    uint32_t* vals_b = nullptr;
+    uint32_t* hist = nullptr;
+    unsigned long long* box = nullptr;
+};
+
+// Device addresses of the scratch arrays, resolved once per device with that
+// device current (host code cannot use the arrays' names as addresses).
+std::mutex g_na_mutex;
+NoAllocScratch g_na_addr[64];
+bool g_na_ready[64] = {};
+
+int noalloc_scratch(int dev, NoAllocScratch& out) {
+    if (dev < 0 || dev >= 64) return AVBD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_ready[dev]) {
+        NoAllocScratch s;
+        if (cudaGetSymbolAddress((void**)&s.keys_a, g_na_keys_a) != cudaSuccess ||
+            cudaGetSymbolAddress((void**)&s.keys_b, g_na_keys_b) != cudaSuccess ||
+            cudaGetSymbolAddress((void**)&s.vals_b, g_na_vals_b) != cudaSuccess ||
+            cudaGetSymbolAddress((void**)&s.hist, g_na_hist) != cudaSuccess ||
+            cudaGetSymbolAddress((void**)&s.box, g_na_box) != cudaSuccess)
+            return AVBD_ERR_CUDA;
+        g_na_addr[dev] = s;
+        g_na_ready[dev] = true;
+    }
+    out = g_na_addr[dev];
+    return AVBD_OK;
+}
+
+// Scene box of caller-provided boxes (min/max are exact, order-preserving
+// integer atomics as in k_prim_bounds).
+__global__ void __launch_bounds__(256) k_box_of_aabbs(const double* __restrict__ aabb, unsigned n,
+                                                      unsigned long long* box) {
+    unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool valid = i < n;
+    unsigned long long e[6];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        e[a] = valid ? ord_enc(aabb[6ull * i + a]) : ~0ull;
+        e[3 + a] = valid ? ord_enc(aabb[6ull * i + 3 + a]) : 0ull;
+    }
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            unsigned long long o = __shfl_xor_sync(0xffffffffu, e[a], m);
+            e[a] = o < e[a] ? o : e[a];
+            o = __shfl_xor_sync(0xffffffffu, e[3 + a], m);
+            e[3 + a] = o > e[3 + a] ? o : e[3 + a];
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            atomicMin(box + a, e[a]);
+            atomicMax(box + 3 + a, e[3 + a]);
+        }
+    }
+}
+
+}  // namespace
+
+// Same results as the context path's Morton codes and sorted order
+// (LBVHBuilder::computeAABB_MortonCode + Algorithm::radixSort), on boxes the
+// caller computed.  Every call shares the scratch arrays, which keep the last
+// call's contents; the scene box is cleared at the start of each call.  Calls
+// that overlap on the GPU (for example on two streams at once) race on the
+// scratch and give wrong results.  The first call on a device resolves the
+// scratch addresses and should come before any stream capture.
+extern "C" int avbd_lbvh_morton_sort_noalloc(const double* aabb6, unsigned n, uint64_t* morton,
+                                             unsigned* sorted_order, void* stream) {
+    if (n == 0) return AVBD_OK;
+    if (!aabb6 || !morton || !sorted_order) return AVBD_ERR_INVALID_ARG;
+    if (n > kNoAllocMax) return AVBD_ERR_CAPACITY;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return AVBD_ERR_NO_DEVICE;
+    NoAllocScratch S;
+    if (int rc = noalloc_scratch(dev, S)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned nblk = (n + RB - 1) / RB;
+    cudaMemsetAsync(S.box, 0xFF, 3 * sizeof(unsigned long long), st);
+    cudaMemsetAsync(S.box + 3, 0x00, 3 * sizeof(unsigned long long), st);
+    k_box_of_aabbs<<<(n + 255) / 256, 256, 0, st>>>(aabb6, n, S.box);
+    LbvhState L;
+    L.n = n;
+    L.aabb = const_cast<double*>(aabb6);
+    L.morton = morton;          // per-primitive codes (output)
+    L.sorted = sorted_order;    // identity, sorted in place below
+    k_morton<<<(n + 255) / 256, 256, 0, st>>>(L, S.box);
+    cudaMemcpyAsync(S.keys_a, morton, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, st);
+    uint64_t *ka = S.keys_a, *kb = S.keys_b;
+    uint32_t *va = sorted_order, *vb = S.vals_b;
+    for (int shift = 0; shift < 64; shift += 8) {
+        k_radix_count<<<nblk, RB, 0, st>>>(ka, n, shift, S.hist, nblk);
+        k_radix_scan<<<1, 1024, 0, st>>>(S.hist, 256 * nblk);
+        k_radix_scatter<<<nblk, RB, 0, st>>>(ka, va, kb, vb, n, shift, S.hist, nblk);
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    // eight passes: sorted keys are back in keys_a, the order in sorted_order
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? AVBD_OK : AVBD_ERR_CUDA;
 }

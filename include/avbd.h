@@ -263,6 +263,25 @@ AVBD_API int avbd_debug_block(avbd_ctx* ctx, unsigned p, double* G, double* H, i
  * sqrt(sum_v |m g|^2)), FP64 reduction on the device. */
 AVBD_API int avbd_residual(avbd_ctx* ctx, double* residual);
 
+/* No counterpart in the reference.  Morton codes and the stable sorted order
+ * of an LBVH build for caller-provided primitive boxes, allocating nothing:
+ * for callers that must not allocate device memory while they run (a loop
+ * being recorded into a CUDA graph, a real-time loop on a fixed memory
+ * budget, an application whose device memory belongs to another framework's
+ * allocator).  Scratch lives in file-scope device arrays sized for
+ * AVBD_NOALLOC_MAX_PRIMITIVES primitives (about 4 MB, resident on every GPU
+ * that loads the library until exit); larger n returns AVBD_ERR_CAPACITY.
+ * aabb6 (n x {min xyz, max xyz} doubles), morton (n codes, one per primitive)
+ * and sorted_order (n indices) are device pointers owned by the caller;
+ * stream is a cudaStream_t (NULL: the default stream).  Results equal the
+ * codes and sorted order of avbd_get_lbvh for the same boxes.  Every call
+ * shares the scratch; calls that overlap on the GPU race.  The first call on
+ * a device resolves the scratch addresses and should come before any stream
+ * capture. */
+#define AVBD_NOALLOC_MAX_PRIMITIVES 262144u
+AVBD_API int avbd_lbvh_morton_sort_noalloc(const double* aabb6, unsigned n, uint64_t* morton,
+                                           unsigned* sorted_order, void* stream);
+
 /* Measurement entry point (no counterpart in the reference): runs `iterations`
  * further solver iterations on the current state without the CUDA graph,
  * bracketing every per-color vertex-solve launch with CUDA events on the
