@@ -205,6 +205,19 @@ class Context:
         check(self.L.avbd_get_velocities(self.h, 0, n, _dp(out)))
         return out
 
+    def rotations(self, out=None):
+        """Unit quaternions (w, x, y, z); identity for positional particles."""
+        n = self.num_particles
+        out = np.empty((n, 4)) if out is None else out
+        check(self.L.avbd_get_rotations(self.h, 0, n, _dp(out)))
+        return out
+
+    def angular_velocities(self, out=None):
+        n = self.num_particles
+        out = np.empty((n, 3)) if out is None else out
+        check(self.L.avbd_get_angular_velocities(self.h, 0, n, _dp(out)))
+        return out
+
     def coloring(self):
         out = np.zeros(self.num_particles, dtype=np.uint32)
         nc = C.c_uint(0)

@@ -575,6 +575,152 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
         CUDA_OR_FAIL(cudaMemcpyAsync(s.tet_e, te.data(), sizeof(V4) * 2 * nt, cudaMemcpyHostToDevice, st));
         s.ntets = nt;
     }
+    // oriented particles: rotation slots in internal order, rods, rigid-body
+    // ground contact and joints (RotationPool::addParticle initial state)
+    s.no = 0;
+    {
+        std::vector<uint32_t> rot(n, UINT32_MAX);
+        std::vector<unsigned> ext_slot_of(c->inertia.size() / 3, UINT32_MAX);
+        unsigned no = 0;
+        for (unsigned i = 0; i < n; i++) {
+            unsigned e = c->perm[i];
+            if (c->rot[e] != UINT32_MAX) {
+                rot[i] = no;
+                ext_slot_of[c->rot[e]] = no;
+                no++;
+            }
+        }
+        if (no > 0) {
+            auto qv = [](const double* q) {
+                V4 r;
+                r.x = (R)q[0]; r.y = (R)q[1]; r.z = (R)q[2]; r.w = (R)q[3];
+                return r;
+            };
+            std::vector<V4> q(no), Iv(no), zero(no), rgk(no), rglam(no), rgcp(no), rgloc(no);
+            std::vector<V4> jk(2ull * no), jlam(2ull * no), jcp(2ull * no), jpo(no), jro(no), jrp(no), jrq(no);
+            std::vector<uint8_t> oflag(no, 0);
+            V4 z = make4<R>(mk3<R>(0, 0, 0), R(0));
+            for (unsigned i = 0; i < n; i++) {
+                if (rot[i] == UINT32_MAX) continue;
+                unsigned e = c->perm[i], es = c->rot[e], sl = rot[i];
+                q[sl] = qv(&c->q[4ull * es]);
+                Iv[sl] = make4<R>(mk3<R>((R)c->inertia[3ull * es], (R)c->inertia[3ull * es + 1],
+                                         (R)c->inertia[3ull * es + 2]), R(0));
+                zero[sl] = z;
+                rgk[sl] = rglam[sl] = rgcp[sl] = rgloc[sl] = z;
+                jk[2 * sl] = jk[2 * sl + 1] = jlam[2 * sl] = jlam[2 * sl + 1] = jcp[2 * sl] = jcp[2 * sl + 1] = z;
+                jpo[sl] = jro[sl] = jrp[sl] = jrq[sl] = z;
+            }
+            for (auto& g : c->rground) {
+                unsigned sl = rot[c->inv[g.p]];
+                R ks = (R)g.k_start;
+                rgk[sl] = make4<R>(mk3<R>(ks, ks, ks), ks);
+                rgcp[sl] = make4<R>(mk3<R>(0, 0, (R)g.mu_s), (R)g.mu_k);
+                rgloc[sl] = make4<R>(mk3<R>((R)g.cp[0], (R)g.cp[1], (R)g.cp[2]), (R)g.radius);
+                oflag[sl] |= OF_RGROUND | OF_RG_ROUND;
+            }
+            for (auto& j : c->joints) {
+                unsigned sl = rot[c->inv[j.p]];
+                V4 k4 = make4<R>(mk3<R>(R(1e4), R(1e4), R(1e4)), R(1e4));
+                jk[2 * sl] = k4;
+                jk[2 * sl + 1] = make4<R>(mk3<R>(R(1e4), R(1e4), 0), R(0));
+                jpo[sl] = make4<R>(mk3<R>((R)j.po[0], (R)j.po[1], (R)j.po[2]), R(0));
+                jro[sl] = qv(j.ro);
+                jrp[sl] = make4<R>(mk3<R>((R)j.rp[0], (R)j.rp[1], (R)j.rp[2]), R(0));
+                jrq[sl] = qv(j.rq);
+                oflag[sl] |= OF_JOINT;
+            }
+            // rods and the per-vertex CSR of their incidences (slot order)
+            const unsigned nr = (unsigned)c->rods.size();
+            std::vector<uint2> ridx(nr);
+            std::vector<V4> rK(2ull * nr), rk0(nr);
+            std::vector<uint32_t> rb(n + 1, 0);
+            for (unsigned r = 0; r < nr; r++) {
+                const HostRod& h = c->rods[r];
+                ridx[r] = make_uint2(c->inv[h.idx[0]], c->inv[h.idx[1]]);
+                rK[2 * r] = make4<R>(mk3<R>((R)h.K[0], (R)h.K[1], (R)h.K[2]), (R)h.K[3]);
+                rK[2 * r + 1] = make4<R>(mk3<R>((R)h.K[4], (R)h.K[5], (R)h.L), R(0));
+                rk0[r] = make4<R>(mk3<R>((R)h.kappa[0], (R)h.kappa[1], (R)h.kappa[2]), R(0));
+                rb[ridx[r].x + 1]++;
+                rb[ridx[r].y + 1]++;
+            }
+            for (unsigned i = 0; i < n; i++) rb[i + 1] += rb[i];
+            std::vector<uint32_t> rinc(std::max(1u, rb[n]));
+            {
+                std::vector<uint32_t> cr(rb.begin(), rb.end() - 1);
+                for (unsigned r = 0; r < nr; r++) {
+                    rinc[cr[ridx[r].x]++] = (r << 1) | 0u;
+                    rinc[cr[ridx[r].y]++] = (r << 1) | 1u;
+                }
+            }
+            // algorithmic bytes of the 6-DOF solve of each color: own state
+            // (x, q, y, qy, inertia; flags, slot, CSR bounds), per rod element
+            // its index, record and the other node's x and q, the contact and
+            // joint records, and the x and q writes
+            {
+                const double V4B = sizeof(V4);
+                for (unsigned col = 0; col < c->num_colors; col++) {
+                    const unsigned b0 = c->color_begin[col] + c->color_solve[col];
+                    for (unsigned i = b0; i < b0 + c->color_orient[col]; i++) {
+                        if (flags[i] & VF_FIXED) continue;
+                        const unsigned sl = rot[i];
+                        double b = 7 * V4B + 2 + 3 * sizeof(uint32_t);
+                        b += (rb[i + 1] - rb[i]) * (sizeof(uint32_t) + sizeof(uint2) + 5 * V4B);
+                        if (oflag[sl] & OF_RGROUND) b += 4 * V4B;
+                        if (oflag[sl] & OF_JOINT) b += 10 * V4B;
+                        c->color_bytes[col] += b;
+                    }
+                }
+            }
+            if ((rc = dalloc(c, &s.rot, n)) || (rc = dalloc(c, &s.q, no)) || (rc = dalloc(c, &s.qy, no)) ||
+                (rc = dalloc(c, &s.qp, no)) || (rc = dalloc(c, &s.ql, no)) || (rc = dalloc(c, &s.qll, no)) ||
+                (rc = dalloc(c, &s.w, no)) || (rc = dalloc(c, &s.wp, no)) || (rc = dalloc(c, &s.Iv, no)) ||
+                (rc = dalloc(c, &s.rgk, no)) || (rc = dalloc(c, &s.rglam, no)) || (rc = dalloc(c, &s.rgcp, no)) ||
+                (rc = dalloc(c, &s.rgloc, no)) || (rc = dalloc(c, &s.jk, 2ull * no)) ||
+                (rc = dalloc(c, &s.jlam, 2ull * no)) || (rc = dalloc(c, &s.jcp, 2ull * no)) ||
+                (rc = dalloc(c, &s.jpo, no)) || (rc = dalloc(c, &s.jro, no)) || (rc = dalloc(c, &s.jrp, no)) ||
+                (rc = dalloc(c, &s.jrq, no)) || (rc = dalloc(c, &s.oflag, no)) ||
+                (rc = dalloc(c, &s.rod_begin, n + 1)) || (rc = dalloc(c, &s.rod_inc, rinc.size())) ||
+                (rc = dalloc(c, &s.rod_idx, std::max(1u, nr))) || (rc = dalloc(c, &s.rod_K, std::max(2u, 2 * nr))) ||
+                (rc = dalloc(c, &s.rod_k0, std::max(1u, nr))))
+                return rc;
+            auto up = [&](void* d, const void* h, size_t bytes) {
+                return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st);
+            };
+            const size_t qb = sizeof(V4) * no;
+            CUDA_OR_FAIL(up(s.rot, rot.data(), sizeof(uint32_t) * n));
+            CUDA_OR_FAIL(up(s.q, q.data(), qb));
+            CUDA_OR_FAIL(up(s.qy, q.data(), qb));
+            CUDA_OR_FAIL(up(s.qp, q.data(), qb));
+            CUDA_OR_FAIL(up(s.ql, q.data(), qb));
+            CUDA_OR_FAIL(up(s.qll, q.data(), qb));
+            CUDA_OR_FAIL(up(s.w, zero.data(), qb));
+            CUDA_OR_FAIL(up(s.wp, zero.data(), qb));
+            CUDA_OR_FAIL(up(s.Iv, Iv.data(), qb));
+            CUDA_OR_FAIL(up(s.rgk, rgk.data(), qb));
+            CUDA_OR_FAIL(up(s.rglam, rglam.data(), qb));
+            CUDA_OR_FAIL(up(s.rgcp, rgcp.data(), qb));
+            CUDA_OR_FAIL(up(s.rgloc, rgloc.data(), qb));
+            CUDA_OR_FAIL(up(s.jk, jk.data(), 2 * qb));
+            CUDA_OR_FAIL(up(s.jlam, jlam.data(), 2 * qb));
+            CUDA_OR_FAIL(up(s.jcp, jcp.data(), 2 * qb));
+            CUDA_OR_FAIL(up(s.jpo, jpo.data(), qb));
+            CUDA_OR_FAIL(up(s.jro, jro.data(), qb));
+            CUDA_OR_FAIL(up(s.jrp, jrp.data(), qb));
+            CUDA_OR_FAIL(up(s.jrq, jrq.data(), qb));
+            CUDA_OR_FAIL(up(s.oflag, oflag.data(), no));
+            CUDA_OR_FAIL(up(s.rod_begin, rb.data(), sizeof(uint32_t) * (n + 1)));
+            CUDA_OR_FAIL(up(s.rod_inc, rinc.data(), sizeof(uint32_t) * rinc.size()));
+            if (nr) {
+                CUDA_OR_FAIL(up(s.rod_idx, ridx.data(), sizeof(uint2) * nr));
+                CUDA_OR_FAIL(up(s.rod_K, rK.data(), sizeof(V4) * 2 * nr));
+                CUDA_OR_FAIL(up(s.rod_k0, rk0.data(), sizeof(V4) * nr));
+            }
+            s.no = no;
+            s.nrods = nr;
+            (void)ext_slot_of;
+        }
+    }
     s.err = c->d_error;
     CUDA_OR_FAIL(cudaStreamSynchronize(st));
     return AVBD_OK;
@@ -590,11 +736,24 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     free_device(c);
     const unsigned n = (unsigned)c->mass.size();
     if (n == 0) return fail(AVBD_ERR_STATE, "no particles");
-    if (!c->rods.empty() || !c->rground.empty() || !c->joints.empty())
-        return fail(AVBD_ERR_UNSUPPORTED, "oriented-particle energies are not enabled in this build");
     for (auto& p : c->prims)
-        if (p.type != AVBD_SHAPE_TRIANGLE)
-            return fail(AVBD_ERR_UNSUPPORTED, "only triangle collision primitives are enabled in this build");
+        if (p.type == AVBD_SHAPE_SPHERE)
+            return fail(AVBD_ERR_UNSUPPORTED, "sphere collision primitives are not enabled in this build");
+    for (auto& g : c->ground)
+        if (c->rot[g.p] != UINT32_MAX)
+            return fail(AVBD_ERR_UNSUPPORTED, "ground energy on an oriented particle (use rigid-body ground)");
+    for (auto& g : c->rground)
+        if (g.shape != AVBD_SHAPE_SPHERE && g.shape != AVBD_SHAPE_ROD_SEGMENT)
+            return fail(AVBD_ERR_UNSUPPORTED, "rigid-body ground contact needs a sphere or rod-segment shape");
+    {
+        std::vector<uint8_t> seen_rg(n, 0), seen_j(n, 0);
+        for (auto& g : c->rground) {
+            if (seen_rg[g.p]++) return fail(AVBD_ERR_UNSUPPORTED, "more than one rigid-body ground energy on a particle");
+        }
+        for (auto& j : c->joints) {
+            if (seen_j[j.p]++) return fail(AVBD_ERR_UNSUPPORTED, "more than one joint on a particle");
+        }
+    }
 
     // scenes: [scene_begin[s], scene_begin[s+1])
     std::vector<unsigned> sb = c->scene_begin;
@@ -608,6 +767,9 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     std::vector<unsigned> inc_off(n + 1, 0);
     c->damping = false;
     for (auto& h : c->nh) {
+        for (int k = 0; k < 4; k++)
+            if (c->rot[h.idx[k]] != UINT32_MAX)
+                return fail(AVBD_ERR_INVALID_ARG, "NeoHookean energy on an oriented particle");
         for (int k = 0; k < 4; k++) inc_off[h.idx[k] + 1]++;
         if (h.kd != 0) c->damping = true;
         unsigned s0 = scene_of[h.idx[0]];
@@ -661,11 +823,13 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     for (unsigned e = 0; e < n; e++) cnt[3ull * c->color[e] + cls(e)]++;
     c->color_begin.assign(nc + 1, 0);
     c->color_solve.assign(nc, 0);
+    c->color_orient.assign(nc, 0);
     std::vector<unsigned> cur(3ull * nc);
     unsigned run = 0;
     for (unsigned k = 0; k < nc; k++) {
         c->color_begin[k] = run;
         c->color_solve[k] = cnt[3ull * k];
+        c->color_orient[k] = cnt[3ull * k + 1];
         for (int t = 0; t < 3; t++) { cur[3ull * k + t] = run; run += cnt[3ull * k + t]; }
     }
     c->color_begin[nc] = run;
@@ -750,24 +914,64 @@ double omega_at(unsigned i, double rho, double prev) {
     return 1;
 }
 
+// Collision stage and step-start hooks + inertial prediction.
+template <typename R>
+void enqueue_begin(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
+    if (c->damping) launch_tet_eprev<R>(c, s, k, st);
+    launch_begin_step<R>(c, s, k, st);
+    launch_begin_step_rot<R>(c, s, k, st);
+}
+
+// One Gauss-Seidel sweep: per color, the positional (3-DOF) slab then the
+// oriented (6-DOF) slab; both are independent sets within the color.
+template <typename R>
+void enqueue_sweep(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, const SceneTol& T) {
+    for (unsigned col = 0; col < c->num_colors; col++) {
+        if (c->color_solve[col])
+            launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st, T);
+        if (c->color_orient[col])
+            launch_solve_rod<R>(c, s, k, c->color_begin[col] + c->color_solve[col], c->color_orient[col], st, T, 0,
+                                nullptr);
+    }
+}
+
+template <typename R>
+void enqueue_chebyshev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+                       const SceneTol& T) {
+    launch_chebyshev_dual<R>(c, s, k, omega, st, T);
+    launch_chebyshev_rot<R>(c, s, k, omega, st, T);
+}
+
+template <typename R>
+void enqueue_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    launch_velocity<R>(c, s, k, st);
+    launch_velocity_rot<R>(c, s, k, st);
+}
+
+// Residual pass over all particles (positional and oriented blocks).
+template <typename R>
+void enqueue_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st,
+                      const SceneTol& T) {
+    launch_residual<R>(c, s, k, out2, st, T);
+    if (s.no) launch_solve_rod<R>(c, s, k, 0, s.n, st, T, 1, out2);
+}
+
 template <typename R>
 void enqueue_iteration(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st) {
-    for (unsigned col = 0; col < c->num_colors; col++)
-        if (c->color_solve[col]) launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st);
-    launch_chebyshev_dual<R>(c, s, k, omega, st);
+    enqueue_sweep<R>(c, s, k, st, SceneTol());
+    enqueue_chebyshev<R>(c, s, k, omega, st, SceneTol());
 }
 
 template <typename R>
 void enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
-    if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
-    if (c->damping) launch_tet_eprev<R>(c, s, k, st);
-    launch_begin_step<R>(c, s, k, st);
+    enqueue_begin<R>(c, s, k, st);
     double omega = 1;
     for (unsigned i = 0; i < c->solver.solver_iters; i++) {
         omega = omega_at(i, c->solver.iter_acceleration, omega);
         enqueue_iteration<R>(c, s, k, omega, st);
     }
-    launch_velocity<R>(c, s, k, st);
+    enqueue_velocity<R>(c, s, k, st);
 }
 
 StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_accel, c->kappa_max}; }
@@ -845,26 +1049,22 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         SceneTol solveT{c->d_scene, c->d_scene_active, nullptr, c->d_scene_r2, nullptr};
         SceneTol resT{c->d_scene, nullptr, c->d_scene_cand, nullptr, c->d_scene_ex};
         for (unsigned t = 0; t < n_steps; t++) {
-            if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
-            if (c->damping) launch_tet_eprev<R>(c, s, k, st);
-            launch_begin_step<R>(c, s, k, st);
+            enqueue_begin<R>(c, s, k, st);
             launch_tol_init(c, st);
             double omega = 1;
             for (unsigned it = 0; it < max_it; it++) {
                 omega = omega_at(it, c->solver.iter_acceleration, omega);
-                for (unsigned col = 0; col < c->num_colors; col++)
-                    if (c->color_solve[col])
-                        launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st, solveT);
-                launch_chebyshev_dual<R>(c, s, k, omega, st, solveT);
+                enqueue_sweep<R>(c, s, k, st, solveT);
+                enqueue_chebyshev<R>(c, s, k, omega, st, solveT);
                 launch_tol_decide_a(c, tol, st);
-                launch_residual<R>(c, s, k, nullptr, st, resT);
+                enqueue_residual<R>(c, s, k, nullptr, st, resT);
                 launch_tol_decide_b(c, tol, max_it, st);
                 int n_active = 0;
                 CUDA_OR_FAIL(cudaMemcpyAsync(&n_active, c->d_tol_count, sizeof(int), cudaMemcpyDeviceToHost, st));
                 CUDA_OR_FAIL(cudaStreamSynchronize(st));
                 if (n_active == 0) break;
             }
-            launch_velocity<R>(c, s, k, st);
+            enqueue_velocity<R>(c, s, k, st);
         }
         CUDA_OR_FAIL(cudaGetLastError());
         return AVBD_OK;
@@ -1072,25 +1272,35 @@ static int get_vec(avbd_ctx* c, int which, unsigned first, unsigned n, double* o
 int avbd_get_positions(avbd_ctx* c, unsigned first, unsigned n, double* out) { return get_vec(c, 0, first, n, out); }
 int avbd_get_velocities(avbd_ctx* c, unsigned first, unsigned n, double* out) { return get_vec(c, 1, first, n, out); }
 
-int avbd_get_rotations(avbd_ctx* c, unsigned first, unsigned n, double* out) {
+// Rotations (which 0, 4 doubles (w,x,y,z) per particle) or angular velocities
+// (which 1, 3 doubles) of particles [first, first+n); positional particles
+// report the identity / zero.
+static int get_rot(avbd_ctx* c, int which, unsigned first, unsigned n, double* out) {
     if (int r = check_ctx(c)) return r;
     if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
-    for (unsigned i = 0; i < n; i++) {
-        unsigned e = first + i;
-        if (c->rot[e] == UINT32_MAX) {
-            out[4 * i] = 1; out[4 * i + 1] = out[4 * i + 2] = out[4 * i + 3] = 0;
-        } else {
-            for (int k = 0; k < 4; k++) out[4 * i + k] = c->q[4ull * c->rot[e] + k];
+    const unsigned stride = which == 0 ? 4 : 3;
+    if (!c->finalized) {
+        for (unsigned i = 0; i < n; i++) {
+            unsigned e = first + i;
+            for (unsigned k = 0; k < stride; k++) out[stride * i + k] = (which == 0 && k == 0) ? 1.0 : 0.0;
+            if (which == 0 && c->rot[e] != UINT32_MAX)
+                for (int k = 0; k < 4; k++) out[4 * i + k] = c->q[4ull * c->rot[e] + k];
         }
+        return AVBD_OK;
     }
-    return AVBD_OK;
+    if (int r = ensure_h2d(c, 4ull * n)) return r;
+    if (use64(c)) launch_store_rot<double>(c->d, which, c->d_h2d, c->d_inv + first, n, c->stream);
+    else launch_store_rot<float>(c->f, which, c->d_h2d, c->d_inv + first, n, c->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    CUDA_OR_FAIL(cudaMemcpyAsync(out, c->d_h2d, sizeof(double) * stride * n, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return device_error(c);
 }
 
+int avbd_get_rotations(avbd_ctx* c, unsigned first, unsigned n, double* out) { return get_rot(c, 0, first, n, out); }
+
 int avbd_get_angular_velocities(avbd_ctx* c, unsigned first, unsigned n, double* w) {
-    if (int r = check_ctx(c)) return r;
-    if ((size_t)first + n > c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "range out of bounds");
-    std::fill(w, w + 3ull * n, 0.0);
-    return AVBD_OK;
+    return get_rot(c, 1, first, n, w);
 }
 
 int avbd_get_coloring(avbd_ctx* c, unsigned* colors, unsigned* num_colors) {
@@ -1105,21 +1315,28 @@ int avbd_debug_block(avbd_ctx* c, unsigned p, double* G, double* H, int* dof) {
     if (int r = check_ctx(c)) return r;
     if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
     if (p >= c->mass.size()) return fail(AVBD_ERR_INVALID_ARG, "particle index out of range");
-    double h[12] = {0};
-    CUDA_OR_FAIL(cudaMemsetAsync(c->d_residual, 0, 4 * sizeof(double), c->stream));
+    double h[42] = {0};
     double* out = nullptr;
-    if (int r = ensure_h2d(c, 12)) return r;
+    if (int r = ensure_h2d(c, 42)) return r;
     out = c->d_h2d;
-    CUDA_OR_FAIL(cudaMemsetAsync(out, 0, 12 * sizeof(double), c->stream));
+    CUDA_OR_FAIL(cudaMemsetAsync(out, 0, 42 * sizeof(double), c->stream));
     StepConsts k = consts(c);
-    if (use64(c)) launch_debug_block<double>(c, c->d, k, c->inv[p], out, c->stream);
-    else launch_debug_block<float>(c, c->f, k, c->inv[p], out, c->stream);
+    const bool oriented = c->rot[p] != UINT32_MAX;
+    const unsigned ip = c->inv[p];
+    if (oriented) {
+        if (use64(c)) launch_solve_rod<double>(c, c->d, k, ip, 1, c->stream, SceneTol(), 2, out);
+        else launch_solve_rod<float>(c, c->f, k, ip, 1, c->stream, SceneTol(), 2, out);
+    } else {
+        if (use64(c)) launch_debug_block<double>(c, c->d, k, ip, out, c->stream);
+        else launch_debug_block<float>(c, c->f, k, ip, out, c->stream);
+    }
     CUDA_OR_FAIL(cudaGetLastError());
     CUDA_OR_FAIL(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
-    for (int i = 0; i < 3; i++) G[i] = h[i];
-    for (int i = 0; i < 9; i++) H[i] = h[3 + i];
-    if (dof) *dof = 3;
+    const int d = oriented ? 6 : 3;
+    for (int i = 0; i < d; i++) G[i] = h[i];
+    for (int i = 0; i < d * d; i++) H[i] = h[d + i];
+    if (dof) *dof = d;
     return AVBD_OK;
 }
 
@@ -1142,13 +1359,19 @@ int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, doubl
             if (c->color_solve[col]) {
                 if (use64(c)) launch_solve_color<double>(c, c->d, k, c->color_begin[col], c->color_solve[col], c->stream);
                 else launch_solve_color<float>(c, c->f, k, c->color_begin[col], c->color_solve[col], c->stream);
-                bytes += c->color_bytes[col];
                 nl++;
             }
+            if (c->color_orient[col]) {
+                unsigned b0 = c->color_begin[col] + c->color_solve[col];
+                if (use64(c)) launch_solve_rod<double>(c, c->d, k, b0, c->color_orient[col], c->stream, SceneTol(), 0, nullptr);
+                else launch_solve_rod<float>(c, c->f, k, b0, c->color_orient[col], c->stream, SceneTol(), 0, nullptr);
+                nl++;
+            }
+            bytes += c->color_bytes[col];
             CUDA_OR_FAIL(cudaEventRecord(b, c->stream));
         }
-        if (use64(c)) launch_chebyshev_dual<double>(c, c->d, k, omega, c->stream);
-        else launch_chebyshev_dual<float>(c, c->f, k, omega, c->stream);
+        if (use64(c)) enqueue_chebyshev<double>(c, c->d, k, omega, c->stream, SceneTol());
+        else enqueue_chebyshev<float>(c, c->f, k, omega, c->stream, SceneTol());
     }
     CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
     double ms = 0;
@@ -1168,8 +1391,8 @@ int avbd_residual(avbd_ctx* c, double* residual) {
     if (int r = check_ctx(c)) return r;
     if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
     StepConsts k = consts(c);
-    if (use64(c)) launch_residual<double>(c, c->d, k, c->d_residual, c->stream);
-    else launch_residual<float>(c, c->f, k, c->d_residual, c->stream);
+    if (use64(c)) enqueue_residual<double>(c, c->d, k, c->d_residual, c->stream, SceneTol());
+    else enqueue_residual<float>(c, c->f, k, c->d_residual, c->stream, SceneTol());
     double h[2];
     CUDA_OR_FAIL(cudaMemcpyAsync(h, c->d_residual, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));

@@ -63,6 +63,39 @@ struct DevState {
     V4* gcp = nullptr;     // cp_x, cp_z, mu_s, mu_k
     uint8_t* gflag = nullptr;
     int* err = nullptr;    // device-side status (AVBD_ERR_*), 0 when healthy
+
+    // ---- oriented particles (RotationPool, common/ParticlePool.hpp:7-68).
+    // rot[p] is the rotation slot of internal vertex p (UINT32_MAX if positional);
+    // quaternions are stored (w, x, y, z) in the x, y, z, w fields.
+    unsigned no = 0;
+    uint32_t* rot = nullptr;
+    V4 *q = nullptr, *qy = nullptr, *qp = nullptr, *ql = nullptr, *qll = nullptr;
+    V4 *w = nullptr, *wp = nullptr, *Iv = nullptr;
+    // Cosserat rods: per oriented vertex a CSR of (rod << 1 | local)
+    unsigned nrods = 0;
+    uint32_t* rod_begin = nullptr;   // n + 1
+    uint32_t* rod_inc = nullptr;
+    uint2* rod_idx = nullptr;        // internal vertex ids of the two nodes
+    V4* rod_K = nullptr;             // (K0..K3), (K4, K5, rest length, 0) per rod
+    V4* rod_k0 = nullptr;            // precurvature
+    // rigid-body ground contact, one per rotation slot
+    V4* rgk = nullptr;               // k_n, k_t, k_b, k_start
+    V4* rglam = nullptr;             // lam_n, lam_t, lam_b, C_n_prev
+    V4* rgcp = nullptr;              // cp_ground.x, cp_ground.z, mu_s, mu_k
+    V4* rgloc = nullptr;             // cp_rb_local xyz, shape radius
+    // one-sided fixed joint, one per rotation slot (6 rows)
+    V4* jk = nullptr;                // k rows 0-3, 4-5 (2 per slot)
+    V4* jlam = nullptr;              // lambda rows (2 per slot)
+    V4* jcp = nullptr;               // C_prev rows (2 per slot)
+    V4* jpo = nullptr;               // position offset
+    V4* jro = nullptr;               // rotation offset (quaternion)
+    V4* jrp = nullptr;               // reference position
+    V4* jrq = nullptr;               // reference rotation (quaternion)
+    uint8_t* oflag = nullptr;        // per rotation slot, OrientedFlags
+};
+
+enum OrientedFlags : uint8_t {
+    OF_RGROUND = 1, OF_RG_USE_STATIC = 2, OF_RG_UNCLAMPED = 4, OF_RG_ROUND = 8, OF_JOINT = 16
 };
 
 // Per-scene run-to-tolerance state passed to the solve, Chebyshev and residual
@@ -156,6 +189,7 @@ struct avbd_ctx {
     std::vector<unsigned> inv;          // external -> internal
     std::vector<unsigned> color_begin;  // internal offset of each color slab
     std::vector<unsigned> color_solve;  // vertices of the slab that run the 3-DOF solve
+    std::vector<unsigned> color_orient; // oriented non-fixed vertices after them (6-DOF solve)
     std::vector<double> color_bytes;    // algorithmic bytes of each color's solve launch
     unsigned max_color_solve = 0;
 
@@ -211,6 +245,20 @@ void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStrea
 template <typename R>
 void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* out2, cudaStream_t st,
                      const SceneTol& T = SceneTol());
+// ---- oriented particles (rods.cu); rod solve modes: 0 solve, 1 residual, 2 debug
+template <typename R>
+void launch_begin_step_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+template <typename R>
+void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
+                      cudaStream_t st, const SceneTol& T, int mode, double* out);
+template <typename R>
+void launch_chebyshev_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+                          const SceneTol& T = SceneTol());
+template <typename R>
+void launch_velocity_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+template <typename R>
+void launch_store_rot(const DevState<R>& s, int which, double* dst, const uint32_t* inv_map, unsigned n,
+                      cudaStream_t st);
 // per-scene tolerance bookkeeping kernels
 void launch_tol_init(avbd_ctx* c, cudaStream_t st);
 void launch_tol_decide_a(avbd_ctx* c, double tol, cudaStream_t st);

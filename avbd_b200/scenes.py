@@ -191,6 +191,140 @@ def cube_drop(n: int = 32, seed: int = 0, iters: int = 20, rho: float = 0.5, dt:
     return sc
 
 
+def quat_mul(a, b):
+    w1, x1, y1, z1 = a
+    w2, x2, y2, z2 = b
+    return np.array([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2, w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                     w1 * y2 + y1 * w2 + z1 * x2 - x1 * z2, w1 * z2 + z1 * w2 + x1 * y2 - y1 * x2])
+
+
+def quat_rotate(q, v):
+    u = np.asarray(q[1:])
+    t = 2 * np.cross(u, v)
+    return np.asarray(v) + q[0] * t + np.cross(u, t)
+
+
+def quat_exp(v):
+    """Math::Exp_s3 (common/Math.hpp:197-222)."""
+    v = np.asarray(v, dtype=np.float64)
+    th = np.linalg.norm(v)
+    if th < 1e-6:
+        q = np.array([1.0, 0.5 * v[0], 0.5 * v[1], 0.5 * v[2]])
+        return q / np.linalg.norm(q)
+    s = np.sin(0.5 * th) / th
+    return np.array([np.cos(0.5 * th), s * v[0], s * v[1], s * v[2]])
+
+
+def quat_from_xyz_euler(deg):
+    """Math::QuaternionFromXYZEulerAngles (common/Math.hpp:298-318): qz qy qx."""
+    x, y, z = np.radians(deg)
+    qx = np.array([np.cos(x / 2), np.sin(x / 2), 0, 0])
+    qy = np.array([np.cos(y / 2), 0, np.sin(y / 2), 0])
+    qz = np.array([np.cos(z / 2), 0, 0, np.sin(z / 2)])
+    return quat_mul(quat_mul(qz, qy), qx)
+
+
+def add_rod(sc: Scene, elements: int, length: float, radius: float, E: float, nu: float, density: float,
+            position, euler_deg, curvature, base_joint=True, base_fixed=False, ground=True, collide=True,
+            object_id=0):
+    """Rod::Rod (simobject/Rod.cpp:10-68): nodes integrated along the local z
+    axis with frames advanced by Exp_s3(curvature ds); lumped translational and
+    rotational mass; Cosserat stiffness (GA, GA, EA, EIx, EIy, GIz).  The base
+    is held by a one-sided fixed joint at its initial pose (the commented
+    alternative of Rod.cpp:79-91) instead of being fixed."""
+    G = E / (2 * (1 + nu))
+    nn = elements + 1
+    ds = length / (nn - 1)
+    dR = np.asarray(curvature, dtype=np.float64) * ds
+    pos = np.asarray(position, dtype=np.float64).copy()
+    rot = quat_from_xyz_euler(euler_deg)
+    P, Qs = [], []
+    for _ in range(nn):
+        P.append(pos.copy())
+        Qs.append(rot.copy())
+        pos = pos + quat_rotate(rot, np.array([0.0, 0.0, ds]))
+        rot = quat_mul(rot, quat_exp(dR))
+    area = np.pi * radius ** 2
+    Ix = np.pi * radius ** 4 / 4.0
+    m_e = ds * area * density
+    I_e = density * ds * np.array([Ix, Ix, 2 * Ix])
+    masses = np.zeros(nn)
+    inert = np.zeros((nn, 3))
+    for e in range(elements):
+        masses[e] += 0.5 * m_e
+        masses[e + 1] += 0.5 * m_e
+        inert[e] += 0.5 * I_e
+        inert[e + 1] += 0.5 * I_e
+    base = sc.num_particles
+    sc.record("add_oriented_particles", np.array(P), np.array(Qs), masses, inert)
+    idx = np.stack([np.arange(elements), np.arange(1, elements + 1)], axis=1) + base
+    K = np.array([G * area, G * area, E * area, E * Ix, E * Ix, G * 2 * Ix])
+    sc.record("add_cosserat_rod", idx, np.tile(K, (elements, 1)), np.full(elements, ds),
+              np.tile(np.asarray(curvature, dtype=np.float64), (elements, 1)))
+    if base_joint:
+        sc.record("add_one_sided_fixed_joint", [base], np.zeros((1, 3)), np.array([[1.0, 0, 0, 0]]),
+                  np.array([P[0]]), np.array([Qs[0]]))
+    if base_fixed:
+        sc.record("set_fixed", [base], [1])
+    if ground:
+        ks = masses / sc.dt ** 2
+        sc.record("add_rigid_body_ground_collision", np.arange(nn) + base, np.full(nn, 1, dtype=np.uint8),
+                  np.full(nn, radius), np.tile([0.0, -radius, 0.0], (nn, 1)), ks, np.full(nn, 0.5),
+                  np.full(nn, 0.2))
+    if collide:
+        sc.record("add_rod_segments", idx, radius, object_id)
+        sc.num_primitives += elements
+    sc.num_particles += nn
+    return base
+
+
+def add_sphere(sc: Scene, radius: float, density: float, position, ground=True):
+    """RigidSphere (simobject/rigid/RigidSphere.cpp:8-22): mass 4/3 pi r^3 rho,
+    inertia 2/5 m r^2; rigid-body ground contact (Simulation.hpp:108-115)."""
+    m = 4 * np.pi / 3 * radius ** 3 * density
+    I = 0.4 * m * radius ** 2
+    base = sc.num_particles
+    sc.record("add_oriented_particles", np.array([position], dtype=np.float64), np.array([[1.0, 0, 0, 0]]), [m],
+              np.array([[I, I, I]]))
+    if ground:
+        sc.record("add_rigid_body_ground_collision", [base], np.array([2], dtype=np.uint8), [radius],
+                  np.array([[0.0, -radius, 0.0]]), [m / sc.dt ** 2], [0.5], [0.2])
+    sc.num_particles += 1
+    return base
+
+
+def rods_and_spheres(num_rods: int = 256, segments: int = 100, num_spheres: int = 64, seed: int = 0,
+                     iters: int = 20, rho: float = 0.5, dt: float = 1.0 / 60.0, length: float = 1.0,
+                     helix_radius: float = 0.02, spacing: float = 0.1) -> Scene:
+    """Cosserat rods and rigid spheres: rods of `segments` elements (radius
+    5 mm, E 1e7, G 4e6 so nu = 0.25, rho 1000), length 1 m, shaped as seeded
+    helices (radius 2 cm, pitch ~ U(2, 10) cm) through a constant precurvature
+    (kappa, 0, tau), hanging from one-sided fixed joints at their bases on a
+    grid 1.2 m above the ground; spheres of radius ~ U(1, 5) cm dropped onto
+    the ground beside them.  Rod nodes and spheres have rigid-body ground
+    contact; rod segments are collision primitives."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(name=f"rods{num_rods}x{segments}_spheres{num_spheres}", dt=dt, solver_iters=iters,
+               iter_acceleration=rho)
+    side = int(np.ceil(np.sqrt(num_rods)))
+    E, nu = 1e7, 0.25
+    for r in range(num_rods):
+        pitch = rng.uniform(0.02, 0.10)
+        b = pitch / (2 * np.pi)
+        a = helix_radius
+        kappa, tau = a / (a * a + b * b), b / (a * a + b * b)
+        ox, oz = (r % side) * spacing, (r // side) * spacing
+        add_rod(sc, segments, length, 0.005, E, nu, 1000.0, (ox, 1.2, oz), (90.0, 0.0, 0.0), (kappa, 0.0, tau),
+                object_id=r)
+    for s in range(num_spheres):
+        rad = rng.uniform(0.01, 0.05)
+        x = rng.uniform(0, side * spacing)
+        z = side * spacing + 0.2 + rng.uniform(0, 1.0)
+        add_sphere(sc, rad, 1000.0, (x, rad + rng.uniform(0.05, 0.5), z))
+    sc.meta["bbox_diagonal"] = float(np.linalg.norm([side * spacing, 1.2, side * spacing + 1.2]))
+    return sc
+
+
 def batched_cube_params(seed: int, s: int, n_min: int = 4, n_max: int = 24):
     """Parameters of scene s of a batch: drawn from a generator seeded by
     (seed, s), so any subset of a batch is reproduced exactly."""

@@ -8,6 +8,11 @@ every step runs AVBD iterations until the residual R <= 1e-4 (at most
 --max-iters).  One step of the batch counts as `scenes` scene-steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--workload batch_cubes|rods_spheres]
+
+`--workload rods_spheres` measures the rod scene instead: 256 Cosserat rods
+of 100 segments hanging from one-sided fixed joints plus 64 rigid spheres,
+all with rigid-body ground contact, 20 iterations per step, FP32 (steps/s).
 
 Prints one JSON line.  `value` is scene-steps/s over all ranks with the state
 resident in HBM; `e2e` repeats the measurement through the C-ABI with the
@@ -48,8 +53,44 @@ def parse():
     p.add_argument("--cpu-sample-scenes", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "fp64"])
-    return p.parse_args()
+    p.add_argument("--precision", default=None, choices=["fp32", "mixed", "fp64"],
+                   help="default: mixed for batch_cubes, fp32 for rods_spheres")
+    p.add_argument("--workload", default="batch_cubes", choices=["batch_cubes", "rods_spheres"])
+    a = p.parse_args()
+    if a.precision is None:
+        a.precision = "fp32" if a.workload == "rods_spheres" else "mixed"
+    return a
+
+
+class Workload:
+    """The scene set one rank advances, and how its steps are counted."""
+
+    def __init__(self, args, seed):
+        from avbd_b200 import scenes
+        self.rods = args.workload == "rods_spheres"
+        if self.rods:
+            self.scene = scenes.rods_and_spheres(seed=seed)
+            self.name = "rods256x100_spheres64"
+            self.units = 1
+            self.unit = "steps/s"
+            self.tol, self.max_iters = 0.0, 0
+            self.method = "plain AVBD, 20 fixed iterations per step"
+        else:
+            self.scene = scenes.batched_cubes(num_scenes=args.scenes, seed=seed)
+            self.name = f"batch{args.scenes}_cubes"
+            self.units = args.scenes
+            self.unit = UNIT
+            self.tol, self.max_iters = args.tol, args.max_iters
+            self.method = "plain AVBD (no warm start)"
+
+    def sample(self, args, seed):
+        """The bounded sample the CPU baseline times, and its unit count."""
+        from avbd_b200 import scenes
+        if self.rods:
+            return self.scene, 1, "the same rod scene"
+        S = args.cpu_sample_scenes
+        return (scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=range(S)), S,
+                f"{S} of {args.scenes} scenes of the same batch")
 
 
 def measured_peaks():
@@ -119,21 +160,19 @@ def traffic_for(workload: str):
         return None
 
 
-def cpu_sample(args, seed, threads):
-    """FP64 oracle port on the first S scenes of the same batch: scene-steps/s."""
-    from avbd_b200 import scenes
+def cpu_sample(args, wl, seed, threads):
+    """FP64 oracle port on a bounded sample of the workload: units/s."""
     from oracle.oracle import Oracle
-    S = args.cpu_sample_scenes
-    sc = scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=range(S))
+    sc, S, what = wl.sample(args, seed)
     o = Oracle(threads=threads)
-    sc.load(o, residual_tolerance=args.tol, max_iters=args.max_iters)
+    sc.load(o, residual_tolerance=wl.tol, max_iters=wl.max_iters)
     o.finalize()
     o.step(1)  # warm-up (first contact step)
     steps, t = 0, 0.0
     while t < args.cpu_seconds and steps < 200:
         t += o.time_steps(1)
         steps += 1
-    return S * steps / t, S, steps, t
+    return S * steps / t, what, steps, t
 
 
 def run_reference(args):
@@ -142,25 +181,24 @@ def run_reference(args):
     if rank != 0:
         return
     threads = min(os.cpu_count() or 1, 32)
-    from avbd_b200 import scenes
     from oracle.oracle import Oracle
-    S = args.cpu_sample_scenes
-    sc = scenes.batched_cubes(num_scenes=args.scenes, seed=args.seed, scene_ids=range(S))
+    wl = Workload(args, args.seed)
+    sc, S, what = wl.sample(args, args.seed)
     o = Oracle(threads=threads)
-    sc.load(o, residual_tolerance=args.tol, max_iters=args.max_iters)
+    sc.load(o, residual_tolerance=wl.tol, max_iters=wl.max_iters)
     o.finalize()
     for _ in range(args.warmup):
         o.step(1)
     t = o.time_steps(args.steps)
     v = S * args.steps / t
-    sample = f"{S} of {args.scenes} scenes of the batch, {args.steps} steps, FP64 oracle port, {threads} threads"
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+    sample = f"{what}, {args.steps} steps, FP64 oracle port, {threads} threads"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": wl.unit, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"batch{args.scenes}_cubes", "scenes_timed": S,
-                       "residual_tolerance": args.tol, "max_iters": args.max_iters},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": wl.name, "units_timed": S,
+                       "residual_tolerance": wl.tol, "max_iters": wl.max_iters},
+            "cpu_baseline": {"value": v, "unit": wl.unit, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -176,11 +214,12 @@ def run_engine(args):
     seed = dist.shard_seed(args.seed, rank)
 
     t0 = time.time()
-    sc = scenes.batched_cubes(num_scenes=args.scenes, seed=seed)
+    wl = Workload(args, seed)
+    sc = wl.scene
     e = Context(device=local)
     stream = torch.cuda.Stream(device=local)
     e.set_stream(stream.cuda_stream)
-    sc.load(e, residual_tolerance=args.tol, max_iters=args.max_iters, precision=args.precision)
+    sc.load(e, residual_tolerance=wl.tol, max_iters=wl.max_iters, precision=args.precision)
     e.finalize()
     setup_s = time.time() - t0
     n = sc.num_particles
@@ -195,12 +234,29 @@ def run_engine(args):
     clocks = Clocks(local)
     clocks.start()
     st0 = e.stats()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    e.step(args.steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    if wl.rods:
+        # the rod scene fits in L2: flush it (256 MB write) before every step
+        # and time only the steps
+        flush = torch.empty(64 << 20, dtype=torch.float32, device=torch.device("cuda", local))
+        evs = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e.step(1)
+            b.record(stream)
+            evs.append((a, b))
+        stream.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        del flush
+    else:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
     st1 = e.stats()
     dist.barrier()
     torch.cuda.synchronize()
@@ -232,37 +288,40 @@ def run_engine(args):
     e.synchronize()
 
     ms_max, ms_e2e_max = dist.reduce([ms, ms_e2e], "max", device=torch.device("cuda", local))
-    value = args.scenes * world * args.steps / (ms_max / 1e3)
-    value_e2e = args.scenes * world * args.steps / (ms_e2e_max / 1e3)
+    value = wl.units * world * args.steps / (ms_max / 1e3)
+    value_e2e = wl.units * world * args.steps / (ms_e2e_max / 1e3)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
         per_launch_ms = solve_ms / max(1, solve_launches)
         per_launch_bytes = solve_bytes / max(1, solve_launches)
         achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
-        workload = f"batch{args.scenes}_cubes"
+        workload = wl.name
+        kernel = ("k_solve_rod (per-color 6-DOF vertex block solve)" if wl.rods
+                  else "k_solve_tet (per-color vertex block solve)")
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic_for(workload), "kernel": "k_solve_tet (per-color vertex block solve)",
+                "traffic": traffic_for(workload), "kernel": kernel,
                 "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "peak_source": peak_kind}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = min(os.cpu_count() or 1, 32)
-            v_cpu, S, steps, t = cpu_sample(args, seed, threads)
-            cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{S} of {args.scenes} scenes of the same batch, {steps} steps in {t:.1f} s, "
-                             f"FP64 oracle port"}
+            v_cpu, what, steps, t = cpu_sample(args, wl, seed, threads)
+            cpu = {"value": v_cpu, "unit": wl.unit, "cores": threads, "kind": "port",
+                   "sample": f"{what}, {steps} steps in {t:.1f} s, FP64 oracle port"}
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
-            "config": {"workload": workload, "scenes_per_gpu": args.scenes, "vertices_per_gpu": n,
-                       "tets_per_gpu": sc.num_tets, "residual_tolerance": args.tol, "max_iters": args.max_iters,
-                       "iterations_per_step": iters, "method": "plain AVBD (no warm start)",
+            "config": {"workload": workload, "scenes_per_gpu": wl.units, "vertices_per_gpu": n,
+                       "tets_per_gpu": sc.num_tets, "residual_tolerance": wl.tol, "max_iters": wl.max_iters,
+                       "iterations_per_step": iters, "method": wl.method,
                        "precision": args.precision,
-                       "l2": f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration",
+                       "l2": (f"L2 flushed (256 MB write) before every timed step; {solve_bytes / 2 / 1e6:.1f} MB "
+                              "of solve data per iteration" if wl.rods else
+                              f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration"),
                        "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
             "clocks": clk, "gpu_launches": launches,
-            "e2e": {"value": value_e2e, "unit": UNIT, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n},
+            "e2e": {"value": value_e2e, "unit": wl.unit, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n},
             "roofline": roof, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -1440,6 +1440,13 @@ void orc_get_rotations(void* h, double* out) {
         out[4 * i] = q.w; out[4 * i + 1] = q.x; out[4 * i + 2] = q.y; out[4 * i + 3] = q.z;
     }
 }
+void orc_get_angular_velocities(void* h, double* out) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < c.np(); i++) {
+        V3 w = c.oriented(i) ? c.w[c.rot[i]] : V3();
+        out[3 * i] = w.x; out[3 * i + 1] = w.y; out[3 * i + 2] = w.z;
+    }
+}
 unsigned orc_num_particles(void* h) { return ((Ctx*)h)->np(); }
 
 unsigned orc_neo_hookean_add(void* h, unsigned n, const unsigned* idx, const double* lam, const double* mu,

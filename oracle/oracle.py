@@ -62,6 +62,7 @@ def lib():
             "orc_get_positions": (None, [vp, dp]),
             "orc_get_velocities": (None, [vp, dp]),
             "orc_get_rotations": (None, [vp, dp]),
+            "orc_get_angular_velocities": (None, [vp, dp]),
             "orc_num_particles": (C.c_uint, [vp]),
             "orc_neo_hookean_add": (C.c_uint, [vp, C.c_uint, up, dp, dp, dp, dp, dp]),
             "orc_cosserat_rod_add": (C.c_uint, [vp, C.c_uint, up, dp, dp, dp]),
@@ -268,6 +269,11 @@ class Oracle:
     def rotations(self):
         out = np.zeros((self.num_particles, 4))
         self.L.orc_get_rotations(self.h, _p(out, C.c_double))
+        return out
+
+    def angular_velocities(self):
+        out = np.zeros((self.num_particles, 3))
+        self.L.orc_get_angular_velocities(self.h, _p(out, C.c_double))
         return out
 
     def coloring(self):

@@ -57,3 +57,34 @@ def test_batched_scene_count():
     sc.load(r)
     assert len(r.calls["begin_scene"]) == 4
     assert len(r.calls["add_particles"]) == 5
+
+
+def test_rods_and_spheres_setup():
+    """Rod::Rod set-up (simobject/Rod.cpp:10-68): lumped masses and inertias,
+    Cosserat stiffness, frames advanced by Exp_s3(kappa ds)."""
+    sc = scenes.rods_and_spheres()
+    assert sc.num_particles == 256 * 101 + 64 and sc.num_primitives == 256 * 100
+    sc = scenes.rods_and_spheres(num_rods=2, segments=10, num_spheres=3, length=0.1)
+    r = Recorder()
+    sc.load(r)
+    (X, Q, m, I), = r.calls["add_oriented_particles"][:1]
+    ds, area, Ix = 0.01, np.pi * 0.005 ** 2, np.pi * 0.005 ** 4 / 4
+    me = ds * area * 1000.0
+    assert np.isclose(m[0], me / 2) and np.isclose(m[1], me) and np.isclose(m.sum(), 10 * me)
+    assert np.allclose(I[1], 1000.0 * ds * np.array([Ix, Ix, 2 * Ix]))
+    assert np.allclose(np.linalg.norm(Q, axis=1), 1)
+    assert np.allclose(np.linalg.norm(np.diff(X, axis=0), axis=1), ds)
+    (idx, K, L, kap), = r.calls["add_cosserat_rod"][:1]
+    G = 1e7 / (2 * 1.25)
+    assert np.allclose(K[0], [G * area, G * area, 1e7 * area, 1e7 * Ix, 1e7 * Ix, G * 2 * Ix])
+    # helix: every segment turns by the same angle |kappa| ds
+    rel = [scenes.quat_mul(Q[i] * [1, -1, -1, -1], Q[i + 1]) for i in range(10)]
+    ang = [2 * np.arctan2(np.linalg.norm(q[1:]), q[0]) for q in rel]
+    assert np.allclose(ang, np.linalg.norm(kap[0]) * ds)
+    # spheres: m = 4/3 pi r^3 rho, I = 2/5 m r^2, on or above the ground
+    sph = r.calls["add_oriented_particles"][2:]
+    assert len(sph) == 3
+    for (Xs, Qs, ms, Is) in sph:
+        assert np.isclose(Is[0][0], 0.4 * ms[0] * (ms[0] / (4 / 3 * np.pi * 1000.0)) ** (2 / 3))
+    joints = r.calls["add_one_sided_fixed_joint"]
+    assert len(joints) == 2 and np.allclose(joints[0][3][0], X[0])
