@@ -41,10 +41,16 @@ def active() -> bool:
         return False
 
 
-def barrier():
+def barrier(timeout_s: float | None = None):
+    """Barrier over all ranks.  With `timeout_s` on a gloo group it is a
+    monitored barrier: a rank that left (or never arrives) raises a
+    RuntimeError naming it on rank 0 after `timeout_s`, instead of a hang."""
     if active():
         import torch.distributed as dist
-        dist.barrier()
+        if timeout_s is not None and dist.get_backend() == "gloo":
+            dist.monitored_barrier(timeout=datetime.timedelta(seconds=timeout_s))
+        else:
+            dist.barrier()
 
 
 def reduce(values, op: str = "max", device=None):
