@@ -22,6 +22,8 @@ PRECISION_FP32 = 0
 PRECISION_FP64 = 1
 PRECISION_MIXED = 2
 SHAPE_TRIANGLE, SHAPE_ROD_SEGMENT, SHAPE_SPHERE = 0, 1, 2
+# learned warm start (include/avbd.h): feature rows of 32 BF16, target rows of 4 FP32
+MLP_IN, MLP_IN_PAD, MLP_HIDDEN, MLP_OUT, MLP_OUT_PAD, MLP_NPARAMS = 27, 32, 128, 3, 16, 39312
 
 
 class AvbdError(RuntimeError):
@@ -52,6 +54,7 @@ _dp = C.POINTER(C.c_double)
 _up = C.POINTER(C.c_uint)
 _u8p = C.POINTER(C.c_uint8)
 _u64p = C.POINTER(C.c_uint64)
+_fp = C.POINTER(C.c_float)
 SIGNATURES = {
     "avbd_create": [C.POINTER(_vp), C.c_int, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint],
     "avbd_destroy": [_vp],
@@ -90,6 +93,17 @@ SIGNATURES = {
     "avbd_residual": [_vp, _dp],
     "avbd_profile_solve": [_vp, C.c_uint, _dp, _dp, _up],
     "avbd_lbvh_morton_sort_noalloc": [_vp, C.c_uint, _vp, _vp, _vp],
+    "avbd_gemm_bf16": [_vp, C.c_uint, _vp, C.c_uint, _vp, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, _vp],
+    "avbd_mlp_create": [C.POINTER(_vp), C.c_int, _fp],
+    "avbd_mlp_forward": [_vp, _vp, C.c_uint, _vp, _vp],
+    "avbd_mlp_destroy": [_vp],
+    "avbd_mlp_trainer_create": [C.POINTER(_vp), C.c_int, C.c_uint, _fp],
+    "avbd_mlp_trainer_step": [_vp, _vp, _vp, C.c_float, _fp],
+    "avbd_mlp_trainer_grad": [_vp, _vp, _vp, _fp, _fp],
+    "avbd_mlp_trainer_get_params": [_vp, _fp],
+    "avbd_mlp_trainer_destroy": [_vp],
+    "avbd_set_warmstart": [_vp, C.c_int, _fp],
+    "avbd_warmstart_sample": [_vp, _vp, _vp, _up],
     "avbd_last_error_string": [],
     "avbd_version": [],
 }

@@ -42,6 +42,7 @@ class Context:
         check(self.L.avbd_create(C.byref(h), device, particles_capacity, oriented_capacity, energies_capacity,
                                  primitives_capacity, sdf_capacity))
         self.h = h
+        self.device = device
         self._params = Params(1e-3, 60.0, 9.81, 33.0, 1e-3)
         self._solver = SolverParams(1, 0.5, 0.0, 0, _lib.PRECISION_FP32)
 
@@ -260,6 +261,25 @@ class Context:
         r = C.c_double(0)
         check(self.L.avbd_residual(self.h, C.byref(r)))
         return r.value
+
+    def set_warmstart(self, mode, params=None):
+        """Learned warm start: 0 off (inertial guess), 1 record features and
+        targets every step, 2 apply the MLP `params` (FP32 flat array)."""
+        p = None
+        if params is not None:
+            params = np.ascontiguousarray(params, dtype=np.float32)
+            p = params.ctypes.data_as(C.POINTER(C.c_float))
+        check(self.L.avbd_set_warmstart(self.h, int(mode), p))
+
+    def warmstart_sample(self, features=None, targets=None):
+        """Copies the last recorded step's feature rows (BF16 CUDA tensor
+        [n, 32]) and target rows (FP32 CUDA tensor [n, 4]; column 3 is 1 on
+        solved tet vertices) in internal vertex order; returns n."""
+        rows = C.c_uint(0)
+        f = features.data_ptr() if features is not None else None
+        t = targets.data_ptr() if targets is not None else None
+        check(self.L.avbd_warmstart_sample(self.h, f, t, C.byref(rows)))
+        return rows.value
 
     def profile_solve(self, iterations=2):
         """Kernel time (ms) and algorithmic bytes of the per-color solve launches

@@ -43,6 +43,7 @@ static void trace(const char* what) {
 
 namespace avbd {
 void count_launch(avbd_ctx* c, unsigned k) { c->stats.kernel_launches += k; }
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
 }
 
 // FP64 and mixed keep the particle state in double precision.
@@ -83,6 +84,12 @@ static void free_device(avbd_ctx* c) {
     c->d_scene_mg2 = nullptr;
     c->d_scene_iters = nullptr;
     c->d_tol_count = nullptr;
+    mlp_device_free(c->ws_mlp);
+    c->ws_mlp = nullptr;
+    c->d_ws_feat = c->d_ws_x0 = nullptr;
+    c->d_ws_target = nullptr;
+    c->ws_mode = 0;
+    c->ws_recorded = false;
     c->finalized = false;
     c->graph_dirty = true;
 }
@@ -921,6 +928,17 @@ void enqueue_begin(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_
     if (c->damping) launch_tet_eprev<R>(c, s, k, st);
     launch_begin_step<R>(c, s, k, st);
     launch_begin_step_rot<R>(c, s, k, st);
+    if (c->ws_mode) {
+        // learned warm start: features at the inertial guess x0, then either
+        // x0 += s MLP(features) or (recording) a copy of x0 for the targets
+        launch_features<R>(c, s, k, c->d_ws_feat, st);
+        if (c->ws_mode == 2) {
+            mlp_apply_state<R>(*c->ws_mlp, c->d_ws_feat, s.n, s.x, s.xl, s.xll, s.flags, k.g * k.dt * k.dt, st);
+            count_launch(c);
+        } else {
+            launch_ws_save<R>(c, s, c->d_ws_x0, st);
+        }
+    }
 }
 
 // One Gauss-Seidel sweep: per color, the positional (3-DOF) slab then the
@@ -947,6 +965,10 @@ template <typename R>
 void enqueue_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
     launch_velocity<R>(c, s, k, st);
     launch_velocity_rot<R>(c, s, k, st);
+    if (c->ws_mode == 1) {  // recording: target (x_end - x0) / (g h^2)
+        launch_ws_target<R>(c, s, c->d_ws_x0, 1.0 / (k.g * k.dt * k.dt), c->d_ws_target, st);
+        c->ws_recorded = true;
+    }
 }
 
 // Residual pass over all particles (positional and oriented blocks).
@@ -1117,6 +1139,7 @@ int device_error(avbd_ctx* c) {
     if (h == AVBD_ERR_NAN) return fail(h, "non-finite particle state");
     if (h == AVBD_ERR_UNSUPPORTED_PAIR) return fail(h, "Unsupported collision!");
     if (h) return fail(h, "device-side error");
+    if (c->ws_mlp) return mlp_device_error(c->ws_mlp, c->stream);
     return AVBD_OK;
 }
 
@@ -1384,6 +1407,50 @@ int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, doubl
     if (solve_ms) *solve_ms = ms;
     if (solve_bytes) *solve_bytes = bytes;
     if (launches) *launches = nl;
+    return device_error(c);
+}
+
+int avbd_set_warmstart(avbd_ctx* c, int mode, const float* params) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (mode < 0 || mode > 2) return fail(AVBD_ERR_INVALID_ARG, "warm-start mode must be 0, 1 or 2");
+    if (mode == 2 && !params) return fail(AVBD_ERR_INVALID_ARG, "mode 2 needs the MLP parameters");
+    if (mode == 2 && !(c->params.g_accel > 0)) return fail(AVBD_ERR_UNSUPPORTED, "the warm start needs g > 0");
+    const size_t n = c->mass.size();
+    if (mode && !c->d_ws_feat) {
+        const size_t v4 = use64(c) ? sizeof(double4a) : sizeof(float4);
+        uint8_t *f = nullptr, *x0 = nullptr;
+        float4* t = nullptr;
+        if (int rc = dalloc(c, &f, 64 * n)) return rc;
+        if (int rc = dalloc(c, &x0, v4 * n)) return rc;
+        if (int rc = dalloc(c, &t, n)) return rc;
+        CUDA_OR_FAIL(cudaMemsetAsync(f, 0, 64 * n, c->stream));
+        CUDA_OR_FAIL(cudaMemsetAsync(t, 0, sizeof(float4) * n, c->stream));
+        c->d_ws_feat = f;
+        c->d_ws_x0 = x0;
+        c->d_ws_target = reinterpret_cast<float*>(t);
+    }
+    if (mode == 2)
+        if (int rc = mlp_device_upload(&c->ws_mlp, c->device, params, c->stream)) return rc;
+    c->ws_mode = mode;
+    c->ws_recorded = false;
+    c->graph_dirty = true;
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return AVBD_OK;
+}
+
+int avbd_warmstart_sample(avbd_ctx* c, void* features, float* targets, unsigned* rows) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (rows) *rows = (unsigned)c->mass.size();
+    if (!features && !targets) return AVBD_OK;
+    if (!c->ws_recorded) return fail(AVBD_ERR_STATE, "no recorded step (set warm-start mode 1 and step)");
+    const size_t n = c->mass.size();
+    if (features)
+        CUDA_OR_FAIL(cudaMemcpyAsync(features, c->d_ws_feat, 64 * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (targets)
+        CUDA_OR_FAIL(cudaMemcpyAsync(targets, c->d_ws_target, 16 * n, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
     return device_error(c);
 }
 

@@ -100,6 +100,8 @@ enum OrientedFlags : uint8_t {
 
 // Per-scene run-to-tolerance state passed to the solve, Chebyshev and residual
 // kernels.  Null pointers disable the corresponding behaviour.
+struct MlpDevice;  // learned warm-start weights on the device (mlp.cu)
+
 struct SceneTol {
     const uint32_t* scene = nullptr;  // scene of each internal vertex
     const uint8_t* active = nullptr;  // solve / update only vertices of these scenes
@@ -223,11 +225,35 @@ struct avbd_ctx {
     int lanes = 8;                      // threads per vertex in the tet solve
     int block = 256;
 
+    // learned warm start (mlp.cu): 0 off, 1 record features/targets, 2 apply
+    int ws_mode = 0;
+    avbd::MlpDevice* ws_mlp = nullptr;
+    void* d_ws_feat = nullptr;          // BF16 [n][32]
+    void* d_ws_x0 = nullptr;            // warm-start positions of the last step (state type)
+    float* d_ws_target = nullptr;       // FP32 [n][4]
+    bool ws_recorded = false;
+
     avbd_stats stats{};
     std::vector<void*> allocations;
 };
 
 namespace avbd {
+
+// ---- learned warm start (mlp.cu)
+int mlp_device_upload(MlpDevice** m, int device, const float* params, cudaStream_t st);
+void mlp_device_free(MlpDevice* m);
+int mlp_device_error(const MlpDevice* m, cudaStream_t st);
+// x0 += scale * MLP(features) for every internal vertex that is neither fixed nor oriented
+template <typename P>
+int mlp_apply_state(const MlpDevice& m, const void* feat, unsigned n, typename Vec4Of<P>::T* x,
+                    typename Vec4Of<P>::T* xl, typename Vec4Of<P>::T* xll, const uint8_t* flags, double scale,
+                    cudaStream_t st);
+template <typename R>
+void launch_features(avbd_ctx* c, DevState<R>& s, const StepConsts& k, void* feat, cudaStream_t st);
+template <typename R>
+void launch_ws_save(avbd_ctx* c, DevState<R>& s, void* x0, cudaStream_t st);
+template <typename R>
+void launch_ws_target(avbd_ctx* c, DevState<R>& s, const void* x0, double inv_s, float* t, cudaStream_t st);
 
 // ---- solve kernels (solve.cu)
 template <typename R>
@@ -283,5 +309,7 @@ void lbvh_stage(avbd_ctx* c, DevState<R>& s, cudaStream_t st);
 
 // counts launches for the stats
 void count_launch(avbd_ctx* c, unsigned k = 1);
+// records the message returned by avbd_last_error_string and returns code
+int set_error(int code, const std::string& msg);
 
 }  // namespace avbd

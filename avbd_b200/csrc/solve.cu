@@ -14,6 +14,8 @@
 //   NeoHookeanEnergySolver::updateAfterTimeStep  energy/elastic/NeoHookeanEnergySolver.hpp:70-90
 //   CollisionConstraintEnergySolver (ground)     energy/collision/CollisionConstraintEnergySolver.hpp:60-285
 //   GroundCollisionEnergySolver                  energy/collision/GroundCollisionEnergySolver.hpp:14-91
+#include <cuda_bf16.h>
+
 #include "engine.h"
 
 namespace avbd {
@@ -273,13 +275,14 @@ AVBD_D void reduce_block(Block3<P, HT>& B) {
     }
 }
 
-enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2 };
+enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2, MODE_FEATURES = 3 };
 
 // Vertex block solve of one color slab: LANES threads per vertex stream the
 // vertex's incidence records, each lane accumulating its tets, then a shuffle
 // reduction and the 3x3 solve by the group's first lane.  MODE_RESIDUAL
 // evaluates |m/h^2 (x-y) + grad| instead of updating; MODE_DEBUG exports the
-// accumulated block.
+// accumulated block; MODE_FEATURES writes the learned warm start's 32 BF16
+// input features of the vertex (row p of `out`) at the current iterate.
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE>
 __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
@@ -296,6 +299,8 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
     if (MODE == MODE_RESIDUAL && T.cand && active && !T.cand[T.scene[p]]) active = false;
     Block3<P, HT> B;
     V3<P> xi = mk3<P>(0, 0, 0);
+    // MODE_FEATURES: sum of the other vertices' velocities and of mu/lambda over the incident tets
+    float fv0 = 0.f, fv1 = 0.f, fv2 = 0.f, fmol = 0.f, fcnt = 0.f;
     if (active) {
         xi = xyz(s.x[p]);
         unsigned b = s.inc_begin[p], e = s.inc_begin[p + 1];
@@ -308,11 +313,32 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
             IncRec<RS> rn;
             if (kn < e) rn = load_rec<RS>(inc + kn);
             accumulate_tet<P, RS, HT, DAMP>(s, r, xi, c.dt, B);
+            if constexpr (MODE == MODE_FEATURES) {
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    typename Vec4Of<P>::T vo = s.v[r.o[j]];
+                    fv0 += (float)vo.x;
+                    fv1 += (float)vo.y;
+                    fv2 += (float)vo.z;
+                }
+                fmol += (float)r.mol;
+                fcnt += 1.f;
+            }
             r = rn;
             k = kn;
         }
     }
     reduce_block<LANES>(B);
+    if constexpr (MODE == MODE_FEATURES) {
+#pragma unroll
+        for (int m = LANES / 2; m >= 1; m >>= 1) {
+            fv0 += shfl_xor(fv0, m);
+            fv1 += shfl_xor(fv1, m);
+            fv2 += shfl_xor(fv2, m);
+            fmol += shfl_xor(fmol, m);
+            fcnt += shfl_xor(fcnt, m);
+        }
+    }
     if (!active || lane != 0) {
         if constexpr (MODE == MODE_RESIDUAL) {
             // keep the warp reduction below well defined
@@ -348,6 +374,50 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
             }
             typename Vec4Of<P>::T o = make4<P>(xi + dx, P(0));
             s.x[p] = o;
+        } else if constexpr (MODE == MODE_FEATURES) {
+            // feature layout of avbd_warmstart_sample (include/avbd.h)
+            Sym3<P> A{cm + (P)B.h00, cm + (P)B.h11, cm + (P)B.h22, (P)B.h01, (P)B.h02, (P)B.h12};
+            V3<P> rhs = mk3<P>(-cm * d.x - B.g0, -cm * d.y - B.g1, -cm * d.z - B.g2);
+            V3<P> dx;
+            solve_sym3<P>(A, rhs, dx);
+            const float sc = 1.0f / (float)(c.g * c.dt * c.dt);
+            const float h = (float)c.dt, icm = 1.0f / (float)cm;
+            typename Vec4Of<P>::T v4 = s.v[p], vp4 = s.vp[p];
+            const float inv3n = fcnt > 0.f ? 1.0f / (3.0f * fcnt) : 0.f;
+            float f[32];
+            f[0] = (float)d.x * sc; f[1] = (float)d.y * sc; f[2] = (float)d.z * sc;
+            f[3] = (float)v4.x * h * sc; f[4] = (float)v4.y * h * sc; f[5] = (float)v4.z * h * sc;
+            f[6] = (float)vp4.x * h * sc; f[7] = (float)vp4.y * h * sc; f[8] = (float)vp4.z * h * sc;
+            f[9] = fcnt > 0.f ? (fv0 * inv3n - (float)v4.x) * h * sc : 0.f;
+            f[10] = fcnt > 0.f ? (fv1 * inv3n - (float)v4.y) * h * sc : 0.f;
+            f[11] = fcnt > 0.f ? (fv2 * inv3n - (float)v4.z) * h * sc : 0.f;
+            f[12] = (float)rhs.x * icm * sc; f[13] = (float)rhs.y * icm * sc; f[14] = (float)rhs.z * icm * sc;
+            f[15] = (float)dx.x * sc; f[16] = (float)dx.y * sc; f[17] = (float)dx.z * sc;
+            f[18] = log1pf(fmaxf(0.f, (float)B.h00 * icm));
+            f[19] = log1pf(fmaxf(0.f, (float)B.h11 * icm));
+            f[20] = log1pf(fmaxf(0.f, (float)B.h22 * icm));
+            f[21] = fcnt > 0.f ? fmol / fcnt : 0.f;
+            f[22] = log10f((float)m) + 3.0f;
+            f[23] = tanhf((float)xi.y * sc * 0.1f);
+            f[24] = (GROUND && (fl & VF_GROUND)) ? (float)s.glam[p].x * icm * sc : 0.f;
+            f[25] = fcnt * (1.0f / 24.0f);
+            f[26] = tanhf((float)y4.y * sc);
+#pragma unroll
+            for (int j = 27; j < 32; j++) f[j] = 0.f;
+            uint32_t w[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                float a = fminf(fmaxf(f[2 * j], -1e4f), 1e4f), b = fminf(fmaxf(f[2 * j + 1], -1e4f), 1e4f);
+                if (!(a == a)) a = 0.f;  // a NaN feature becomes 0
+                if (!(b == b)) b = 0.f;
+                __nv_bfloat162 hb = __floats2bfloat162_rn(a, b);
+                w[j] = *reinterpret_cast<uint32_t*>(&hb);
+            }
+            uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(out) + (size_t)p * 64);
+            dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+            dst[2] = make_uint4(w[8], w[9], w[10], w[11]);
+            dst[3] = make_uint4(w[12], w[13], w[14], w[15]);
         } else if constexpr (MODE == MODE_RESIDUAL) {
             double u0 = (double)cm * (double)d.x + (double)B.g0;
             double u1 = (double)cm * (double)d.y + (double)B.g1;
@@ -668,6 +738,46 @@ void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsign
     solve_lanes<MODE_DEBUG>(c, s, k, p, 1, st, out, SceneTol());
 }
 
+// warm-start features of every solved tet vertex at the current iterate,
+// one 64-byte BF16 row per internal vertex
+template <typename R>
+void launch_features(avbd_ctx* c, DevState<R>& s, const StepConsts& k, void* feat, cudaStream_t st) {
+    solve_lanes<MODE_FEATURES>(c, s, k, 0, s.n, st, reinterpret_cast<double*>(feat), SceneTol());
+}
+
+// copy of the solved vertices' warm-start positions (x0)
+template <typename R>
+__global__ void k_ws_save(const DevState<R> s, typename Vec4Of<R>::T* x0) {
+    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < s.n) x0[p] = s.x[p];
+}
+
+// target row (x_end - x0) / s, column 3 = 1 for solved tet vertices, else 0
+template <typename R>
+__global__ void k_ws_target(const DevState<R> s, const typename Vec4Of<R>::T* x0, float inv_s, float4* t) {
+    unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s.n) return;
+    if (s.flags[p] & (VF_FIXED | VF_ORIENTED)) {
+        t[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    typename Vec4Of<R>::T a = s.x[p], b = x0[p];
+    t[p] = make_float4((float)(a.x - b.x) * inv_s, (float)(a.y - b.y) * inv_s, (float)(a.z - b.z) * inv_s, 1.f);
+}
+
+template <typename R>
+void launch_ws_save(avbd_ctx* c, DevState<R>& s, void* x0, cudaStream_t st) {
+    k_ws_save<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, reinterpret_cast<typename Vec4Of<R>::T*>(x0));
+    count_launch(c);
+}
+
+template <typename R>
+void launch_ws_target(avbd_ctx* c, DevState<R>& s, const void* x0, double inv_s, float* t, cudaStream_t st) {
+    k_ws_target<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, reinterpret_cast<const typename Vec4Of<R>::T*>(x0),
+                                                       (float)inv_s, reinterpret_cast<float4*>(t));
+    count_launch(c);
+}
+
 template <typename R>
 void launch_load_positions(DevState<R>& s, const double* src, const uint32_t* inv_map, unsigned first, unsigned n,
                            int mode, cudaStream_t st) {
@@ -694,6 +804,9 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
                                      const SceneTol&);                                                          \
     template void launch_debug_block<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, double*,          \
                                         cudaStream_t);                                                          \
+    template void launch_features<R>(avbd_ctx*, DevState<R>&, const StepConsts&, void*, cudaStream_t);          \
+    template void launch_ws_save<R>(avbd_ctx*, DevState<R>&, void*, cudaStream_t);                               \
+    template void launch_ws_target<R>(avbd_ctx*, DevState<R>&, const void*, double, float*, cudaStream_t);       \
     template void launch_load_positions<R>(DevState<R>&, const double*, const uint32_t*, unsigned, unsigned, int, \
                                            cudaStream_t);                                                       \
     template void launch_store_vec<R>(const DevState<R>&, int, double*, const uint32_t*, unsigned, cudaStream_t);

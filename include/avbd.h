@@ -292,6 +292,83 @@ AVBD_API int avbd_lbvh_morton_sort_noalloc(const double* aabb6, unsigned n, uint
 AVBD_API int avbd_profile_solve(avbd_ctx* ctx, unsigned iterations, double* solve_ms, double* solve_bytes,
                                 unsigned* launches);
 
+/* ------------------------------------------------ learned warm start
+ * No counterpart in the reference (it has no learned component).  A
+ * per-vertex MLP 27 -> 128 -> 128 -> 128 -> 3 with SiLU, BF16 weights and
+ * activations, FP32 accumulation (tcgen05.mma), predicts the correction of
+ * the inertial initial guess of every solved tet vertex at the start of a
+ * step: x0 <- x0 + s * f(features), s = g h^2.  Parameters travel as one FP32
+ * array of AVBD_MLP_NPARAMS values, PyTorch Linear layout ([out][in],
+ * row-major) with padded shapes:
+ *   W1 [128][32]  at 0        (inputs 27..31 are zero padding)
+ *   b1 [128]      at 4096
+ *   W2 [128][128] at 4224,    b2 [128] at 20608
+ *   W3 [128][128] at 20736,   b3 [128] at 37120
+ *   W4 [16][128]  at 37248    (outputs 3..15 are zero padding)
+ *   b4 [16]       at 39296
+ * Feature rows are 32 BF16 values (27 used, the layout is listed with
+ * avbd_warmstart_sample); target rows are 4 FP32 values (3 used). */
+#define AVBD_MLP_IN 27
+#define AVBD_MLP_IN_PAD 32
+#define AVBD_MLP_HIDDEN 128
+#define AVBD_MLP_OUT 3
+#define AVBD_MLP_OUT_PAD 16
+#define AVBD_MLP_NPARAMS 39312u
+
+/* D = A B^T on the tensor cores: A [M x K] and B [N x K] row-major BF16 device
+ * arrays (lda, ldb in elements, multiples of 8; K a multiple of 16), C [M x N]
+ * FP32 (ldc in elements).  accumulate != 0 adds to C.  stream: cudaStream_t. */
+AVBD_API int avbd_gemm_bf16(const void* A, unsigned lda, const void* B, unsigned ldb, float* C, unsigned ldc,
+                            unsigned M, unsigned N, unsigned K, int accumulate, void* stream);
+
+/* Inference of the MLP on n feature rows (device, BF16 [n][32]) into out
+ * (device, FP32 [n][16], columns 3..15 are the zero padding). */
+typedef struct avbd_mlp avbd_mlp;
+AVBD_API int avbd_mlp_create(avbd_mlp** out, int device, const float* params);
+AVBD_API int avbd_mlp_forward(avbd_mlp* m, const void* features, unsigned n, float* out, void* stream);
+AVBD_API int avbd_mlp_destroy(avbd_mlp* m);
+
+/* Training: mini-batches of `batch` rows (a multiple of 128) of device
+ * features (BF16 [batch][32]) and targets (FP32 [batch][4]); loss = mean
+ * squared error over the 3 outputs; Adam (beta1 0.9, beta2 0.999, eps 1e-8)
+ * on FP32 master weights.  avbd_mlp_trainer_grad evaluates the loss and the
+ * gradient (host FP32 [AVBD_MLP_NPARAMS]) without updating. */
+typedef struct avbd_mlp_trainer avbd_mlp_trainer;
+AVBD_API int avbd_mlp_trainer_create(avbd_mlp_trainer** out, int device, unsigned batch, const float* params);
+AVBD_API int avbd_mlp_trainer_step(avbd_mlp_trainer* t, const void* features, const float* targets, float lr,
+                                   float* loss);
+AVBD_API int avbd_mlp_trainer_grad(avbd_mlp_trainer* t, const void* features, const float* targets, float* loss,
+                                   float* grad);
+AVBD_API int avbd_mlp_trainer_get_params(avbd_mlp_trainer* t, float* params);
+AVBD_API int avbd_mlp_trainer_destroy(avbd_mlp_trainer* t);
+
+/* Warm start of a context (after avbd_finalize; tet vertices only):
+ *   mode 0  off (the adaptive inertial guess of VBDSolver.hpp:208-248);
+ *   mode 1  record: every step stores the features of each solved tet vertex
+ *           at the inertial guess x0 and, after the step, the target
+ *           (x_end - x0) / s, for avbd_warmstart_sample;
+ *   mode 2  apply: x0 <- x0 + s * MLP(features) before the iterations.
+ * params (mode 2): AVBD_MLP_NPARAMS floats, with any input normalisation
+ * folded into W1/b1 and the output scale folded into W4/b4. */
+AVBD_API int avbd_set_warmstart(avbd_ctx* ctx, int mode, const float* params);
+
+/* Features and targets of the last recorded step, one row per solved tet
+ * vertex (*rows of them, internal order), into caller device buffers
+ * (features BF16 [rows][32], targets FP32 [rows][4]; either may be NULL to
+ * query *rows).  Feature layout, displacements in units of s = g h^2:
+ *   0-2   x0 - y                      (inertial guess minus inertial target)
+ *   3-5   v h,  6-8 v_prev h          (last two step displacements)
+ *   9-11  (mean over incident tets of the other vertices' v - v) h
+ *   12-14 block RHS h^2 / m = -(x0 - y) - grad E(x0) h^2 / m
+ *   15-17 block Newton step A^-1 RHS  (A = m/h^2 I + H(x0))
+ *   18-20 log(1 + diag H(x0) h^2 / m)
+ *   21    mean mu/lambda of the incident tets
+ *   22    log10(m) + 3
+ *   23    tanh(x0_y / 10),  26 tanh(y_y)   (height above the ground)
+ *   24    ground normal multiplier lambda_n h^2 / (m s)
+ *   25    incident tet count / 24 */
+AVBD_API int avbd_warmstart_sample(avbd_ctx* ctx, void* features, float* targets, unsigned* rows);
+
 AVBD_API const char* avbd_last_error_string(void);
 AVBD_API const char* avbd_version(void);
 
