@@ -45,7 +45,8 @@ class SolverParams(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_ulonglong), ("iterations", C.c_ulonglong), ("fp64_fallbacks", C.c_ulonglong),
                 ("candidate_pairs", C.c_ulonglong), ("last_residual", C.c_double), ("num_colors", C.c_uint),
-                ("num_scenes", C.c_uint)]
+                ("num_scenes", C.c_uint), ("capped_scene_steps", C.c_ulonglong),
+                ("warmstart_applied", C.c_ulonglong)]
 
 
 # name -> argtypes (all return int unless listed in _RESTYPE)

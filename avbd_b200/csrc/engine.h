@@ -230,7 +230,9 @@ struct avbd_ctx {
     avbd::MlpDevice* ws_mlp = nullptr;
     void* d_ws_feat = nullptr;          // BF16 [n][32]
     void* d_ws_x0 = nullptr;            // warm-start positions of the last step (state type)
-    float* d_ws_target = nullptr;       // FP32 [n][4]
+    float* d_ws_target = nullptr;       // FP32 [n][4]: (x_end - x0) / s of the last step
+    const float* ws_prev_arg = nullptr; // previous-correction rows for the features launch in flight
+    float ws_kappa = 0.5f;              // relative error assumed by the acceptance test
     bool ws_recorded = false;
 
     avbd_stats stats{};
@@ -247,9 +249,10 @@ int mlp_device_error(const MlpDevice* m, cudaStream_t st);
 template <typename P>
 int mlp_apply_state(const MlpDevice& m, const void* feat, unsigned n, typename Vec4Of<P>::T* x,
                     typename Vec4Of<P>::T* xl, typename Vec4Of<P>::T* xll, const uint8_t* flags, double scale,
-                    cudaStream_t st);
+                    float kappa, unsigned long long* applied, cudaStream_t st);
 template <typename R>
-void launch_features(avbd_ctx* c, DevState<R>& s, const StepConsts& k, void* feat, cudaStream_t st);
+void launch_features(avbd_ctx* c, DevState<R>& s, const StepConsts& k, void* feat, const float* prev,
+                     cudaStream_t st);
 template <typename R>
 void launch_ws_save(avbd_ctx* c, DevState<R>& s, void* x0, cudaStream_t st);
 template <typename R>

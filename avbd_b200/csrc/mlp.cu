@@ -190,6 +190,8 @@ struct MlpSink {
     typename Vec4Of<P>::T *x, *xl, *xll;
     const uint8_t* flags;  // row = internal vertex; fixed and oriented vertices are skipped
     P scale;
+    float kappa;           // relative error assumed by the acceptance test
+    unsigned long long* applied;  // count of accepted corrections (may be null)
 };
 
 constexpr unsigned SM_W1 = 0, SM_W2 = 8192, SM_W3 = 40960, SM_W4 = 73728, SM_X = 77824, SM_H = 86016,
@@ -211,6 +213,24 @@ AVBD_D void epilogue_hidden(uint32_t tacc, const float* bias, uint8_t* H, unsign
         *reinterpret_cast<uint4*>(H + (c / 8) * (128 * 16) + r * 16) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
         *reinterpret_cast<uint4*>(H + (c / 8 + 1) * (128 * 16) + r * 16) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
     }
+}
+
+// Acceptance of the correction y (in units of s = g h^2) of one vertex.  The
+// block residual at the inertial guess is r0 = |features 12-14| (units of
+// m g, L1).  Applying y with a relative error kappa leaves a residual of
+// about kappa * sum_a (1 + H_aa h^2 / m) |y_a| (features 18-20 hold
+// log(1 + H_aa h^2 / m)), so the correction is applied only where it removes
+// more residual than its error adds, and never below 1e-4 m g (a vertex in
+// free flight, where the inertial guess is exact up to rounding).
+constexpr float WS_GATE = 1e-4f;
+AVBD_D bool accept(const uint8_t* Xs, unsigned r, const float* y, float kappa) {
+    const bf16* f = reinterpret_cast<const bf16*>(Xs + tc::kmaj_off(r, 12, 128));
+    const bf16* h = reinterpret_cast<const bf16*>(Xs + tc::kmaj_off(r, 16, 128));  // features 16..23
+    const float r0 = fabsf(__bfloat162float(f[0])) + fabsf(__bfloat162float(f[1])) + fabsf(__bfloat162float(f[2]));
+    const float added = kappa * (__expf(__bfloat162float(h[2])) * fabsf(y[0]) +
+                                 __expf(__bfloat162float(h[3])) * fabsf(y[1]) +
+                                 __expf(__bfloat162float(h[4])) * fabsf(y[2]));
+    return r0 > WS_GATE && r0 > added;
 }
 
 // Persistent: one CTA per SM, weights resident in shared memory, 128 feature
@@ -307,14 +327,17 @@ __global__ void __launch_bounds__(256, 1) k_mlp_apply(MlpW w, const bf16* __rest
 #pragma unroll
                     for (int j = 0; j < 16; j++) sink.out[(size_t)row * OUT + j] = v[j] + b4[j];
                 } else if (!(sink.flags[row] & (VF_FIXED | VF_ORIENTED))) {
-                    const unsigned p = row;
-                    typename Vec4Of<P>::T x4 = sink.x[p];
-                    x4.x += sink.scale * (P)(v[0] + b4[0]);
-                    x4.y += sink.scale * (P)(v[1] + b4[1]);
-                    x4.z += sink.scale * (P)(v[2] + b4[2]);
-                    sink.x[p] = x4;
-                    sink.xl[p] = x4;
-                    sink.xll[p] = x4;
+                    const float y[3] = {v[0] + b4[0], v[1] + b4[1], v[2] + b4[2]};
+                    if (accept(Xs, warp * 32 + lane, y, sink.kappa)) {
+                        if (sink.applied) atomicAdd(sink.applied, 1ull);
+                        typename Vec4Of<P>::T x4 = sink.x[row];
+                        x4.x += sink.scale * (P)y[0];
+                        x4.y += sink.scale * (P)y[1];
+                        x4.z += sink.scale * (P)y[2];
+                        sink.x[row] = x4;
+                        sink.xl[row] = x4;
+                        sink.xll[row] = x4;
+                    }
                 }
             }
         }
@@ -523,14 +546,14 @@ static int mlp_launch(const MlpDevice& m, const bf16* feat, unsigned n, const Ml
 template <typename P>
 int mlp_apply_state(const MlpDevice& m, const void* feat, unsigned n, typename Vec4Of<P>::T* x,
                     typename Vec4Of<P>::T* xl, typename Vec4Of<P>::T* xll, const uint8_t* flags, double scale,
-                    cudaStream_t st) {
-    MlpSink<P> s{nullptr, x, xl, xll, flags, (P)scale};
+                    float kappa, unsigned long long* applied, cudaStream_t st) {
+    MlpSink<P> s{nullptr, x, xl, xll, flags, (P)scale, kappa, applied};
     return mlp_launch<P>(m, (const bf16*)feat, n, s, st);
 }
 template int mlp_apply_state<float>(const MlpDevice&, const void*, unsigned, float4*, float4*, float4*,
-                                    const uint8_t*, double, cudaStream_t);
+                                    const uint8_t*, double, float, unsigned long long*, cudaStream_t);
 template int mlp_apply_state<double>(const MlpDevice&, const void*, unsigned, double4a*, double4a*, double4a*,
-                                     const uint8_t*, double, cudaStream_t);
+                                     const uint8_t*, double, float, unsigned long long*, cudaStream_t);
 
 int mlp_device_upload(MlpDevice** m, int device, const float* params, cudaStream_t st) {
     if (!*m) {
@@ -619,7 +642,7 @@ int avbd_mlp_forward(avbd_mlp* m, const void* features, unsigned n, float* out, 
     if (!m || !features || !out) return set_error(AVBD_ERR_INVALID_ARG, "null argument");
     if ((uintptr_t)features & 15) return set_error(AVBD_ERR_INVALID_ARG, "features must be 16-byte aligned");
     cudaStream_t st = stream ? (cudaStream_t)stream : m->st;
-    MlpSink<float> s{out, nullptr, nullptr, nullptr, nullptr, 0.f};
+    MlpSink<float> s{out, nullptr, nullptr, nullptr, nullptr, 0.f, 0.f, nullptr};
     if (int rc = mlp_launch<float>(*m->m, (const bf16*)features, n, s, st)) return rc;
     return mlp_device_error(m->m, st);
 }

@@ -286,7 +286,8 @@ enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2, MODE_FEATURES = 3 };
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE>
 __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
-                                                   unsigned long long* counters, double* out, SceneTol T) {
+                                                   unsigned long long* counters, double* out, SceneTol T,
+                                                   const float4* __restrict__ aux) {
     unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned gi = tid / LANES;
     unsigned lane = tid % LANES;
@@ -382,12 +383,15 @@ __global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<R
             solve_sym3<P>(A, rhs, dx);
             const float sc = 1.0f / (float)(c.g * c.dt * c.dt);
             const float h = (float)c.dt, icm = 1.0f / (float)cm;
-            typename Vec4Of<P>::T v4 = s.v[p], vp4 = s.vp[p];
+            typename Vec4Of<P>::T v4 = s.v[p];
+            const float4* prev = aux;  // MODE_FEATURES: previous-correction rows (may be null)
             const float inv3n = fcnt > 0.f ? 1.0f / (3.0f * fcnt) : 0.f;
             float f[32];
             f[0] = (float)d.x * sc; f[1] = (float)d.y * sc; f[2] = (float)d.z * sc;
             f[3] = (float)v4.x * h * sc; f[4] = (float)v4.y * h * sc; f[5] = (float)v4.z * h * sc;
-            f[6] = (float)vp4.x * h * sc; f[7] = (float)vp4.y * h * sc; f[8] = (float)vp4.z * h * sc;
+            // the previous step's converged correction (x_end - x0) / s, kept by k_ws_target
+            const float4 pc = prev ? prev[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+            f[6] = pc.x; f[7] = pc.y; f[8] = pc.z;
             f[9] = fcnt > 0.f ? (fv0 * inv3n - (float)v4.x) * h * sc : 0.f;
             f[10] = fcnt > 0.f ? (fv1 * inv3n - (float)v4.y) * h * sc : 0.f;
             f[11] = fcnt > 0.f ? (fv2 * inv3n - (float)v4.z) * h * sc : 0.f;
@@ -581,14 +585,15 @@ static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, c
     bool damp = c->damping, ground = !c->ground.empty();
     auto kc = mkc<P>(k);
     auto* ctr = c->d_counters;
+    const float4* aux = reinterpret_cast<const float4*>(c->ws_prev_arg);
     if (damp && ground)
-        k_solve_tet<P, RS, HT, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
+        k_solve_tet<P, RS, HT, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
     else if (damp)
-        k_solve_tet<P, RS, HT, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
+        k_solve_tet<P, RS, HT, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
     else if (ground)
-        k_solve_tet<P, RS, HT, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
+        k_solve_tet<P, RS, HT, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
     else
-        k_solve_tet<P, RS, HT, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T);
+        k_solve_tet<P, RS, HT, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
     count_launch(c);
 }
 
@@ -696,13 +701,18 @@ __global__ void k_tol_decide_b(uint8_t* active, uint8_t* cand, double* ex, const
     unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     if (active[s]) {
+        bool done = false;
         if (cand[s]) {
             double R = scene_R(ex[s], m2[s] * g2);
             atomicMax(maxr, ord_enc64(R));
-            if (R <= tol) active[s] = 0;
+            done = R <= tol;
         }
-        if (iters[s] >= max_it) active[s] = 0;
-        if (active[s]) atomicAdd(n_active, 1);
+        if (!done && iters[s] >= max_it) {  // stopped at the cap, unconverged
+            done = true;
+            atomicAdd(maxr + 1, 1ull);
+        }
+        if (done) active[s] = 0;
+        else atomicAdd(n_active, 1);
     }
     cand[s] = 0;
     ex[s] = 0;
@@ -741,8 +751,11 @@ void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsign
 // warm-start features of every solved tet vertex at the current iterate,
 // one 64-byte BF16 row per internal vertex
 template <typename R>
-void launch_features(avbd_ctx* c, DevState<R>& s, const StepConsts& k, void* feat, cudaStream_t st) {
+void launch_features(avbd_ctx* c, DevState<R>& s, const StepConsts& k, void* feat, const float* prev,
+                     cudaStream_t st) {
+    c->ws_prev_arg = prev;
     solve_lanes<MODE_FEATURES>(c, s, k, 0, s.n, st, reinterpret_cast<double*>(feat), SceneTol());
+    c->ws_prev_arg = nullptr;
 }
 
 // copy of the solved vertices' warm-start positions (x0)
@@ -804,7 +817,8 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
                                      const SceneTol&);                                                          \
     template void launch_debug_block<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, double*,          \
                                         cudaStream_t);                                                          \
-    template void launch_features<R>(avbd_ctx*, DevState<R>&, const StepConsts&, void*, cudaStream_t);          \
+    template void launch_features<R>(avbd_ctx*, DevState<R>&, const StepConsts&, void*, const float*,           \
+                                     cudaStream_t);                                                             \
     template void launch_ws_save<R>(avbd_ctx*, DevState<R>&, void*, cudaStream_t);                               \
     template void launch_ws_target<R>(avbd_ctx*, DevState<R>&, const void*, double, float*, cudaStream_t);       \
     template void launch_load_positions<R>(DevState<R>&, const double*, const uint32_t*, unsigned, unsigned, int, \

@@ -31,8 +31,11 @@ IN, IN_PAD, HID, OUT, OUT_PAD, NPARAMS = (_lib.MLP_IN, _lib.MLP_IN_PAD, _lib.MLP
 # name -> (offset, shape) in the flat parameter array
 LAYOUT = {"W1": (0, (HID, IN_PAD)), "b1": (4096, (HID,)), "W2": (4224, (HID, HID)), "b2": (20608, (HID,)),
           "W3": (20736, (HID, HID)), "b3": (37120, (HID,)), "W4": (37248, (OUT_PAD, HID)), "b4": (39296, (OUT_PAD,))}
+# the applied correction is gated off where the block residual at the
+# inertial guess is below GATE m g (L1 of features 12-14), as in the kernel
+GATE = 1e-4
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_mlp.npz")
-FEATURE_NAMES = (["x0-y"] * 3 + ["v h"] * 3 + ["v_prev h"] * 3 + ["ring dv h"] * 3 + ["rhs h2/m"] * 3 +
+FEATURE_NAMES = (["x0-y"] * 3 + ["v h"] * 3 + ["prev correction"] * 3 + ["ring dv h"] * 3 + ["rhs h2/m"] * 3 +
                  ["newton step"] * 3 + ["log1p diag H h2/m"] * 3 + ["mu/lambda", "log10 m + 3", "tanh x0_y/10",
                                                                     "lambda_n h2/m", "tets/24", "tanh y_y"])
 
@@ -183,7 +186,10 @@ def collect(ctx, steps: int, rows_per_step: int, seed: int = 0):
     for _ in range(steps):
         ctx.step(1)
         ctx.warmstart_sample(F, T)
-        valid = torch.nonzero(T[:, 3] > 0).squeeze(1)
+        # solved tet vertices whose block residual at the inertial guess is
+        # above GATE m g: the rows the applied MLP acts on
+        gate = F[:, 12:15].float().abs().sum(1) > GATE
+        valid = torch.nonzero((T[:, 3] > 0) & gate).squeeze(1)
         if valid.numel() == 0:
             continue
         k = min(rows_per_step, valid.numel())

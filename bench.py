@@ -10,6 +10,12 @@ every step runs AVBD iterations until the residual R <= 1e-4 (at most
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
                     [--workload batch_cubes|rods_spheres]
 
+The batched-cubes line times two arms on identically built contexts: plain
+AVBD (the adaptive inertial guess) and the learned warm start (the fused
+tensor-core MLP corrects the guess before the same iterations); `value` is
+the learned arm, `config.arms` holds both with their iterations per
+scene-step and the fraction of scene-steps stopped at max_iters.
+
 `--workload rods_spheres` measures the rod scene instead: 256 Cosserat rods
 of 100 segments hanging from one-sided fixed joints plus 64 rigid spheres,
 all with rigid-body ground contact, 20 iterations per step, FP32 (steps/s).
@@ -56,6 +62,9 @@ def parse():
     p.add_argument("--precision", default=None, choices=["fp32", "mixed", "fp64"],
                    help="default: mixed for batch_cubes, fp32 for rods_spheres")
     p.add_argument("--workload", default="batch_cubes", choices=["batch_cubes", "rods_spheres"])
+    p.add_argument("--warmstart", default="learned", choices=["learned", "none"],
+                   help="batch_cubes: time the learned warm start beside plain AVBD (value = learned)")
+    p.add_argument("--weights", default=os.path.join(ROOT, "avbd_b200", "data", "warmstart_mlp.npz"))
     a = p.parse_args()
     if a.precision is None:
         a.precision = "fp32" if a.workload == "rods_spheres" else "mixed"
@@ -91,6 +100,14 @@ class Workload:
         S = args.cpu_sample_scenes
         return (scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=range(S)), S,
                 f"{S} of {args.scenes} scenes of the same batch")
+
+
+def measured_bf16():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
 
 
 def measured_peaks():
@@ -202,44 +219,24 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_engine(args):
-    import numpy as np
-    import torch
-
-    from avbd_b200 import Context, dist, scenes
-
-    rank, world, local = dist.env()
-    torch.cuda.set_device(local)
-    dist.init("nccl")
-    seed = dist.shard_seed(args.seed, rank)
-
-    t0 = time.time()
-    wl = Workload(args, seed)
-    sc = wl.scene
+def make_context(wl, args, local, stream):
+    from avbd_b200 import Context
     e = Context(device=local)
-    stream = torch.cuda.Stream(device=local)
     e.set_stream(stream.cuda_stream)
-    sc.load(e, residual_tolerance=wl.tol, max_iters=wl.max_iters, precision=args.precision)
+    wl.scene.load(e, residual_tolerance=wl.tol, max_iters=wl.max_iters, precision=args.precision)
     e.finalize()
-    setup_s = time.time() - t0
-    n = sc.num_particles
+    return e
 
-    # warm-up
-    e.step(args.warmup)
-    e.synchronize()
 
-    # ---- device-resident timing
-    dist.barrier()
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    clocks.start()
+def time_steps(e, stream, steps, flush=None):
+    """Device time (ms) of `steps` steps on the engine's stream, with the
+    counters they moved.  With `flush` (a tensor larger than L2) every step
+    is preceded by a write of it and timed alone."""
+    import torch
     st0 = e.stats()
-    if wl.rods:
-        # the rod scene fits in L2: flush it (256 MB write) before every step
-        # and time only the steps
-        flush = torch.empty(64 << 20, dtype=torch.float32, device=torch.device("cuda", local))
+    if flush is not None:
         evs = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -249,50 +246,129 @@ def run_engine(args):
             evs.append((a, b))
         stream.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in evs)
-        del flush
     else:
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        e.step(args.steps)
-        ev1.record(stream)
-        ev1.synchronize()
-        ms = ev0.elapsed_time(ev1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e.step(steps)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b)
     st1 = e.stats()
-    dist.barrier()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    launches = st1["kernel_launches"] - st0["kernel_launches"]
-    iters = (st1["iterations"] - st0["iterations"]) / args.steps
+    d = {k: st1[k] - st0[k] for k in ("kernel_launches", "iterations", "capped_scene_steps", "warmstart_applied")}
+    return ms, d
 
-    # ---- end to end through the C-ABI with pinned host buffers
+
+def time_e2e(e, stream, steps, n):
+    """The same steps through the C-ABI with the state in pinned host memory:
+    positions and velocities uploaded before and read back after every step."""
+    import torch
     x_host = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     v_host = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     x_host[:] = e.positions()
     v_host[:] = e.velocities()
-    dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
         e.set_state(x_host, v_host)
         e.step(1)
         e.positions(out=x_host)
         e.velocities(out=v_host)
-    e1.record(stream)
-    e1.synchronize()
-    ms_e2e = e0.elapsed_time(e1)
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def mlp_roofline(e, n, local, peak):
+    """Tensor-core roofline of the fused MLP kernel on this step's feature
+    rows: 2 (27*128 + 2*128^2 + 128*3) FLOP per row over CUDA-event time."""
+    import torch
+    from avbd_b200 import warmstart
+    F = torch.empty((n, 32), dtype=torch.bfloat16, device=torch.device("cuda", local))
+    e.warmstart_sample(F, None)
+    m = warmstart.MLP(e._ws_params, local)
+    st = torch.cuda.Stream(device=local)
+    for _ in range(3):
+        m.forward(F, st.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    a.record(st)
+    for _ in range(reps):
+        m.forward(F, st.cuda_stream)
+    b.record(st)
+    b.synchronize()
+    ms = a.elapsed_time(b) / reps
+    m.close()
+    flop = 2.0 * (27 * 128 + 2 * 128 * 128 + 128 * 3) * n
+    tf = flop / (ms / 1e3) / 1e12
+    return {"bound": "tensor", "kernel": "k_mlp_apply (fused MLP, tcgen05)", "achieved": tf, "peak": peak,
+            "unit": "TFLOP/s", "frac": tf / peak, "traffic": None, "ms_per_launch": ms, "rows": n,
+            "peak_source": "measured bf16_tflops (burst)"}
+
+
+def run_engine(args):
+    import numpy as np
+    import torch
+
+    from avbd_b200 import dist, warmstart
+
+    rank, world, local = dist.env()
+    torch.cuda.set_device(local)
+    dist.init("nccl")
+    seed = dist.shard_seed(args.seed, rank)
+    dev = torch.device("cuda", local)
+
+    t0 = time.time()
+    wl = Workload(args, seed)
+    sc = wl.scene
+    n = sc.num_particles
+    stream = torch.cuda.Stream(device=local)
+    learned = not wl.rods and args.warmstart == "learned"
+    ep = make_context(wl, args, local, stream)       # plain AVBD
+    el = None
+    if learned:                                      # learned warm start, same scenes
+        params = warmstart.load_params(args.weights)
+        el = make_context(wl, args, local, stream)
+        el.set_warmstart(2, params)
+        el._ws_params = params
+    setup_s = time.time() - t0
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if wl.rods else None
+
+    for e in (ep, el):
+        if e is not None:
+            e.step(args.warmup)
+            e.synchronize()
+
+    # ---- device-resident timing: plain, then learned
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ms_plain, c_plain = time_steps(ep, stream, args.steps, flush)
+    ms_learn, c_learn = time_steps(el, stream, args.steps, flush) if el is not None else (None, None)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    main_e, ms, cnt = (el, ms_learn, c_learn) if el is not None else (ep, ms_plain, c_plain)
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    dist.barrier()
+    ms_e2e = time_e2e(main_e, stream, args.steps, n)
     dist.barrier()
 
-    # ---- per-kernel roofline of the vertex solve
-    solve_ms, solve_bytes, solve_launches = e.profile_solve(2)
-    e.synchronize()
+    # ---- rooflines: the per-color vertex solve, and the MLP on the tensor cores
+    solve_ms, solve_bytes, solve_launches = ep.profile_solve(2)
+    ep.synchronize()
+    peak, peak_kind = measured_peaks()
+    roof_mlp = mlp_roofline(el, n, local, measured_bf16()) if el is not None else None
 
-    ms_max, ms_e2e_max = dist.reduce([ms, ms_e2e], "max", device=torch.device("cuda", local))
+    red = dist.reduce([ms, ms_e2e, ms_plain], "max", device=dev)
+    ms_max, ms_e2e_max, ms_plain_max = red
     value = wl.units * world * args.steps / (ms_max / 1e3)
     value_e2e = wl.units * world * args.steps / (ms_e2e_max / 1e3)
+    value_plain = wl.units * world * args.steps / (ms_plain_max / 1e3)
 
     if rank == 0:
-        peak, peak_kind = measured_peaks()
         per_launch_ms = solve_ms / max(1, solve_launches)
         per_launch_bytes = solve_bytes / max(1, solve_launches)
         achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
@@ -308,24 +384,36 @@ def run_engine(args):
             v_cpu, what, steps, t = cpu_sample(args, wl, seed, threads)
             cpu = {"value": v_cpu, "unit": wl.unit, "cores": threads, "kind": "port",
                    "sample": f"{what}, {steps} steps in {t:.1f} s, FP64 oracle port"}
+        su = args.steps * wl.units
+        arms = {"plain": {"value": value_plain, "ms_per_step": ms_plain_max / args.steps,
+                          "iterations_per_scene_step": c_plain["iterations"] / su,
+                          "capped_fraction": c_plain["capped_scene_steps"] / su if wl.tol > 0 else None}}
+        if el is not None:
+            arms["learned"] = {"value": value, "ms_per_step": ms_max / args.steps,
+                               "iterations_per_scene_step": c_learn["iterations"] / su,
+                               "capped_fraction": c_learn["capped_scene_steps"] / su,
+                               "corrections_applied_fraction": c_learn["warmstart_applied"] / (args.steps * n)}
+        method = (wl.method if el is None else
+                  "learned warm start (MLP 27-128-128-128-3, BF16 tcgen05) + plain AVBD iterations")
         line = {
             "metric": METRIC, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
             "config": {"workload": workload, "scenes_per_gpu": wl.units, "vertices_per_gpu": n,
                        "tets_per_gpu": sc.num_tets, "residual_tolerance": wl.tol, "max_iters": wl.max_iters,
-                       "iterations_per_step": iters, "method": wl.method,
-                       "precision": args.precision,
+                       "method": method, "arms": arms, "precision": args.precision,
                        "l2": (f"L2 flushed (256 MB write) before every timed step; {solve_bytes / 2 / 1e6:.1f} MB "
                               "of solve data per iteration" if wl.rods else
                               f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration"),
                        "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
-            "clocks": clk, "gpu_launches": launches,
+            "clocks": clk, "gpu_launches": cnt["kernel_launches"],
             "e2e": {"value": value_e2e, "unit": wl.unit, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n},
-            "roofline": roof, "cpu_baseline": cpu,
+            "roofline": roof, "roofline_mlp": roof_mlp, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    e.close()
+    for e in (ep, el):
+        if e is not None:
+            e.close()
     dist.shutdown()
 
 

@@ -103,6 +103,10 @@ typedef struct avbd_stats {
     double   last_residual;               /* R after the last sweep (or -1)   */
     unsigned num_colors;
     unsigned num_scenes;
+    unsigned long long capped_scene_steps; /* run-to-tolerance scene-steps that
+                                              stopped at max_iters unconverged */
+    unsigned long long warmstart_applied;  /* vertex-steps whose learned correction
+                                              passed the acceptance test */
 } avbd_stats;
 
 /* ------------------------------------------------------------- lifetime */
@@ -347,7 +351,14 @@ AVBD_API int avbd_mlp_trainer_destroy(avbd_mlp_trainer* t);
  *   mode 1  record: every step stores the features of each solved tet vertex
  *           at the inertial guess x0 and, after the step, the target
  *           (x_end - x0) / s, for avbd_warmstart_sample;
- *   mode 2  apply: x0 <- x0 + s * MLP(features) before the iterations.
+ *   mode 2  apply: x0 <- x0 + s * y, y = MLP(features), before the
+ *           iterations, for each vertex whose correction passes an
+ *           acceptance test: the block residual at x0 (L1 of features 12-14,
+ *           units of m g) must exceed 1e-4 and the residual the correction's
+ *           error would add, kappa * sum_a (1 + H_aa h^2/m) |y_a| with
+ *           kappa = 0.5 (the environment variable AVBD_WS_KAPPA overrides it
+ *           when the mode is set).  Other vertices keep the inertial guess;
+ *           avbd_stats.warmstart_applied counts the accepted ones.
  * params (mode 2): AVBD_MLP_NPARAMS floats, with any input normalisation
  * folded into W1/b1 and the output scale folded into W4/b4. */
 AVBD_API int avbd_set_warmstart(avbd_ctx* ctx, int mode, const float* params);
@@ -357,7 +368,8 @@ AVBD_API int avbd_set_warmstart(avbd_ctx* ctx, int mode, const float* params);
  * (features BF16 [rows][32], targets FP32 [rows][4]; either may be NULL to
  * query *rows).  Feature layout, displacements in units of s = g h^2:
  *   0-2   x0 - y                      (inertial guess minus inertial target)
- *   3-5   v h,  6-8 v_prev h          (last two step displacements)
+ *   3-5   v h                         (last step's displacement)
+ *   6-8   previous step's (x_end - x0) / s  (0 on the first step)
  *   9-11  (mean over incident tets of the other vertices' v - v) h
  *   12-14 block RHS h^2 / m = -(x0 - y) - grad E(x0) h^2 / m
  *   15-17 block Newton step A^-1 RHS  (A = m/h^2 I + H(x0))
