@@ -283,8 +283,18 @@ enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2, MODE_FEATURES = 3 };
 // evaluates |m/h^2 (x-y) + grad| instead of updating; MODE_DEBUG exports the
 // accumulated block; MODE_FEATURES writes the learned warm start's 32 BF16
 // input features of the vertex (row p of `out`) at the current iterate.
+// Resident blocks of 256 threads asked of the compiler: the mixed mode
+// (double state, float records) would take 92 registers (2 blocks per SM);
+// at 3 blocks (80 registers, ~100 bytes of spill) its vertex solve ran 15 %
+// faster over a whole run-to-tolerance step of the 1024-cube batch.  FP32
+// fits 4 blocks (64 registers) without spills; FP64 keeps the default.
+template <typename P, typename RS>
+struct SolveMinBlocks {
+    static constexpr int value = sizeof(P) == 4 ? 4 : (sizeof(RS) == 4 ? 3 : 1);
+};
+
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE>
-__global__ void __launch_bounds__(256) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
+__global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
                                                    unsigned long long* counters, double* out, SceneTol T,
                                                    const float4* __restrict__ aux) {
