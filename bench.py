@@ -267,6 +267,7 @@ def time_e2e(e, stream, steps, n):
     x_host[:] = e.positions()
     v_host[:] = e.velocities()
     torch.cuda.synchronize()
+    st0 = e.stats()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
     for _ in range(steps):
@@ -276,7 +277,8 @@ def time_e2e(e, stream, steps, n):
         e.velocities(out=v_host)
     b.record(stream)
     b.synchronize()
-    return a.elapsed_time(b)
+    st1 = e.stats()
+    return a.elapsed_time(b), st1["iterations"] - st0["iterations"]
 
 
 def mlp_roofline(e, n, local, peak):
@@ -359,7 +361,10 @@ def run_engine(args):
     # ---- end to end through the C-ABI with pinned host buffers, on a context
     # built and warmed like the timed arm, so it runs the same simulation steps
     dist.barrier()
-    ms_e2e = time_e2e(ee, stream, args.steps, n)
+    clocks_e2e = Clocks(local)
+    clocks_e2e.start()
+    ms_e2e, it_e2e = time_e2e(ee, stream, args.steps, n)
+    clk_e2e = clocks_e2e.stop()
     dist.barrier()
 
     # ---- rooflines: the per-color vertex solve, and the MLP on the tensor cores
@@ -413,7 +418,8 @@ def run_engine(args):
                               f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration"),
                        "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
             "clocks": clk, "gpu_launches": cnt["kernel_launches"],
-            "e2e": {"value": value_e2e, "unit": wl.unit, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n},
+            "e2e": {"value": value_e2e, "unit": wl.unit, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
+                    "iterations_per_scene_step": it_e2e / su, "clocks": clk_e2e},
             "roofline": roof, "roofline_mlp": roof_mlp, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
