@@ -607,11 +607,14 @@ static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, c
     count_launch(c);
 }
 
-// The solve runs with the context's lane count; residual and debug passes use 8.
+// The solve, residual and features passes run with the context's lane count
+// (the residual pass spans every vertex every iteration, so its thread count
+// matters even when few scenes are candidates); the one-vertex debug pass
+// uses 8.
 template <typename P, typename RS, typename HT, int MODE>
 static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
                           unsigned count, cudaStream_t st, double* out, const SceneTol& T) {
-    if constexpr (MODE != MODE_SOLVE) {
+    if constexpr (MODE == MODE_DEBUG) {
         solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T);
     } else {
         switch (c->lanes) {

@@ -14,7 +14,8 @@ The batched-cubes line times two arms on identically built contexts: plain
 AVBD (the adaptive inertial guess) and the learned warm start (the fused
 tensor-core MLP corrects the guess before the same iterations); `value` is
 the learned arm, `config.arms` holds both with their iterations per
-scene-step and the fraction of scene-steps stopped at max_iters.
+scene-step, the fraction of scene-steps stopped at max_iters and the p50/p99
+latency of one batch step (CUDA events around every step).
 
 `--workload rods_spheres` measures the rod scene instead: 256 Cosserat rods
 of 100 segments hanging from one-sided fixed joints plus 64 rigid spheres,
@@ -232,29 +233,25 @@ def time_steps(e, stream, steps, flush=None):
     """Device time (ms) of `steps` steps on the engine's stream, with the
     counters they moved.  With `flush` (a tensor larger than L2) every step
     is preceded by a write of it and timed alone."""
+    import numpy as np
     import torch
     st0 = e.stats()
-    if flush is not None:
-        evs = []
-        for _ in range(steps):
+    evs = []
+    for _ in range(steps):
+        if flush is not None:
             with torch.cuda.stream(stream):
                 flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            e.step(1)
-            b.record(stream)
-            evs.append((a, b))
-        stream.synchronize()
-        ms = sum(a.elapsed_time(b) for a, b in evs)
-    else:
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        e.step(steps)
+        e.step(1)
         b.record(stream)
-        b.synchronize()
-        ms = a.elapsed_time(b)
+        evs.append((a, b))
+    stream.synchronize()
+    per = [a.elapsed_time(b) for a, b in evs]
+    ms = sum(per)
     st1 = e.stats()
     d = {k: st1[k] - st0[k] for k in ("kernel_launches", "iterations", "capped_scene_steps", "warmstart_applied")}
+    d["p50_ms"], d["p99_ms"] = float(np.percentile(per, 50)), float(np.percentile(per, 99))
     return ms, d
 
 
@@ -397,10 +394,12 @@ def run_engine(args):
                    "sample": f"{what}, {steps} steps in {t:.1f} s, FP64 oracle port"}
         su = args.steps * wl.units
         arms = {"plain": {"value": value_plain, "ms_per_step": ms_plain_max / args.steps,
+                          "step_latency_ms": {"p50": c_plain["p50_ms"], "p99": c_plain["p99_ms"]},
                           "iterations_per_scene_step": c_plain["iterations"] / su,
                           "capped_fraction": c_plain["capped_scene_steps"] / su if wl.tol > 0 else None}}
         if el is not None:
             arms["learned"] = {"value": value, "ms_per_step": ms_max / args.steps,
+                               "step_latency_ms": {"p50": c_learn["p50_ms"], "p99": c_learn["p99_ms"]},
                                "iterations_per_scene_step": c_learn["iterations"] / su,
                                "capped_fraction": c_learn["capped_scene_steps"] / su,
                                "corrections_applied_fraction": c_learn["warmstart_applied"] / (args.steps * n)}
