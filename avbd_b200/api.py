@@ -251,6 +251,21 @@ class Context:
             check(self.L.avbd_get_candidate_pairs(self.h, cnt.value, _up(out), C.byref(cnt)))
         return out
 
+    def contacts(self):
+        """Triangle-sphere contacts of the last collision stage, ascending key:
+        dict of key [k], tri [k, 3], rigid [k], normal / barys / cp_local [k, 3]."""
+        cnt = C.c_uint(0)
+        check(self.L.avbd_get_contacts(self.h, 0, None, None, None, C.byref(cnt)))
+        n = cnt.value
+        keys = np.zeros(n, dtype=np.uint64)
+        idx = np.zeros((n, 4), dtype=np.uint32)
+        vec = np.zeros((n, 9))
+        if n:
+            check(self.L.avbd_get_contacts(self.h, n, keys.ctypes.data_as(C.POINTER(C.c_uint64)), _up(idx),
+                                           _dp(vec), C.byref(cnt)))
+        return {"key": keys, "tri": idx[:, :3], "rigid": idx[:, 3], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
+                "cp_local": vec[:, 6:9]}
+
     def debug_block(self, p):
         G, H, dof = np.zeros(6), np.zeros(36), C.c_int(0)
         check(self.L.avbd_debug_block(self.h, p, _dp(G), _dp(H), C.byref(dof)))

@@ -2,7 +2,7 @@
 
 Every .cu file under csrc/ is compiled by nvcc with
 `-gencode arch=compute_100a,code=sm_100a -lineinfo -O3` (in parallel, one
-object per file under _build/) and linked into avbd_b200/libavbd_b200.so,
+object per file under _build/; lbvh.cu and narrow.cu with --fmad=false) and linked into avbd_b200/libavbd_b200.so,
 which exports exactly the C-ABI declared in include/avbd.h.
 """
 from __future__ import annotations
@@ -25,6 +25,11 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--ex
                   "-Xcompiler", "-fvisibility=hidden", "-I" + os.path.join(ROOT, "include")]
 
 
+# Files whose FP64 results must round like the CPU restatement (built
+# without contraction): the LBVH bounds and Morton codes, the narrow phase.
+FILE_FLAGS = {"lbvh.cu": ["--fmad=false"], "narrow.cu": ["--fmad=false"]}
+
+
 def _nvcc() -> str:
     p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not os.path.exists(p):
@@ -42,7 +47,7 @@ def _deps():
 
 def _compile(src: str, extra) -> str:
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    cmd = [_nvcc()] + NVFLAGS + list(extra) + ["-c", src, "-o", obj]
+    cmd = [_nvcc()] + NVFLAGS + FILE_FLAGS.get(os.path.basename(src), []) + list(extra) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

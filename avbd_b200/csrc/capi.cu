@@ -743,9 +743,6 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     free_device(c);
     const unsigned n = (unsigned)c->mass.size();
     if (n == 0) return fail(AVBD_ERR_STATE, "no particles");
-    for (auto& p : c->prims)
-        if (p.type == AVBD_SHAPE_SPHERE)
-            return fail(AVBD_ERR_UNSUPPORTED, "sphere collision primitives are not enabled in this build");
     for (auto& g : c->ground)
         if (c->rot[g.p] != UINT32_MAX)
             return fail(AVBD_ERR_UNSUPPORTED, "ground energy on an oriented particle (use rigid-body ground)");
@@ -1409,6 +1406,46 @@ int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, doubl
     if (solve_ms) *solve_ms = ms;
     if (solve_bytes) *solve_bytes = bytes;
     if (launches) *launches = nl;
+    return device_error(c);
+}
+
+int avbd_get_contacts(avbd_ctx* c, unsigned capacity, uint64_t* keys, unsigned* idx4, double* vec9,
+                      unsigned* count) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (!count) return fail(AVBD_ERR_INVALID_ARG, "null count");
+    const LbvhState& L = c->lbvh;
+    *count = 0;
+    if (!L.contact_capacity) return AVBD_OK;
+    uint32_t n = 0;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&n, L.contact_count, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    if (n > L.contact_capacity) return fail(AVBD_ERR_CAPACITY, "more contacts than the contact buffer holds");
+    std::vector<uint64_t> k(n);
+    std::vector<uint4> ix(n);
+    std::vector<double> v(9ull * n);
+    if (n) {
+        CUDA_OR_FAIL(cudaMemcpyAsync(k.data(), L.contact_key, 8ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_OR_FAIL(cudaMemcpyAsync(ix.data(), L.contact_idx, 16ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_OR_FAIL(cudaMemcpyAsync(v.data(), L.contact_vec, 72ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    }
+    // ascending key, as CollisionDetector::_handleDetectedCollisions orders them
+    std::vector<uint32_t> ord(n);
+    std::iota(ord.begin(), ord.end(), 0u);
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return k[a] < k[b]; });
+    *count = n;
+    for (uint32_t j = 0; j < n && j < capacity; j++) {
+        const uint32_t o = ord[j];
+        if (keys) keys[j] = k[o];
+        if (idx4) {
+            idx4[4 * j] = c->perm[ix[o].x];
+            idx4[4 * j + 1] = c->perm[ix[o].y];
+            idx4[4 * j + 2] = c->perm[ix[o].z];
+            idx4[4 * j + 3] = c->perm[ix[o].w];
+        }
+        if (vec9) std::copy(v.begin() + 9ull * o, v.begin() + 9ull * o + 9, vec9 + 9ull * j);
+    }
     return device_error(c);
 }
 

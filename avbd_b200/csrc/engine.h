@@ -153,6 +153,13 @@ struct LbvhState {
     double* xd = nullptr;           // FP64 copies of positions / velocities
     double* vd = nullptr;
     unsigned hist_blocks = 0;
+    uint32_t* obj = nullptr;        // object id of each primitive
+    // narrow-phase detections (triangle-sphere), allocated when spheres exist
+    unsigned contact_capacity = 0;
+    uint64_t* contact_key = nullptr;
+    uint4* contact_idx = nullptr;   // triangle's three vertices, sphere particle (internal order)
+    double* contact_vec = nullptr;  // normal, barycentrics, contact point in the sphere frame
+    uint32_t* contact_count = nullptr;
 };
 
 }  // namespace avbd
@@ -309,6 +316,9 @@ int gpu_dsatur(const std::vector<unsigned>& p_off, const std::vector<unsigned>& 
 int lbvh_allocate(avbd_ctx* c, std::string& err);
 template <typename R>
 void lbvh_stage(avbd_ctx* c, DevState<R>& s, cudaStream_t st);
+// narrow phase over the broad phase's pairs (narrow.cu)
+template <typename R>
+void launch_narrow(avbd_ctx* c, DevState<R>& s, cudaStream_t st);
 
 // counts launches for the stats
 void count_launch(avbd_ctx* c, unsigned k = 1);

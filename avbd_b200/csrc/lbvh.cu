@@ -22,6 +22,7 @@
 #include <mutex>
 
 #include "engine.h"
+#include "s3math.cuh"
 
 namespace avbd {
 
@@ -43,6 +44,13 @@ AVBD_D void pos_vel(const DevState<R>& s, unsigned p, double* x, double* v) {
     typename Vec4Of<R>::T a = s.x[p], b = s.v[p];
     x[0] = (double)a.x; x[1] = (double)a.y; x[2] = (double)a.z;
     v[0] = (double)b.x; v[1] = (double)b.y; v[2] = (double)b.z;
+}
+
+// |R| v, rows summed left to right
+AVBD_D V3<double> abs_mat_vec(const M3<double>& R, V3<double> v) {
+    return mk3(fabs(R.a[0][0]) * v.x + fabs(R.a[0][1]) * v.y + fabs(R.a[0][2]) * v.z,
+               fabs(R.a[1][0]) * v.x + fabs(R.a[1][1]) * v.y + fabs(R.a[1][2]) * v.z,
+               fabs(R.a[2][0]) * v.x + fabs(R.a[2][1]) * v.y + fabs(R.a[2][2]) * v.z);
 }
 
 // Swept bounds of every primitive and the scene box (exact min/max through
@@ -74,6 +82,32 @@ __global__ void __launch_bounds__(256) k_prim_bounds(DevState<R> s, LbvhState L,
                     mn[a] = dmin_ref(mn[a], nx);
                     mx[a] = dmax_ref(mx[a], nx);
                 }
+            }
+        } else if (t == AVBD_SHAPE_SPHERE) {
+            // analytic shape: local box [-r, r]^3 rotated into the world at the
+            // current and at the predicted pose (CollisionPrimitivePool.hpp:199-231);
+            // this file is compiled without FMA contraction, so the expressions
+            // below round like the reference's
+            const unsigned op = id.x, slot = s.rot[op];
+            const double r = L.radius[i];
+            const V3<double> lmin = mk3(-r, -r, -r), lmax = mk3(r, r, r);
+            const V3<double> ctr = 0.5 * (lmin + lmax), he = 0.5 * (lmax - lmin);
+            const typename Vec4Of<R>::T q4 = s.q[slot], w4 = s.w[slot];
+            const Q4<double> q{(double)q4.x, (double)q4.y, (double)q4.z, (double)q4.w};
+            double x[3], v[3];
+            pos_vel(s, op, x, v);
+            const V3<double> xp = mk3(x[0], x[1], x[2]), vp = mk3(v[0], v[1], v[2]);
+            const V3<double> wc = qrot(q, ctr) + xp;
+            const V3<double> we = abs_mat_vec(qmat(q), he);
+            const Q4<double> nq = plus_s3(q, dt * mk3((double)w4.x, (double)w4.y, (double)w4.z));
+            const V3<double> nwc = qrot(nq, ctr) + xp + dt * vp;
+            const V3<double> nwe = abs_mat_vec(qmat(nq), he);
+            const double c0[3] = {wc.x, wc.y, wc.z}, e0[3] = {we.x, we.y, we.z};
+            const double c1[3] = {nwc.x, nwc.y, nwc.z}, e1[3] = {nwe.x, nwe.y, nwe.z};
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                mn[a] = dmin_ref(c0[a] - e0[a], c1[a] - e1[a]);
+                mx[a] = dmax_ref(c0[a] + e0[a], c1[a] + e1[a]);
             }
         } else {  // rod segment
             double x1[3], v1[3], x2[3], v2[3];
@@ -362,9 +396,13 @@ int lbvh_allocate(avbd_ctx* c, std::string& err) {
     std::vector<uint8_t> type(n);
     std::vector<uint4> pidx(n);
     std::vector<double> radius(n);
+    std::vector<uint32_t> obj(n);
+    unsigned spheres = 0;
     for (unsigned i = 0; i < n; i++) {
         const HostPrim& p = c->prims[i];
         type[i] = p.type;
+        obj[i] = p.object_id;
+        spheres += p.type == AVBD_SHAPE_SPHERE;
         pidx[i] = make_uint4(c->inv[p.idx[0]], p.type == AVBD_SHAPE_SPHERE ? 0 : c->inv[p.idx[1]],
                              p.type == AVBD_SHAPE_TRIANGLE ? c->inv[p.idx[2]] : 0, 0);
         radius[i] = p.radius;
@@ -388,8 +426,19 @@ int lbvh_allocate(avbd_ctx* c, std::string& err) {
         !alloc((void**)&L.visited, sizeof(uint32_t) * nn) || !alloc((void**)&L.nbounds, sizeof(double) * 6 * nn) ||
         !alloc((void**)&L.scene_box, sizeof(unsigned long long) * 8) || !alloc((void**)&L.root, sizeof(uint32_t) * 2) ||
         !alloc((void**)&L.pairs, sizeof(uint2) * L.pair_capacity) || !alloc((void**)&L.pair_count, sizeof(uint32_t)) ||
-        !alloc((void**)&L.range, sizeof(uint2) * std::max(1u, n - 1)))
+        !alloc((void**)&L.range, sizeof(uint2) * std::max(1u, n - 1)) ||
+        !alloc((void**)&L.obj, sizeof(uint32_t) * n))
         return AVBD_ERR_CUDA;
+    if (spheres) {  // room for 64 triangle contacts per sphere
+        L.contact_capacity = std::max(1024u, 64u * spheres);
+        if (!alloc((void**)&L.contact_key, sizeof(uint64_t) * L.contact_capacity) ||
+            !alloc((void**)&L.contact_idx, sizeof(uint4) * L.contact_capacity) ||
+            !alloc((void**)&L.contact_vec, sizeof(double) * 9 * L.contact_capacity) ||
+            !alloc((void**)&L.contact_count, sizeof(uint32_t)))
+            return AVBD_ERR_CUDA;
+        cudaMemsetAsync(L.contact_count, 0, sizeof(uint32_t), c->stream);
+    }
+    cudaMemcpyAsync(L.obj, obj.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(L.pidx, pidx.data(), sizeof(uint4) * n, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(L.radius, radius.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
@@ -438,6 +487,7 @@ void lbvh_stage(avbd_ctx* c, DevState<R>& s, cudaStream_t st) {
     k_refit<<<nb(n, 256), 256, 0, st>>>(L);
     k_traverse<<<nb(n, 128), 128, 0, st>>>(L, L.range, n > 1 ? n : 0, c->d_error);
     count_launch(c, 2);
+    launch_narrow<R>(c, s, st);
 }
 
 template void lbvh_stage<float>(avbd_ctx*, DevState<float>&, cudaStream_t);

@@ -257,6 +257,20 @@ AVBD_API int avbd_get_lbvh(avbd_ctx* ctx, unsigned* num_primitives, uint64_t* mo
 AVBD_API int avbd_get_candidate_pairs(avbd_ctx* ctx, unsigned capacity, unsigned* pairs2,
                              unsigned* count);
 
+/* Triangle-sphere contacts found by the last collision stage's narrow phase
+ * (CollisionDetector::_triangleSphere / _triangleSDF_CCD,
+ * collision/CollisionDetector.cpp:504-540,689-876), in ascending key order
+ * (DetectedCollision::generateKey, collision/DetectedCollision.hpp:43-66).
+ * Per contact: keys[k]; idx4 = the triangle's three particle slots and the
+ * sphere's particle slot; vec9 = contact normal (world), barycentrics of the
+ * contact point on the triangle, contact point on the sphere in its body
+ * frame.  Up to `capacity` contacts are written (pointers may be NULL);
+ * *count receives the number found.  The contact energies these detections
+ * create in the reference (TriangleRigidCollisionEnergy) are not part of
+ * this engine's step. */
+AVBD_API int avbd_get_contacts(avbd_ctx* ctx, unsigned capacity, uint64_t* keys, unsigned* idx4, double* vec9,
+                               unsigned* count);
+
 /* Block gradient and Hessian of particle p at the current state: the
  * grad/hess accumulated by VBDSolver::_solveParticle<DOF>
  * (simulation/VBDSolver.hpp:293-447).  G is 3 or 6 doubles, H is 9 or 36

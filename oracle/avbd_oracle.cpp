@@ -359,6 +359,9 @@ struct Ctx {
     std::vector<double> nbounds;            // 6 per node
     unsigned root = 0;
     std::vector<std::pair<unsigned, unsigned>> pairs;
+    // detected triangle-sphere contacts of the last collision stage, ascending key
+    struct Detected { uint64_t key; unsigned tri[3], rb; V3 normal, barys, cp_local; };
+    std::vector<Detected> contacts;
 
     // statistics
     double last_residual = -1;
@@ -1301,6 +1304,171 @@ static void traverse(Ctx& c) {
     std::sort(c.pairs.begin(), c.pairs.end());
 }
 
+// ------------------------------------------------ narrow phase
+// SDF::evaluate / SDF::gradient for spheres (collision/SDF.hpp:46-107)
+static inline double sdf_sphere(double r, V3 p) { return norm(p) - r; }
+static inline V3 sdf_sphere_grad(V3 p) {
+    double d = norm(p);
+    return d > 1e-8 ? p / d : V3(1, 0, 0);
+}
+
+// Algorithm::goldenSectionSearch (common/Algorithm.hpp:252-294): minimises f
+// over the segment [lo, hi] (a time interval or a segment in space); the
+// search stops when the bracket is 1e-3 wide.
+static inline double gss_width(double x) { return std::fabs(x); }
+static inline double gss_width(V3 x) { return norm(x); }
+static inline double gss_lerp(double a, double b, double s) { return (1 - s) * a + s * b; }
+static inline V3 gss_lerp(V3 a, V3 b, double s) { return (1 - s) * a + s * b; }
+template <typename T, typename F>
+static T gss(T lo, T hi, F&& f) {
+    const double phi = 1.61803398875, r = 1 / phi, sg = 1 - r, tol = 1e-3;
+    double a0 = 0, a1 = sg, a2 = r, a3 = 1;
+    T t0 = lo, t1 = gss_lerp(lo, hi, a1), t2 = gss_lerp(lo, hi, a2), t3 = hi;
+    double f0 = f(t0), f1 = f(t1), f2 = f(t2), f3 = f(t3);
+    while (gss_width(t3 - t0) > tol) {
+        if (std::min(f0, f1) < std::min(f2, f3)) {
+            a3 = a2; t3 = t2; f3 = f2;
+            a2 = a1; t2 = t1; f2 = f1;
+            a1 = r * a2 + sg * a0;
+            t1 = gss_lerp(lo, hi, a1);
+            f1 = f(t1);
+        } else {
+            a0 = a1; t0 = t1; f0 = f1;
+            a1 = a2; t1 = t2; f1 = f2;
+            a2 = r * a1 + sg * a3;
+            t2 = gss_lerp(lo, hi, a2);
+            f2 = f(t2);
+        }
+    }
+    T tm = gss_lerp(lo, hi, 0.5 * (a0 + a3));
+    double fm = f(tm);
+    if (f0 < fm && f0 < f3) return t0;
+    if (fm < f3) return tm;
+    return t3;
+}
+
+// Math::barycentricCoordinates (common/Math.hpp:421-438)
+static inline V3 barycentric(V3 p, V3 a, V3 b, V3 c) {
+    V3 v0 = b - a, v1 = c - a, v2 = p - a;
+    double d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+    double den = d00 * d11 - d01 * d01;
+    double v = (d11 * d20 - d01 * d21) / den;
+    double w = (d00 * d21 - d01 * d20) / den;
+    return V3(1 - v - w, v, w);
+}
+
+// rotation of v by the inverse of q (Eigen's inverse: conjugate / |q|^2)
+static inline V3 qrot_inv(Q4 q, V3 v) {
+    double n2 = q.w * q.w + q.x * q.x + q.y * q.y + q.z * q.z;
+    Q4 i{q.w / n2, -q.x / n2, -q.y / n2, -q.z / n2};
+    return qrot(i, v);
+}
+
+// CollisionDetector::_triangleSDF_CCD (collision/CollisionDetector.cpp:689-876):
+// alternating temporal and spatial golden-section searches for the first
+// contact of a moving triangle with a moving sphere over [0, dt].
+static bool tri_sphere_ccd(const Ctx& c, const Prim& T, const Prim& S, V3& normal, V3& barys, V3& cp_local) {
+    const unsigned rb = S.idx[0];
+    const double rad = S.radius, dt = c.dt;
+    const V3 xr = c.x[rb], vr = c.v[rb], wr = c.w[c.rot[rb]];
+    const Q4 qr = c.q[c.rot[rb]];
+    auto rb_pos = [&](double t) { return xr + t * vr; };
+    auto rb_rot = [&](double t) { return qmul(qr, exp_s3(t * wr)); };
+    auto to_local = [&](V3 xg, double t) { return qrot_inv(rb_rot(t), xg - rb_pos(t)); };
+    auto body_vel = [&](V3 xg, double t) { return vr + cross(qrot(rb_rot(t), wr), xg - rb_pos(t)); };
+    auto rel_vel = [&](V3 xg, V3 vg, double t) { return qrot_inv(rb_rot(t), vg - body_vel(xg, t)); };
+    const V3 p1 = c.x[T.idx[0]], p2 = c.x[T.idx[1]], p3 = c.x[T.idx[2]];
+    const V3 v1 = c.v[T.idx[0]], v2 = c.v[T.idx[1]], v3 = c.v[T.idx[2]];
+    auto first_eval = [&](V3 pk, V3 vk) { return dot(rel_vel(pk, vk, 0), sdf_sphere_grad(to_local(pk, 0))); };
+    const double e1 = first_eval(p1, v1), e2 = first_eval(p2, v2), e3 = first_eval(p3, v3);
+    double t_start = 0, t_end = dt, t = 0, u, v, w;
+    if (e1 < e2 && e1 < e3) { u = 1; v = 0; w = 0; }
+    else if (e2 < e1 && e2 < e3) { u = 0; v = 1; w = 0; }
+    else { u = 0; v = 0; w = 1; }
+    auto interp = [&](double t_) { return u * (p1 + t_ * v1) + v * (p2 + t_ * v2) + w * (p3 + t_ * v3); };
+    auto sd_time = [&](double t_) { return sdf_sphere(rad, to_local(interp(t_), t_)); };
+    auto ud_time = [&](double t_) { return std::fabs(sd_time(t_)); };
+    auto sd_point = [&](V3 xl) { return sdf_sphere(rad, xl); };
+    double sd = 0;
+    V3 grad, x_ti;
+    for (int it = 0; it < 16; it++) {
+        const double t_old = t;
+        V3 xg = interp(t), vg = u * v1 + v * v2 + w * v3;
+        x_ti = to_local(xg, t);
+        V3 v_ti = rel_vel(xg, vg, t);
+        sd = sdf_sphere(rad, x_ti);
+        if (sd <= 0) {
+            t_end = std::min(t, t_end);
+            t = gss(t_start, t, ud_time);
+        } else {
+            double vdg = dot(v_ti, sdf_sphere_grad(x_ti));
+            if (vdg > 0) t = gss(t_start, t, sd_time);
+            else t = gss(t, t_end, sd_time);
+        }
+        xg = interp(t);
+        x_ti = to_local(xg, t);
+        sd = sdf_sphere(rad, x_ti);
+        grad = sdf_sphere_grad(x_ti);
+        if (sd <= 0) t_end = std::min(t, t_end);
+        V3 l1 = to_local(p1 + t * v1, t), l2 = to_local(p2 + t * v2, t), l3 = to_local(p3 + t * v3, t);
+        double s1 = dot(l1, grad), s2 = dot(l2, grad), s3 = dot(l3, grad);
+        V3 sv = (s1 < s2 && s1 < s3) ? l1 : ((s2 < s1 && s2 < s3) ? l2 : l3);
+        V3 x_new = gss(x_ti, sv, sd_point);
+        V3 b = barycentric(x_new, l1, l2, l3);
+        u = b.x; v = b.y; w = b.z;
+        if (std::fabs(t_old - t) < 1e-6 && norm(x_new - x_ti) < 1e-6) break;
+    }
+    barys = V3(u, v, w);
+    cp_local = x_ti - sd * grad;
+    normal = qrot(rb_rot(t), grad);
+    return sd < c.margin;
+}
+
+// DetectedCollision::generateKey (collision/DetectedCollision.hpp:43-66)
+static inline uint64_t collision_key(unsigned type, unsigned a, unsigned b, unsigned code) {
+    if (a > b) std::swap(a, b);
+    uint64_t k = type & 31u;
+    k = (k << 26) | (a & 0x3FFFFFFu);
+    k = (k << 26) | (b & 0x3FFFFFFu);
+    return (k << 7) | (code & 127u);
+}
+
+// CollisionDetector::_narrowPhaseCollisionDetection + _processPotentialCollision
+// (collision/CollisionDetector.cpp:132-215) for the pairs this engine
+// supports: same-object primitives sharing a vertex are skipped,
+// triangle-triangle and rod-rod are no-ops, triangle-sphere runs the CCD
+// (DetectedCollisionType::TriangleRigid = 2).  Detections are kept in
+// ascending key order, as _handleDetectedCollisions sorts them.
+static void narrow_phase(Ctx& c) {
+    c.contacts.clear();
+    for (auto [la, lb] : c.pairs) {
+        unsigned a = c.sorted[la], b = c.sorted[lb];
+        const Prim& A = c.prims[a];
+        const Prim& B = c.prims[b];
+        if (A.object_id == B.object_id) {
+            bool share = false;
+            for (int i = 0; i < A.np; i++)
+                for (int j = 0; j < B.np; j++) share |= A.idx[i] == B.idx[j];
+            if (share) continue;
+        }
+        unsigned ia = a, ib = b;
+        if (c.prims[ia].type > c.prims[ib].type) std::swap(ia, ib);
+        const Prim& P = c.prims[ia];
+        const Prim& Q = c.prims[ib];
+        if (P.type == 0 && Q.type == 2) {
+            Ctx::Detected d;
+            if (tri_sphere_ccd(c, P, Q, d.normal, d.barys, d.cp_local)) {
+                d.key = collision_key(2, ia, ib, 0);
+                d.tri[0] = P.idx[0]; d.tri[1] = P.idx[1]; d.tri[2] = P.idx[2];
+                d.rb = Q.idx[0];
+                c.contacts.push_back(d);
+            }
+        }
+    }
+    std::stable_sort(c.contacts.begin(), c.contacts.end(),
+                     [](const Ctx::Detected& x, const Ctx::Detected& y) { return x.key < y.key; });
+}
+
 // LBVHBuilder::buildBVH + broad phase (collision/LBVHBuilder.cpp:13-25,
 // collision/CollisionDetector.cpp:24-55).  Narrow phase: triangle-triangle and
 // rod-rod are no-ops in the reference (CollisionDetector.cpp:589-599,668-676);
@@ -1344,6 +1512,7 @@ static void collision_stage(Ctx& c) {
     construct_tree(c, n);
     refit(c, n);
     traverse(c);
+    narrow_phase(c);
 }
 
 }  // namespace orc
@@ -1591,6 +1760,24 @@ void orc_get_adjacency(void* h, unsigned* e_off, uint8_t* type, unsigned* idx, u
 unsigned orc_num_neighbors(void* h) { return (unsigned)((Ctx*)h)->p_nbr.size(); }
 
 unsigned orc_num_pairs(void* h) { return (unsigned)((Ctx*)h)->pairs.size(); }
+// contacts of the last collision stage: per contact key, tri[3], rigid,
+// normal[3], barys[3], cp_local[3] (ascending key)
+unsigned orc_get_contacts(void* h, uint64_t* keys, unsigned* idx4, double* vec9) {
+    Ctx& c = *(Ctx*)h;
+    for (size_t k = 0; k < c.contacts.size(); k++) {
+        const auto& d = c.contacts[k];
+        if (keys) keys[k] = d.key;
+        if (idx4) { idx4[4 * k] = d.tri[0]; idx4[4 * k + 1] = d.tri[1]; idx4[4 * k + 2] = d.tri[2]; idx4[4 * k + 3] = d.rb; }
+        if (vec9) {
+            for (int i = 0; i < 3; i++) {
+                vec9[9 * k + i] = d.normal[i];
+                vec9[9 * k + 3 + i] = d.barys[i];
+                vec9[9 * k + 6 + i] = d.cp_local[i];
+            }
+        }
+    }
+    return (unsigned)c.contacts.size();
+}
 void orc_get_lbvh(void* h, uint64_t* morton, unsigned* sorted, unsigned* left, unsigned* right, unsigned* parent,
                   unsigned* subtree, double* bounds, unsigned* root, unsigned* pairs) {
     Ctx& c = *(Ctx*)h;

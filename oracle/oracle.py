@@ -62,6 +62,7 @@ def lib():
             "orc_get_positions": (None, [vp, dp]),
             "orc_get_velocities": (None, [vp, dp]),
             "orc_get_rotations": (None, [vp, dp]),
+            "orc_get_contacts": (C.c_uint, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint), dp]),
             "orc_get_angular_velocities": (None, [vp, dp]),
             "orc_num_particles": (C.c_uint, [vp]),
             "orc_neo_hookean_add": (C.c_uint, [vp, C.c_uint, up, dp, dp, dp, dp, dp]),
@@ -270,6 +271,18 @@ class Oracle:
         out = np.zeros((self.num_particles, 4))
         self.L.orc_get_rotations(self.h, _p(out, C.c_double))
         return out
+
+    def contacts(self):
+        """Triangle-sphere contacts of the last collision stage, ascending key:
+        dict of key [k], tri [k, 3], rigid [k], normal / barys / cp_local [k, 3]."""
+        n = self.L.orc_get_contacts(self.h, None, None, None)
+        keys = np.zeros(n, dtype=np.uint64)
+        idx = np.zeros((n, 4), dtype=np.uint32)
+        vec = np.zeros((n, 9))
+        if n:
+            self.L.orc_get_contacts(self.h, _p(keys, C.c_uint64), _p(idx, C.c_uint), _p(vec, C.c_double))
+        return {"key": keys, "tri": idx[:, :3], "rigid": idx[:, 3], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
+                "cp_local": vec[:, 6:9]}
 
     def angular_velocities(self):
         out = np.zeros((self.num_particles, 3))
