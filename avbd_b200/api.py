@@ -266,6 +266,31 @@ class Context:
         return {"key": keys, "tri": idx[:, :3], "rigid": idx[:, 3], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
                 "cp_local": vec[:, 6:9]}
 
+    def dynamic_info(self):
+        """Contact pool and recoloring state of the last step: live contacts,
+        pool size, colors, conflicted particles, particles still dirty,
+        dynamic adjacency entries."""
+        out = np.zeros(6, dtype=np.uint32)
+        check(self.L.avbd_dynamic_info(self.h, _up(out)))
+        return dict(zip(["live", "pool_size", "colors", "conflicted", "dirty", "entries"], (int(v) for v in out)))
+
+    def contact_pool(self):
+        """Triangle-rigid contact pool by slot (layout of avbd_get_contact_pool)."""
+        size = C.c_uint(0)
+        check(self.L.avbd_get_contact_pool(self.h, 0, None, None, None, C.byref(size)))
+        n = size.value
+        p4 = np.zeros((n, 4), dtype=np.uint32)
+        act = np.zeros(n, dtype=np.uint8)
+        d = np.zeros((n, 24))
+        if n:
+            check(self.L.avbd_get_contact_pool(self.h, n, _up(p4), _u8p(act), _dp(d), C.byref(size)))
+        return {"particles": p4, "active": act.astype(bool), "n": d[:, 0:3], "t": d[:, 3:6], "b": d[:, 6:9],
+                "barys": d[:, 9:12], "cp_local": d[:, 12:15], "k": d[:, 15:19], "lam": d[:, 19:23],
+                "flags": d[:, 23].astype(np.uint8)}
+
+    def set_recolor_rounds(self, rounds):
+        check(self.L.avbd_debug_set_recolor_rounds(self.h, rounds))
+
     def debug_block(self, p):
         G, H, dof = np.zeros(6), np.zeros(36), C.c_int(0)
         check(self.L.avbd_debug_block(self.h, p, _dp(G), _dp(H), C.byref(dof)))

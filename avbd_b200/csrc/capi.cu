@@ -66,6 +66,7 @@ static void free_device(avbd_ctx* c) {
     }
     for (void* p : c->allocations) cudaFree(p);
     c->allocations.clear();
+    dyn_destroy(c);
     c->f = DevState<float>();
     c->d = DevState<double>();
     c->lbvh = LbvhState();
@@ -897,6 +898,14 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     if (!c->prims.empty()) {
         std::string err;
         if (int r2 = lbvh_allocate(c, err)) return fail(r2, err);
+        // triangle-sphere pairs give dynamic contact energies, managed per step
+        bool tri = false, sph = false;
+        for (auto& pr : c->prims) {
+            tri |= pr.type == AVBD_SHAPE_TRIANGLE;
+            sph |= pr.type == AVBD_SHAPE_SPHERE;
+        }
+        if (tri && sph)
+            if (int r2 = dyn_create(c, p_off, p_nbr, err)) return fail(r2, err);
     }
     c->stats.num_colors = nc;
     c->stats.num_scenes = (unsigned)sb.size() - 1;
@@ -918,10 +927,14 @@ double omega_at(unsigned i, double rho, double prev) {
     return 1;
 }
 
-// Collision stage and step-start hooks + inertial prediction.
+// Collision stage and step-start hooks + inertial prediction.  With dynamic
+// contacts the collision stage ends on the host (contact pool, recoloring),
+// which synchronizes the stream.
 template <typename R>
-void enqueue_begin(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+int enqueue_begin(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
     if (!c->prims.empty()) lbvh_stage<R>(c, s, st);
+    if (c->dyn)
+        if (int r = dyn_manage<R>(c, s, k, st)) return r;
     if (c->damping) launch_tet_eprev<R>(c, s, k, st);
     launch_begin_step<R>(c, s, k, st);
     launch_begin_step_rot<R>(c, s, k, st);
@@ -936,12 +949,18 @@ void enqueue_begin(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_
             count_launch(c);
         }
     }
+    return AVBD_OK;
 }
 
 // One Gauss-Seidel sweep: per color, the positional (3-DOF) slab then the
 // oriented (6-DOF) slab; both are independent sets within the color.
 template <typename R>
 void enqueue_sweep(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, const SceneTol& T) {
+    if (c->dyn) {  // recolored vertices and conflicts of the dynamic contacts
+        const unsigned nc = dyn_num_colors(c);
+        for (unsigned col = 0; col < nc; col++) dyn_solve_color<R>(c, s, k, col, st, T);
+        return;
+    }
     for (unsigned col = 0; col < c->num_colors; col++) {
         if (c->color_solve[col])
             launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st, T);
@@ -956,6 +975,7 @@ void enqueue_chebyshev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double 
                        const SceneTol& T) {
     launch_chebyshev_dual<R>(c, s, k, omega, st, T);
     launch_chebyshev_rot<R>(c, s, k, omega, st, T);
+    if (c->dyn) launch_trc_after_iter<R>(c, s, st, T);
 }
 
 template <typename R>
@@ -983,14 +1003,15 @@ void enqueue_iteration(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double 
 }
 
 template <typename R>
-void enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
-    enqueue_begin<R>(c, s, k, st);
+int enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    if (int r = enqueue_begin<R>(c, s, k, st)) return r;
     double omega = 1;
     for (unsigned i = 0; i < c->solver.solver_iters; i++) {
         omega = omega_at(i, c->solver.iter_acceleration, omega);
         enqueue_iteration<R>(c, s, k, omega, st);
     }
     enqueue_velocity<R>(c, s, k, st);
+    return AVBD_OK;
 }
 
 StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_accel, c->kappa_max}; }
@@ -1068,7 +1089,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         SceneTol solveT{c->d_scene, c->d_scene_active, nullptr, c->d_scene_r2, nullptr};
         SceneTol resT{c->d_scene, nullptr, c->d_scene_cand, nullptr, c->d_scene_ex};
         for (unsigned t = 0; t < n_steps; t++) {
-            enqueue_begin<R>(c, s, k, st);
+            if (int r = enqueue_begin<R>(c, s, k, st)) return r;
             launch_tol_init(c, st);
             double omega = 1;
             for (unsigned it = 0; it < max_it; it++) {
@@ -1088,7 +1109,8 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         CUDA_OR_FAIL(cudaGetLastError());
         return AVBD_OK;
     }
-    bool capturable = c->use_graph && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+    // a step with dynamic contacts runs host work between its launches: no graph
+    bool capturable = c->use_graph && !c->dyn && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
     if (capturable && (c->graph_dirty || !c->graph)) {
         if (c->graph) {
             cudaGraphExecDestroy(c->graph);
@@ -1097,7 +1119,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         unsigned long long before = c->stats.kernel_launches;
         cudaGraph_t g;
         CUDA_OR_FAIL(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        enqueue_step_fixed<R>(c, s, k, st);
+        enqueue_step_fixed<R>(c, s, k, st);  // no host step without dynamic contacts: cannot fail
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (e != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&c->graph, g, 0);
@@ -1112,7 +1134,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
             CUDA_OR_FAIL(cudaGraphLaunch(c->graph, st));
             c->stats.kernel_launches += c->launches_per_step;
         } else {
-            enqueue_step_fixed<R>(c, s, k, st);
+            if (int r = enqueue_step_fixed<R>(c, s, k, st)) return r;
         }
         c->host_iterations += (unsigned long long)c->solver.solver_iters * c->num_scenes;
     }
@@ -1328,8 +1350,9 @@ int avbd_get_angular_velocities(avbd_ctx* c, unsigned first, unsigned n, double*
 int avbd_get_coloring(avbd_ctx* c, unsigned* colors, unsigned* num_colors) {
     if (int r = check_ctx(c)) return r;
     if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
-    if (colors) std::copy(c->color.begin(), c->color.end(), colors);
-    if (num_colors) *num_colors = c->num_colors;
+    // the recolored colors when the context has dynamic contacts
+    if (colors) dyn_coloring(c, colors);
+    if (num_colors) *num_colors = dyn_num_colors(c);
     return AVBD_OK;
 }
 

@@ -92,15 +92,37 @@ struct DevState {
     V4* jrp = nullptr;               // reference position
     V4* jrq = nullptr;               // reference rotation (quaternion)
     uint8_t* oflag = nullptr;        // per rotation slot, OrientedFlags
+
+    // ---- triangle-rigid contacts (TriangleRigidCollisionEnergyPool), by pool
+    // slot; the host manages the pool between steps (contacts.cu)
+    unsigned trc_cap = 0;            // slots allocated on the device
+    uint4* trc_p = nullptr;          // internal vertex ids: triangle x3, rigid body
+    V4* trc_n = nullptr;             // contact frame: normal, tangent, binormal
+    V4* trc_t = nullptr;
+    V4* trc_b = nullptr;
+    V4* trc_bar = nullptr;           // barycentrics of the triangle point, mu_s in w
+    V4* trc_cpl = nullptr;           // contact point in the body frame, mu_k in w
+    V4* trc_k = nullptr;             // k_n, k_t, k_b, k_start
+    V4* trc_lam = nullptr;           // lam_n, lam_t, lam_b, C_n_prev
+    uint8_t* trc_flag = nullptr;     // ContactFlags
+    // dynamic adjacency per internal vertex: entries (slot << 2 | local);
+    // null when the context has no triangle-sphere pairs
+    uint32_t* dyn_begin = nullptr;   // n + 1
+    uint32_t* dyn_ent = nullptr;
+    uint8_t* dyn_skip = nullptr;     // 1: has contacts or a new color, solved from its color's list, not its slab
+    uint8_t* conflicted = nullptr;   // 1: intra-color conflict, the update is buffered
+    V4* buffered = nullptr;          // buffered positions of conflicted vertices
 };
 
 enum OrientedFlags : uint8_t {
     OF_RGROUND = 1, OF_RG_USE_STATIC = 2, OF_RG_UNCLAMPED = 4, OF_RG_ROUND = 8, OF_JOINT = 16
 };
+enum ContactFlags : uint8_t { CF_ACTIVE = 1, CF_USE_STATIC = 2, CF_UNCLAMPED = 4 };
 
 // Per-scene run-to-tolerance state passed to the solve, Chebyshev and residual
 // kernels.  Null pointers disable the corresponding behaviour.
 struct MlpDevice;  // learned warm-start weights on the device (mlp.cu)
+struct DynHost;    // host side of the dynamic contacts (contacts.cu)
 
 struct SceneTol {
     const uint32_t* scene = nullptr;  // scene of each internal vertex
@@ -242,6 +264,10 @@ struct avbd_ctx {
     float ws_kappa = 0.5f;              // relative error assumed by the acceptance test
     bool ws_recorded = false;
 
+    // dynamic triangle-rigid contacts: pool, recoloring and per-color lists,
+    // managed on the host every step (contacts.cu); null without sphere primitives
+    avbd::DynHost* dyn = nullptr;
+
     avbd_stats stats{};
     std::vector<void*> allocations;
 };
@@ -265,14 +291,38 @@ void launch_ws_save(avbd_ctx* c, DevState<R>& s, void* x0, cudaStream_t st);
 template <typename R>
 void launch_ws_target(avbd_ctx* c, DevState<R>& s, const void* x0, double inv_s, float* t, cudaStream_t st);
 
+// ---- dynamic triangle-rigid contacts (contacts.cu)
+// set-up after the static coloring: keeps the static adjacency and colors
+int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vector<unsigned>& p_nbr,
+               std::string& err);
+void dyn_destroy(avbd_ctx* c);
+// contact handling of the collision stage: merge of the narrow phase's
+// detections into the pool, dynamic adjacency, incremental recoloring, then
+// the contacts' step-start hook (run before the inertial prediction)
+template <typename R>
+int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+// the solve of one color: static slabs (less recolored vertices), recolored
+// vertices of this color, commit of the color's conflicted vertices
+template <typename R>
+void dyn_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned color, cudaStream_t st,
+                     const SceneTol& T);
+template <typename R>
+void launch_trc_after_iter(avbd_ctx* c, DevState<R>& s, cudaStream_t st, const SceneTol& T);
+unsigned dyn_num_colors(const avbd_ctx* c);
+// the positional vertices solved from lists (all colors), for the residual pass
+void dyn_positional_list(const avbd_ctx* c, const uint32_t** list, unsigned* count);
+int dyn_coloring(const avbd_ctx* c, unsigned* colors);
+
 // ---- solve kernels (solve.cu)
 template <typename R>
 void launch_begin_step(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
 template <typename R>
 void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
+// list: when given, the count vertices of list (internal ids) instead of the
+// slab [begin, begin + count)
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, const SceneTol& T = SceneTol());
+                        cudaStream_t st, const SceneTol& T = SceneTol(), const uint32_t* list = nullptr);
 template <typename R>
 void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
                            const SceneTol& T = SceneTol());
@@ -286,7 +336,7 @@ template <typename R>
 void launch_begin_step_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
 template <typename R>
 void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                      cudaStream_t st, const SceneTol& T, int mode, double* out);
+                      cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list = nullptr);
 template <typename R>
 void launch_chebyshev_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
                           const SceneTol& T = SceneTol());

@@ -14,6 +14,7 @@
 // solved by LU with partial pivoting in FP64.
 #include "engine.h"
 #include "s3math.cuh"
+#include "contact_dyn.cuh"
 
 namespace avbd {
 
@@ -374,12 +375,14 @@ enum { RMODE_SOLVE = 0, RMODE_RESIDUAL = 1, RMODE_DEBUG = 2 };
 
 template <typename R, int MODE>
 __global__ void __launch_bounds__(128) k_solve_rod(DevState<R> s, unsigned begin, unsigned count, R dt, double g,
-                                                   double* out, SceneTol T) {
+                                                   double* out, SceneTol T, const uint32_t* __restrict__ list) {
     unsigned gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= count) return;
-    unsigned p = begin + gi;
+    unsigned p = list ? list[gi] : begin + gi;
     uint8_t fl = s.flags[p];
     if (!(fl & VF_ORIENTED) || (fl & VF_FIXED)) return;
+    // a recolored vertex is solved from its new color's list, not its slab
+    if (MODE == RMODE_SOLVE && !list && s.dyn_skip && s.dyn_skip[p]) return;
     if (MODE == RMODE_SOLVE && T.active && !T.active[T.scene[p]]) return;
     if (MODE == RMODE_RESIDUAL && T.cand && !T.cand[T.scene[p]]) return;
     unsigned slot = s.rot[p];
@@ -394,6 +397,9 @@ __global__ void __launch_bounds__(128) k_solve_rod(DevState<R> s, unsigned begin
     uint8_t f = s.oflag[slot];
     if (f & OF_RGROUND) accumulate_rground<R>(s, slot, x, q, B);
     if (f & OF_JOINT) accumulate_joint<R>(s, slot, x, q, B);
+    // dynamic energies (VBDSolver.hpp:397-446): the body's triangle-rigid contacts
+    if (s.dyn_begin)
+        for (unsigned k = s.dyn_begin[p]; k < s.dyn_begin[p + 1]; k++) trc_accumulate6<R>(s, s.dyn_ent[k] >> 2, B);
     typename Vec4Of<R>::T y4 = s.y[p];
     R m = y4.w;
     V3<R> I = xyz(s.Iv[slot]);
@@ -443,6 +449,13 @@ __global__ void __launch_bounds__(128) k_solve_rod(DevState<R> s, unsigned begin
     double dx[6];
     lu_solve_d<6>(A, rhs, dx);
     V3<R> xn = x + mk3<R>((R)dx[0], (R)dx[1], (R)dx[2]);
+    if (s.conflicted && s.conflicted[p]) {
+        // intra-color conflict: the position is buffered and committed after the
+        // color; the rotation update is dropped, as the reference commits
+        // positions only (VBDSolver.hpp:108-119,474-479)
+        s.buffered[p] = make4<R>(xn, R(0));
+        return;
+    }
     s.x[p] = make4<R>(xn, R(0));
     s.q[slot] = q_store(plus_s3_stored(q, mk3<R>((R)dx[3], (R)dx[4], (R)dx[5])));
 }
@@ -524,14 +537,14 @@ void launch_begin_step_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cud
 
 template <typename R>
 void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                      cudaStream_t st, const SceneTol& T, int mode, double* out) {
+                      cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list) {
     if (count == 0) return;
     if (mode == RMODE_RESIDUAL)
-        k_solve_rod<R, RMODE_RESIDUAL><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T);
+        k_solve_rod<R, RMODE_RESIDUAL><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     else if (mode == RMODE_DEBUG)
-        k_solve_rod<R, RMODE_DEBUG><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T);
+        k_solve_rod<R, RMODE_DEBUG><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     else
-        k_solve_rod<R, RMODE_SOLVE><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T);
+        k_solve_rod<R, RMODE_SOLVE><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     count_launch(c);
 }
 
@@ -561,7 +574,7 @@ void launch_store_rot(const DevState<R>& s, int which, double* dst, const uint32
 #define INST(R)                                                                                                 \
     template void launch_begin_step_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);         \
     template void launch_solve_rod<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,          \
-                                      cudaStream_t, const SceneTol&, int, double*);                            \
+                                      cudaStream_t, const SceneTol&, int, double*, const uint32_t*);           \
     template void launch_chebyshev_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t,    \
                                           const SceneTol&);                                                     \
     template void launch_velocity_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);            \

@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 
 #include "engine.h"
+#include "contact_dyn.cuh"
 
 namespace avbd {
 
@@ -277,6 +278,7 @@ AVBD_D void reduce_block(Block3<P, HT>& B) {
 
 enum { MODE_SOLVE = 0, MODE_RESIDUAL = 1, MODE_DEBUG = 2, MODE_FEATURES = 3 };
 
+
 // Vertex block solve of one color slab: LANES threads per vertex stream the
 // vertex's incidence records, each lane accumulating its tets, then a shuffle
 // reduction and the 3x3 solve by the group's first lane.  MODE_RESIDUAL
@@ -293,18 +295,24 @@ struct SolveMinBlocks {
     static constexpr int value = sizeof(P) == 4 ? 4 : (sizeof(RS) == 4 ? 3 : 1);
 };
 
-template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE>
+// DYN: the instantiation for vertices with dynamic contact energies or a
+// color changed by the recoloring, launched over per-color lists; the slab
+// launches (DYN false) skip those vertices and carry no dynamic code.
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
 __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
                                                    unsigned long long* counters, double* out, SceneTol T,
-                                                   const float4* __restrict__ aux) {
+                                                   const float4* __restrict__ aux, const uint32_t* __restrict__ list) {
     unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned gi = tid / LANES;
     unsigned lane = tid % LANES;
     bool active = gi < count;
-    unsigned p = begin + (active ? gi : 0);
+    unsigned p = list ? (active ? list[gi] : 0u) : begin + (active ? gi : 0);
     uint8_t fl = active ? s.flags[p] : 0;
     if (MODE != MODE_SOLVE && (fl & (VF_FIXED | VF_ORIENTED))) active = false;
+    // vertices with dynamic contacts or a new color are solved from their color's list
+    if ((MODE == MODE_SOLVE || MODE == MODE_RESIDUAL) && !DYN && s.dyn_skip && active && s.dyn_skip[p])
+        active = false;
     // per-scene run-to-tolerance: converged scenes are skipped before any record is read
     if (MODE == MODE_SOLVE && T.active && active && !T.active[T.scene[p]]) active = false;
     if (MODE == MODE_RESIDUAL && T.cand && active && !T.cand[T.scene[p]]) active = false;
@@ -360,6 +368,14 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
     double r2 = 0.0, mg2 = 0.0;
     if (active && lane == 0) {
         if (GROUND && (fl & VF_GROUND)) accumulate_ground<P, HT>(s, p, xi, B);
+        if constexpr (DYN) {
+            // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid contacts in slot order
+            const unsigned e = s.dyn_begin[p + 1];
+            for (unsigned k = s.dyn_begin[p]; k < e; k++) {
+                const uint32_t en = s.dyn_ent[k];
+                trc_accumulate3<P, HT>(s, en >> 2, en & 3u, B);
+            }
+        }
         typename Vec4Of<P>::T y4 = s.y[p];
         P m = y4.w;
         P cm = m * c.inv_dt2;
@@ -384,7 +400,9 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
                 atomicAdd(counters, 1ull);
             }
             typename Vec4Of<P>::T o = make4<P>(xi + dx, P(0));
-            s.x[p] = o;
+            // an intra-color conflict buffers the update (VBDSolver.hpp:505-509)
+            if (DYN && s.conflicted[p]) s.buffered[p] = o;
+            else s.x[p] = o;
         } else if constexpr (MODE == MODE_FEATURES) {
             // feature layout of avbd_warmstart_sample (include/avbd.h)
             Sym3<P> A{cm + (P)B.h00, cm + (P)B.h11, cm + (P)B.h22, (P)B.h01, (P)B.h02, (P)B.h12};
@@ -586,9 +604,9 @@ void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStre
     count_launch(c);
 }
 
-template <typename P, typename RS, typename HT, int LANES, int MODE>
+template <typename P, typename RS, typename HT, int LANES, int MODE, bool DYN = false>
 static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
-                           unsigned count, cudaStream_t st, double* out, const SceneTol& T) {
+                           unsigned count, cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list) {
     unsigned threads = count * LANES;
     unsigned blocks = nblocks(threads, 256);
     if (blocks == 0) return;
@@ -597,13 +615,13 @@ static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, c
     auto* ctr = c->d_counters;
     const float4* aux = reinterpret_cast<const float4*>(c->ws_prev_arg);
     if (damp && ground)
-        k_solve_tet<P, RS, HT, LANES, true, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
+        k_solve_tet<P, RS, HT, LANES, true, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
     else if (damp)
-        k_solve_tet<P, RS, HT, LANES, true, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
+        k_solve_tet<P, RS, HT, LANES, true, false, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
     else if (ground)
-        k_solve_tet<P, RS, HT, LANES, false, true, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
+        k_solve_tet<P, RS, HT, LANES, false, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
     else
-        k_solve_tet<P, RS, HT, LANES, false, false, MODE><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux);
+        k_solve_tet<P, RS, HT, LANES, false, false, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
     count_launch(c);
 }
 
@@ -613,17 +631,21 @@ static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, c
 // uses 8.
 template <typename P, typename RS, typename HT, int MODE>
 static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
-                          unsigned count, cudaStream_t st, double* out, const SceneTol& T) {
+                          unsigned count, cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list) {
     if constexpr (MODE == MODE_DEBUG) {
-        solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T);
+        if (c->dyn) solve_dispatch<P, RS, HT, 8, MODE, true>(c, s, inc, k, begin, count, st, out, T, list);
+        else solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T, list);
+    } else if (list) {
+        if constexpr (MODE == MODE_SOLVE || MODE == MODE_RESIDUAL)
+            solve_dispatch<P, RS, HT, 8, MODE, true>(c, s, inc, k, begin, count, st, out, T, list);
     } else {
         switch (c->lanes) {
-            case 1: solve_dispatch<P, RS, HT, 1, MODE>(c, s, inc, k, begin, count, st, out, T); break;
-            case 2: solve_dispatch<P, RS, HT, 2, MODE>(c, s, inc, k, begin, count, st, out, T); break;
-            case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, begin, count, st, out, T); break;
-            case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, begin, count, st, out, T); break;
-            case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, begin, count, st, out, T); break;
-            default: solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T); break;
+            case 1: solve_dispatch<P, RS, HT, 1, MODE>(c, s, inc, k, begin, count, st, out, T, list); break;
+            case 2: solve_dispatch<P, RS, HT, 2, MODE>(c, s, inc, k, begin, count, st, out, T, list); break;
+            case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, begin, count, st, out, T, list); break;
+            case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, begin, count, st, out, T, list); break;
+            case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, begin, count, st, out, T, list); break;
+            default: solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T, list); break;
         }
     }
 }
@@ -632,22 +654,22 @@ static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, co
 // state and gradient, float records and Hessian.
 template <int MODE>
 static void solve_lanes(avbd_ctx* c, DevState<float>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out, const SceneTol& T) {
-    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out, T);
+                        cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list = nullptr) {
+    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out, T, list);
 }
 template <int MODE>
 static void solve_lanes(avbd_ctx* c, DevState<double>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out, const SceneTol& T) {
+                        cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list = nullptr) {
     if (c->solver.precision == AVBD_PRECISION_MIXED)
-        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out, T);
+        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out, T, list);
     else
-        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out, T);
+        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out, T, list);
 }
 
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, const SceneTol& T) {
-    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr, T);
+                        cudaStream_t st, const SceneTol& T, const uint32_t* list) {
+    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr, T, list);
 }
 
 template <typename R>
@@ -669,6 +691,12 @@ void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* o
                      const SceneTol& T) {
     if (out2) cudaMemsetAsync(out2, 0, 2 * sizeof(double), st);
     solve_lanes<MODE_RESIDUAL>(c, s, k, 0, s.n, st, out2, T);
+    if (c->dyn) {  // the positional vertices the slab pass skipped
+        const uint32_t* list = nullptr;
+        unsigned m = 0;
+        dyn_positional_list(c, &list, &m);
+        if (m) solve_lanes<MODE_RESIDUAL>(c, s, k, 0, m, st, out2, T, list);
+    }
 }
 
 // ------------------------------------------- per-scene run-to-tolerance
@@ -822,7 +850,7 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
     template void launch_begin_step<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);               \
     template void launch_tet_eprev<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                \
     template void launch_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,         \
-                                        cudaStream_t, const SceneTol&);                                         \
+                                        cudaStream_t, const SceneTol&, const uint32_t*);                        \
     template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t,    \
                                            const SceneTol&);                                                    \
     template void launch_velocity<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                 \

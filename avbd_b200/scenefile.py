@@ -29,9 +29,11 @@ uses and builds a `scenes.Scene` whose replay is the reference's set-up
   (Simulation.hpp:108-137): tet vertices k_start = m/h^2, mu 0.4 / 0.2; rod
   nodes and spheres rigid-body ground with mu 0.5 / 0.2.
 
-Sphere collision primitives are left out unless `sphere_primitives=True`: the
-narrow phase for sphere pairs is not part of this engine, and the reference
-throws on sphere-rod and sphere-sphere pairs (collision/CollisionDetector.cpp:180-213).
+Sphere collision primitives are left out unless `sphere_primitives=True`:
+with them, spheres near rods or near each other give sphere-rod and
+sphere-sphere candidate pairs, on which the reference throws
+(collision/CollisionDetector.cpp:180-213,678-687) and the engine returns
+AVBD_ERR_UNSUPPORTED_PAIR; triangle-sphere pairs become contact energies.
 """
 from __future__ import annotations
 

@@ -293,6 +293,34 @@ def add_sphere(sc: Scene, radius: float, density: float, position, ground=True):
     return base
 
 
+def spheres_on_cube(n: int = 4, num_spheres: int = 4, seed: int = 0, iters: int = 20, rho: float = 0.5,
+                    dt: float = 1.0 / 60.0, size: float = 1.0, E: float = 1e5, nu: float = 0.4,
+                    radius=(0.08, 0.15), drop: float = 0.02, speed: float = 1.0, sphere_density: float = 500.0,
+                    fix_bottom: bool = True) -> Scene:
+    """Rigid spheres dropped on a soft tet cube: a cube of n^3 cells (E, nu,
+    rho 1000) with its bottom face fixed (or resting on the ground when
+    fix_bottom is False) and its surface triangles as collision primitives;
+    spheres of seeded radius ~ U(radius) spread over the top face, `drop`
+    above it and falling at `speed`, each a collision sphere of its own object
+    with rigid-body ground contact.  Their contacts with the cube's surface are
+    the triangle-rigid contact energies of the collision stage."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(name=f"cube{n}_spheres{num_spheres}", dt=dt, solver_iters=iters, iter_acceleration=rho)
+    add_tet_cube(sc, n, size=size, E=E, nu=nu, density=1000.0, fix_bottom=fix_bottom, ground=not fix_bottom,
+                 surface=True, object_id=0)
+    side = int(np.ceil(np.sqrt(num_spheres)))
+    for s in range(num_spheres):
+        r = rng.uniform(*radius)
+        cx = (s % side + 0.5) / side * size + rng.uniform(-0.05, 0.05) * size / side
+        cz = (s // side + 0.5) / side * size + rng.uniform(-0.05, 0.05) * size / side
+        base = add_sphere(sc, r, sphere_density, (cx, size + r + drop, cz))
+        vel = np.array([[0.0, -speed, 0.0]])
+        sc.record("set_velocities", base, vel, vel)
+        sc.record("add_spheres", [base], [r], [1 + s])
+        sc.num_primitives += 1
+    return sc
+
+
 def rods_and_spheres(num_rods: int = 256, segments: int = 100, num_spheres: int = 64, seed: int = 0,
                      iters: int = 20, rho: float = 0.5, dt: float = 1.0 / 60.0, length: float = 1.0,
                      helix_radius: float = 0.02, spacing: float = 0.1) -> Scene:

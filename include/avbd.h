@@ -265,11 +265,40 @@ AVBD_API int avbd_get_candidate_pairs(avbd_ctx* ctx, unsigned capacity, unsigned
  * sphere's particle slot; vec9 = contact normal (world), barycentrics of the
  * contact point on the triangle, contact point on the sphere in its body
  * frame.  Up to `capacity` contacts are written (pointers may be NULL);
- * *count receives the number found.  The contact energies these detections
- * create in the reference (TriangleRigidCollisionEnergy) are not part of
- * this engine's step. */
+ * *count receives the number found.  Inside avbd_step these detections
+ * become the triangle-rigid contact energies below. */
 AVBD_API int avbd_get_contacts(avbd_ctx* ctx, unsigned capacity, uint64_t* keys, unsigned* idx4, double* vec9,
                                unsigned* count);
+
+/* Dynamic contact state after the last step's collision stage (contexts
+ * with triangle and sphere primitives; zeros otherwise): out[0] live
+ * triangle-rigid contacts, out[1] pool size (highest slot + 1,
+ * TombstonePool::totalSize, common/TombstonePool.hpp:53), out[2] colors after
+ * the incremental recoloring (ColorList::incrementalRecoloring,
+ * common/ColorList.hpp:381-474), out[3] conflicted particles
+ * (ColorList::finalizeConflicts, :476-522), out[4] particles left dirty for
+ * the next stage, out[5] dynamic adjacency entries
+ * (DynamicParticleAdjacency::buildAdjacency,
+ * common/DynamicParticleAdjacency.hpp:33-118). */
+AVBD_API int avbd_dynamic_info(avbd_ctx* ctx, unsigned out[6]);
+
+/* The triangle-rigid contact pool (TriangleRigidCollisionEnergyPool,
+ * energy/collision/TriangleRigidCollisionEnergyPool.hpp:10-78) by slot, slots
+ * [0, min(capacity, pool size)): p4 = the triangle's three particle slots and
+ * the rigid body's; active[s] = 1 for a live slot; data24 = per slot the
+ * normal, tangent, binormal, barycentrics, contact point in the body frame
+ * (3 each), k_start, k_n, k_t, k_b, lambda_n, lambda_t, lambda_b, C_n_prev,
+ * and flags (1 static friction, 2 unclamped friction) as a double.  Values
+ * as of the device state when called.  Pointers may be NULL; *size receives
+ * the pool size. */
+AVBD_API int avbd_get_contact_pool(avbd_ctx* ctx, unsigned capacity, unsigned* p4, uint8_t* active, double* data24,
+                                   unsigned* size);
+
+/* Test hook: the round limit of the incremental recoloring (6 in the
+ * reference, ColorList.hpp:384).  Fewer rounds leave more particles
+ * conflicted, which exercises the conflict buffering of the solve
+ * (VBDSolver.hpp:82-87,108-119,474-509). */
+AVBD_API int avbd_debug_set_recolor_rounds(avbd_ctx* ctx, unsigned rounds);
 
 /* Block gradient and Hessian of particle p at the current state: the
  * grad/hess accumulated by VBDSolver::_solveParticle<DOF>

@@ -304,6 +304,9 @@ struct Joint {
     double k[6], lam[6], cprev[6];
     V3 pos_off; Q4 rot_off; V3 ref_p; Q4 ref_q;
 };
+// TriangleRigidCollisionEnergyInfo (energy/collision/TriangleRigidCollisionEnergyPool.hpp:10-16):
+// p[0..2] the triangle's vertices, p[3] the rigid body
+struct TriRigid : Contact { unsigned p[4]; V3 barys, cp_local; };
 struct Prim { uint8_t type; unsigned idx[3]; uint8_t np; unsigned object_id; double radius; };
 struct Entry { uint8_t type; unsigned idx; uint16_t local; };
 
@@ -360,8 +363,25 @@ struct Ctx {
     unsigned root = 0;
     std::vector<std::pair<unsigned, unsigned>> pairs;
     // detected triangle-sphere contacts of the last collision stage, ascending key
-    struct Detected { uint64_t key; unsigned tri[3], rb; V3 normal, barys, cp_local; };
-    std::vector<Detected> contacts;
+    struct Detected { uint64_t key; unsigned tri[3], rb; V3 normal, barys, cp_local; unsigned e_idx = 0; };
+    std::vector<Detected> detected;                 // narrow-phase output of the last stage
+    std::vector<Detected> contacts, prev_contacts;  // managed detections with their pool slots
+
+    // TriangleRigidCollisionEnergyPool over a TombstonePool (common/TombstonePool.hpp:13-103)
+    std::vector<TriRigid> trc;
+    std::vector<uint8_t> trc_active;
+    std::vector<unsigned> trc_slots;        // free-slot stack
+    unsigned trc_top = 0, trc_high = 0, trc_count = 0;
+    // DynamicParticleAdjacency (common/DynamicParticleAdjacency.hpp:17-118)
+    std::vector<unsigned> dyn_off;          // np + 1
+    std::vector<std::pair<unsigned, uint16_t>> dyn_ent;   // (slot, local)
+    std::vector<unsigned> dnb_off, dnb;
+    // ColorList incremental recoloring state (common/ColorList.hpp:62-90)
+    std::vector<unsigned> last_dirty, dirty, next_dirty, touched_frame, cand_color, touched_conflicted;
+    std::vector<uint8_t> conflicted;
+    std::vector<unsigned> conf_off, conf_list;   // conflicted particles per color
+    std::vector<V3> buffered;               // buffered positions of conflicted particles
+    unsigned recolor_rounds = 6;            // incrementalRecoloring's MAX_COLOR_ITERS
 
     // statistics
     double last_residual = -1;
@@ -631,6 +651,49 @@ static void rground_accumulate(const Ctx& c, const RGround& e, double H[6][6], d
     contact_accumulate<6>(e, Cn, Ct, Cb, gn, gt, gb, hn, ht, hb, H, G);
 }
 
+// TriangleRigidCollisionConstraintSolver::evaluateConstraint
+// (energy/collision/TriangleRigidCollisionEnergySolver.hpp:14-41)
+static void trc_eval(const Ctx& c, const TriRigid& e, double& Cn, double& Ct, double& Cb) {
+    V3 cp_tri = e.barys.x * c.x[e.p[0]] + e.barys.y * c.x[e.p[1]] + e.barys.z * c.x[e.p[2]];
+    V3 cp_rb = c.x[e.p[3]] + qrot(c.q[c.rot[e.p[3]]], e.cp_local);
+    V3 d = cp_rb - cp_tri;
+    Cn = dot(e.n, d); Ct = dot(e.t, d); Cb = dot(e.b, d);
+}
+
+// TriangleRigidCollisionConstraintSolver::constraintGradientHessian
+// (energy/collision/TriangleRigidCollisionEnergySolver.hpp:43-118) inside
+// CollisionConstraintEnergySolver::accumulate<DOF>.  A triangle vertex (DOF 3)
+// has gradients -bary (n, t, b) and no constraint Hessian.  The rigid body
+// (DOF 6) has the normal's gradient (n, -(R S)^T n) with S = skew(cp_local),
+// zero tangent and binormal gradients (the reference overwrites them), and
+// rotational Hessian blocks sym(R^T skew(d) R S) for d = n, t, b.
+template <int DOF>
+static void trc_accumulate(const Ctx& c, const TriRigid& e, unsigned local, double H[DOF][DOF], double G[DOF]) {
+    double Cn, Ct, Cb;
+    trc_eval(c, e, Cn, Ct, Cb);
+    double gn[DOF] = {}, gt[DOF] = {}, gb[DOF] = {};
+    if constexpr (DOF == 6) {
+        M3 R = qmat(c.q[c.rot[e.p[3]]]);
+        M3 S = skew(e.cp_local);
+        M3 RS = R * S;
+        double hn[6][6] = {}, ht[6][6] = {}, hb[6][6] = {};
+        for (int i = 0; i < 3; i++) gn[i] = e.n[i];
+        for (int j = 0; j < 3; j++) gn[3 + j] = -(e.n.x * RS.a[0][j] + e.n.y * RS.a[1][j] + e.n.z * RS.a[2][j]);
+        auto rot_hess = [&](V3 d, double h[6][6]) {
+            M3 Hd = R.T() * skew(d) * R * S;
+            M3 Hs = 0.5 * (Hd + Hd.T());
+            for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) h[3 + i][3 + j] = Hs.a[i][j];
+        };
+        rot_hess(e.n, hn); rot_hess(e.t, ht); rot_hess(e.b, hb);
+        contact_accumulate<6>(e, Cn, Ct, Cb, gn, gt, gb, hn, ht, hb, (double(*)[6])H, G);
+    } else {
+        if (local >= 3) throw std::runtime_error("TriangleRigidCollisionEnergySolver::constraintGradientHessian local_idx out of bounds!");
+        double br = e.barys[local];
+        for (int i = 0; i < 3; i++) { gn[i] = -br * e.n[i]; gt[i] = -br * e.t[i]; gb[i] = -br * e.b[i]; }
+        contact_accumulate<DOF>(e, Cn, Ct, Cb, gn, gt, gb, nullptr, nullptr, nullptr, H, G);
+    }
+}
+
 // OneSidedFixedJointConstraintSolver::evaluateConstraint
 // (energy/joint/OneSidedFixedJointEnergySolver.hpp:16-34)
 static void joint_eval(const Ctx& c, const Joint& e, double C[6]) {
@@ -730,6 +793,10 @@ static void accumulate_block(const Ctx& c, unsigned p, double H[DOF][DOF], doubl
                 break;
         }
     }
+    // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid contacts in slot order
+    if (!c.dyn_off.empty())
+        for (unsigned k = c.dyn_off[p]; k < c.dyn_off[p + 1]; k++)
+            trc_accumulate<DOF>(c, c.trc[c.dyn_ent[k].first], c.dyn_ent[k].second, H, G);
 }
 
 // VBDSolver::_solveParticle<DOF> assembly and solve (simulation/VBDSolver.hpp:449-510)
@@ -755,8 +822,14 @@ static void solve_particle(Ctx& c, unsigned p) {
         }
         double dx[6];
         lu_solve<6>(H, rhs, dx);
-        c.x[p] += V3(dx[0], dx[1], dx[2]);
-        c.q[r] = plus_s3(c.q[r], V3(dx[3], dx[4], dx[5]));
+        if (!c.conflicted.empty() && c.conflicted[p]) {
+            // intra-color conflict: the update is buffered; _commitConflictedInColor
+            // later copies the position only, so the rotation update is dropped
+            c.buffered[p] = c.x[p] + V3(dx[0], dx[1], dx[2]);
+        } else {
+            c.x[p] += V3(dx[0], dx[1], dx[2]);
+            c.q[r] = plus_s3(c.q[r], V3(dx[3], dx[4], dx[5]));
+        }
     } else {
         double H[3][3], G[3];
         accumulate_block<3>(c, p, H, G);
@@ -768,7 +841,8 @@ static void solve_particle(Ctx& c, unsigned p) {
         if (!c.sweep_r2.empty()) c.sweep_r2[p] = rhs[0] * rhs[0] + rhs[1] * rhs[1] + rhs[2] * rhs[2];
         double dx[3];
         lu_solve<3>(H, rhs, dx);
-        c.x[p] += V3(dx[0], dx[1], dx[2]);
+        if (!c.conflicted.empty() && c.conflicted[p]) c.buffered[p] = c.x[p] + V3(dx[0], dx[1], dx[2]);
+        else c.x[p] += V3(dx[0], dx[1], dx[2]);
     }
 }
 
@@ -899,6 +973,13 @@ static void after_time_step(Ctx& c) {
         rground_eval(c, e, Cn, Ct, Cb);
         contact_after_step(e, Cn);
     }
+    // TriangleRigidCollisionEnergySolver::updateAfterTimeStep over the live slots
+    for (unsigned i = 0; i < c.trc.size(); i++) {
+        if (!c.trc_active[i]) continue;
+        double Cn, Ct, Cb;
+        trc_eval(c, c.trc[i], Cn, Ct, Cb);
+        contact_after_step(c.trc[i], Cn);
+    }
     for (auto& e : c.joints) joint_after_step(c, e, c.joint_k_start);
 }
 
@@ -919,17 +1000,23 @@ static void after_iteration(Ctx& c) {
         rground_eval(c, e, Cn, Ct, Cb);
         contact_after_iter(e, Cn, Ct, Cb);
     }
+    for (unsigned i = 0; i < c.trc.size(); i++) {
+        if (!c.trc_active[i] || !scene_on(c, c.trc[i].p[3])) continue;
+        double Cn, Ct, Cb;
+        trc_eval(c, c.trc[i], Cn, Ct, Cb);
+        contact_after_iter(c.trc[i], Cn, Ct, Cb);
+    }
     for (auto& e : c.joints)
         if (scene_on(c, e.p)) joint_after_iter(c, e);
 }
 
-static void collision_stage(Ctx& c);
+static void collision_stage(Ctx& c, bool manage);
 
 // VBDSolver::solve_Parallel (simulation/VBDSolver.hpp:48-103) preceded by the
 // collision stage of SimulationExecutor::_workerTimeStep
 // (simulation/SimulationExecutor.hpp:142-156).
 static void time_step(Ctx& c) {
-    if (!c.prims.empty()) collision_stage(c);
+    if (!c.prims.empty()) collision_stage(c, true);
     after_time_step(c);
     long n = (long)c.np();
     c.pool.parallel_for(0, n, [&](long p) { inertial(c, (unsigned)p); });
@@ -961,6 +1048,14 @@ static void time_step(Ctx& c) {
         for (unsigned col = 0; col < c.num_colors; col++) {
             c.pool.parallel_for(c.color_offsets[col], c.color_offsets[col + 1],
                                 [&](long k) { solve_particle(c, c.work_list[k]); });
+            // VBDSolver::_commitConflictedInColor (simulation/VBDSolver.hpp:82-87,108-119).
+            // A fixed conflicted particle never writes its buffer; the reference
+            // then copies an uninitialised buffer, here it keeps its position.
+            if (col + 1 < c.conf_off.size())
+                for (unsigned k = c.conf_off[col]; k < c.conf_off[col + 1]; k++) {
+                    unsigned q = c.conf_list[k];
+                    if (!c.fixed[q] && scene_on(c, q)) c.x[q] = c.buffered[q];
+                }
         }
         c.pool.parallel_for(0, n, [&](long p) {
             if (scene_on(c, (unsigned)p)) chebyshev(c, (unsigned)p, omega);
@@ -1440,7 +1535,7 @@ static inline uint64_t collision_key(unsigned type, unsigned a, unsigned b, unsi
 // (DetectedCollisionType::TriangleRigid = 2).  Detections are kept in
 // ascending key order, as _handleDetectedCollisions sorts them.
 static void narrow_phase(Ctx& c) {
-    c.contacts.clear();
+    c.detected.clear();
     for (auto [la, lb] : c.pairs) {
         unsigned a = c.sorted[la], b = c.sorted[lb];
         const Prim& A = c.prims[a];
@@ -1455,25 +1550,272 @@ static void narrow_phase(Ctx& c) {
         if (c.prims[ia].type > c.prims[ib].type) std::swap(ia, ib);
         const Prim& P = c.prims[ia];
         const Prim& Q = c.prims[ib];
+        // sphere-rod has no case and sphere-sphere throws (CollisionDetector.cpp:180-213,678-687)
+        if (Q.type == 2 && P.type != 0) throw std::runtime_error("Unsupported collision!");
         if (P.type == 0 && Q.type == 2) {
             Ctx::Detected d;
             if (tri_sphere_ccd(c, P, Q, d.normal, d.barys, d.cp_local)) {
                 d.key = collision_key(2, ia, ib, 0);
                 d.tri[0] = P.idx[0]; d.tri[1] = P.idx[1]; d.tri[2] = P.idx[2];
                 d.rb = Q.idx[0];
-                c.contacts.push_back(d);
+                c.detected.push_back(d);
             }
         }
     }
-    std::stable_sort(c.contacts.begin(), c.contacts.end(),
+    std::stable_sort(c.detected.begin(), c.detected.end(),
                      [](const Ctx::Detected& x, const Ctx::Detected& y) { return x.key < y.key; });
+}
+
+// ------------------------------------------------ dynamic contact energies
+static constexpr unsigned DIRTY_SENTINEL = 0xFFFFFFFFu;   // ColorList::SENTINEL
+
+// Eigen's MatrixBase::unitOrthogonal for a 3-vector (Eigen 3.3+, the
+// third-party library of the reference; the published behaviour: a unit
+// vector orthogonal to v, built from (x, y) unless both are negligible next
+// to z at dummy precision 1e-12, then from (y, z)).
+static V3 unit_orthogonal(V3 v) {
+    const double prec = 1e-12;
+    auto negligible = [&](double a, double b) { return std::fabs(a) <= std::fabs(b) * prec; };
+    if (!negligible(v.x, v.z) || !negligible(v.y, v.z)) {
+        double inv = 1.0 / std::sqrt(v.x * v.x + v.y * v.y);
+        return V3(-v.y * inv, v.x * inv, 0.0);
+    }
+    double inv = 1.0 / std::sqrt(v.y * v.y + v.z * v.z);
+    return V3(0.0, -v.z * inv, v.y * inv);
+}
+
+// Math::completeOrthonormalBasisGivenNormal (common/Math.hpp:323-327)
+static void normal_basis(V3 n, V3& t, V3& b) {
+    t = unit_orthogonal(n);
+    b = cross(n, t);
+}
+
+// CollisionConstraintEnergySolver::updateCollisionFrame
+// (energy/collision/CollisionConstraintEnergySolver.hpp:17-53): the tangent is
+// carried over by projection, the friction multipliers keep the force
+static void update_frame(Contact& e, V3 nn) {
+    V3 f = e.lam_t * e.t + e.lam_b * e.b;
+    V3 tp = e.t - dot(e.t, nn) * nn;
+    double m = norm(tp);
+    if (m > 1e-8) {
+        e.t = tp / m;
+        e.b = cross(nn, e.t);
+    } else {
+        normal_basis(nn, e.t, e.b);
+    }
+    e.n = nn;
+    e.lam_t = dot(f, e.t);
+    e.lam_b = dot(f, e.b);
+}
+
+// TombstonePool::allocSlot / freeSlot (common/TombstonePool.hpp:56-103).  The
+// stack grows on demand; a slot never reached holds its own index, as the
+// reference's iota-initialised stack does.  freeSlot's lowering of
+// highest_index runs while the freed slot is still active, so it never
+// lowers; the live slots are always a subset of [0, size).
+static unsigned trc_alloc(Ctx& c) {
+    if (c.trc_top == c.trc_slots.size()) c.trc_slots.push_back((unsigned)c.trc_slots.size());
+    unsigned slot = c.trc_slots[c.trc_top++];
+    if (slot >= c.trc.size()) {
+        c.trc.resize(slot + 1);
+        c.trc_active.resize(slot + 1, 0);
+    }
+    c.trc_active[slot] = 1;
+    c.trc_count++;
+    c.trc_high = std::max(c.trc_high, slot);
+    return slot;
+}
+static void trc_free(Ctx& c, unsigned slot) {
+    if (slot >= c.trc_active.size() || !c.trc_active[slot]) throw std::runtime_error("freeSlot called on inactive slot");
+    c.trc_active[slot] = 0;
+    c.trc_count--;
+    c.trc_slots[--c.trc_top] = slot;
+}
+
+// ColorList::markParticleDirty (common/ColorList.hpp:365-378)
+static void mark_dirty(Ctx& c, unsigned p) {
+    if (c.last_dirty[p] != 0) {
+        c.last_dirty[p] = 0;
+        c.touched_frame.push_back(p);
+        c.dirty.push_back(p);
+    }
+}
+
+// CollisionDetector::_addCollision, TriangleRigid case (collision/CollisionDetector.cpp:336-378)
+static void add_contact(Ctx& c, Ctx::Detected& d) {
+    double mn = std::min({c.m[d.tri[0]], c.m[d.tri[1]], c.m[d.tri[2]], c.m[d.rb]});
+    double ks = mn / (c.dt * c.dt);
+    V3 t, b;
+    normal_basis(d.normal, t, b);
+    unsigned slot = trc_alloc(c);
+    TriRigid& e = c.trc[slot];
+    e = TriRigid{};
+    // CollisionConstraintEnergyPool::addEnergy (energy/collision/CollisionConstraintEnergyPool.hpp:48-69)
+    e.lam_n = e.lam_t = e.lam_b = 0;
+    e.k_start = e.k_n = e.k_t = e.k_b = ks;
+    e.cn_prev = 0;
+    e.mu_s = 0.4; e.mu_k = 0.2;
+    e.use_static = false; e.unclamped = false;
+    e.p[0] = d.tri[0]; e.p[1] = d.tri[1]; e.p[2] = d.tri[2]; e.p[3] = d.rb;
+    e.n = d.normal; e.t = t; e.b = b;
+    e.barys = d.barys;
+    e.cp_local = d.cp_local;
+    d.e_idx = slot;
+    for (int k = 0; k < 3; k++) mark_dirty(c, d.tri[k]);
+    mark_dirty(c, d.rb);
+}
+
+// CollisionDetector::_updateCollision, TriangleRigid case (collision/CollisionDetector.cpp:474-481)
+static void update_contact(Ctx& c, const Ctx::Detected& d) {
+    TriRigid& e = c.trc[d.e_idx];
+    e.cp_local = d.cp_local;
+    e.barys = d.barys;
+    update_frame(e, d.normal);
+}
+
+// CollisionDetector::_handleDetectedCollisions (collision/CollisionDetector.cpp:265-318):
+// merge of this stage's detections with the last stage's, both in ascending
+// key order.  Collision primitives are never removed here, so the generation
+// check of equal keys always passes.
+static void handle_detections(Ctx& c) {
+    auto& cur = c.contacts;
+    auto& prev = c.prev_contacts;
+    size_t i = 0, j = 0;
+    while (i < cur.size() && j < prev.size()) {
+        if (cur[i].key < prev[j].key) {
+            add_contact(c, cur[i++]);
+        } else if (cur[i].key > prev[j].key) {
+            trc_free(c, prev[j++].e_idx);
+        } else {
+            cur[i].e_idx = prev[j].e_idx;
+            update_contact(c, cur[i]);
+            i++;
+            j++;
+        }
+    }
+    for (; i < cur.size(); i++) add_contact(c, cur[i]);
+    for (; j < prev.size(); j++) trc_free(c, prev[j].e_idx);
+}
+
+// DynamicParticleAdjacency::buildAdjacency (common/DynamicParticleAdjacency.hpp:33-118):
+// per particle its contact entries in slot order; neighbours with repeats
+static void build_dynamic_adjacency(Ctx& c) {
+    const unsigned n = c.np();
+    c.dyn_off.assign(n + 1, 0);
+    c.dnb_off.assign(n + 1, 0);
+    for (unsigned s = 0; s < c.trc.size(); s++) {
+        if (!c.trc_active[s]) continue;
+        for (int k = 0; k < 4; k++) { c.dyn_off[c.trc[s].p[k] + 1]++; c.dnb_off[c.trc[s].p[k] + 1] += 3; }
+    }
+    for (unsigned p = 0; p < n; p++) { c.dyn_off[p + 1] += c.dyn_off[p]; c.dnb_off[p + 1] += c.dnb_off[p]; }
+    c.dyn_ent.assign(c.dyn_off[n], {0u, (uint16_t)0});
+    c.dnb.assign(c.dnb_off[n], 0);
+    std::vector<unsigned> ec(c.dyn_off.begin(), c.dyn_off.end() - 1), nc(c.dnb_off.begin(), c.dnb_off.end() - 1);
+    for (unsigned s = 0; s < c.trc.size(); s++) {
+        if (!c.trc_active[s]) continue;
+        const TriRigid& e = c.trc[s];
+        for (int k = 0; k < 4; k++) {
+            unsigned p = e.p[k];
+            c.dyn_ent[ec[p]++] = {s, (uint16_t)k};
+            for (int k2 = 0; k2 < 4; k2++)
+                if (k2 != k) c.dnb[nc[p]++] = e.p[k2];
+        }
+    }
+}
+
+// ForEachNeighbor (common/ColorList.hpp:41-60): static, then dynamic neighbours
+template <typename F>
+static void for_each_neighbor(const Ctx& c, unsigned p, F&& f) {
+    for (unsigned k = c.p_off[p]; k < c.p_off[p + 1]; k++) f(c.p_nbr[k]);
+    if (!c.dnb_off.empty())
+        for (unsigned k = c.dnb_off[p]; k < c.dnb_off[p + 1]; k++) f(c.dnb[k]);
+}
+
+// ColorList::finalizeConflicts (common/ColorList.hpp:476-522)
+static void finalize_conflicts(Ctx& c) {
+    for (unsigned p : c.dirty)
+        for_each_neighbor(c, p, [&](unsigned q) {
+            if (c.color[q] == c.color[p]) {
+                if (!c.conflicted[p]) { c.conflicted[p] = 1; c.touched_conflicted.push_back(p); }
+                if (!c.conflicted[q]) { c.conflicted[q] = 1; c.touched_conflicted.push_back(q); }
+            }
+        });
+    std::vector<unsigned> cnt(c.num_colors, 0);
+    for (unsigned p : c.touched_conflicted) cnt[c.color[p]]++;
+    c.conf_off.assign(c.num_colors + 1, 0);
+    for (unsigned k = 0; k < c.num_colors; k++) c.conf_off[k + 1] = c.conf_off[k] + cnt[k];
+    c.conf_list.assign(c.conf_off.back(), 0);
+    std::vector<unsigned> cur(c.conf_off.begin(), c.conf_off.end() - 1);
+    for (unsigned p : c.touched_conflicted) c.conf_list[cur[c.color[p]]++] = p;
+}
+
+// ColorList::incrementalRecoloring (common/ColorList.hpp:381-474): at most six
+// rounds; a dirty particle with a same-colored neighbour of lower index takes
+// the first color unused by its neighbours (256 colors at most); a changed
+// color makes every neighbour dirty for the next round.  Particles still dirty
+// after the last round stay dirty for the next stage, and they and their
+// same-colored neighbours are marked conflicted.
+static void incremental_recoloring(Ctx& c) {
+    const unsigned MAX_ROUNDS = c.recolor_rounds;
+    for (unsigned p : c.touched_conflicted) c.conflicted[p] = 0;
+    c.touched_conflicted.clear();
+    unsigned iter = 0;
+    while (!c.dirty.empty() && iter < MAX_ROUNDS) {
+        for (unsigned p : c.dirty) {
+            uint64_t bits[4] = {0, 0, 0, 0};
+            bool must = false;
+            for_each_neighbor(c, p, [&](unsigned q) {
+                unsigned cq = c.color[q];
+                if (cq >= 256) throw std::runtime_error("Ran out of colors!");
+                bits[cq / 64] |= 1ull << (cq % 64);
+                if (cq == c.color[p] && q < p) must = true;
+            });
+            if (must) {
+                unsigned cand = UINT32_MAX;
+                for (unsigned w = 0; w < 4 && cand == UINT32_MAX; w++)
+                    if (~bits[w]) cand = w * 64 + (unsigned)__builtin_ctzll(~bits[w]);
+                if (cand == UINT32_MAX) throw std::runtime_error("Ran out of colors!");
+                c.cand_color[p] = cand;
+                if (cand >= c.num_colors) c.num_colors++;
+            } else {
+                c.cand_color[p] = c.color[p];
+            }
+        }
+        c.next_dirty.clear();
+        for (unsigned p : c.dirty) {
+            if (c.cand_color[p] == c.color[p]) continue;
+            c.color[p] = c.cand_color[p];
+            for_each_neighbor(c, p, [&](unsigned q) {
+                if (c.last_dirty[q] != iter + 1) {
+                    c.last_dirty[q] = iter + 1;
+                    c.touched_frame.push_back(q);
+                    c.next_dirty.push_back(q);
+                }
+            });
+        }
+        c.dirty.swap(c.next_dirty);
+        iter++;
+    }
+    if (!c.dirty.empty()) {
+        finalize_conflicts(c);
+    } else {
+        c.conf_off.assign(c.num_colors + 1, 0);
+        c.conf_list.clear();
+    }
+    rebuild_work_list(c);
+    for (unsigned p : c.touched_frame) c.last_dirty[p] = DIRTY_SENTINEL;
+    c.touched_frame.clear();
+    for (unsigned p : c.dirty) c.last_dirty[p] = 0;
 }
 
 // LBVHBuilder::buildBVH + broad phase (collision/LBVHBuilder.cpp:13-25,
 // collision/CollisionDetector.cpp:24-55).  Narrow phase: triangle-triangle and
 // rod-rod are no-ops in the reference (CollisionDetector.cpp:589-599,668-676);
 // sphere-sphere and sphere-rod throw there (CollisionDetector.cpp:180-213,678-687).
-static void collision_stage(Ctx& c) {
+// `manage` adds the contact handling of detectCollisionsAndRecolor_Parallel
+// (CollisionDetector.cpp:57-128): merge into the contact pool, dynamic
+// adjacency, incremental recoloring.  Without it the stage only detects.
+static void collision_stage(Ctx& c, bool manage) {
     unsigned n = (unsigned)c.prims.size();
     if (n == 0) { c.pairs.clear(); return; }
     c.aabb.assign((size_t)n * 6, 0);
@@ -1513,6 +1855,12 @@ static void collision_stage(Ctx& c) {
     refit(c, n);
     traverse(c);
     narrow_phase(c);
+    if (!manage) return;
+    c.prev_contacts.swap(c.contacts);
+    c.contacts = c.detected;
+    handle_detections(c);
+    build_dynamic_adjacency(c);
+    incremental_recoloring(c);
 }
 
 }  // namespace orc
@@ -1593,6 +1941,11 @@ void orc_set_positions_raw(void* h, unsigned first, unsigned n, const double* x)
 void orc_set_rotations_raw(void* h, unsigned first, unsigned n, const double* q) {
     Ctx& c = *(Ctx*)h;
     for (unsigned i = 0; i < n; i++) c.q[c.rot[first + i]] = Q4{q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
+}
+void orc_set_angular_velocities(void* h, unsigned first, unsigned n, const double* w) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned i = 0; i < n; i++)
+        if (c.oriented(first + i)) c.w[c.rot[first + i]] = V3(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
 }
 void orc_get_positions(void* h, double* out) {
     Ctx& c = *(Ctx*)h;
@@ -1717,6 +2070,12 @@ int orc_finalize(void* h, int reference_dsatur) {
         if (reference_dsatur) dsatur_reference(c); else dsatur_fast(c);
         if (c.num_colors > 256) throw std::runtime_error("Ran out of colors!");
         rebuild_work_list(c);
+        const unsigned n = c.np();
+        c.last_dirty.assign(n, DIRTY_SENTINEL);
+        c.cand_color.assign(n, 0);
+        c.conflicted.assign(n, 0);
+        c.buffered.assign(n, V3());
+        c.conf_off.assign(c.num_colors + 1, 0);
         c.finalized = true;
     });
 }
@@ -1736,7 +2095,7 @@ double orc_time_steps(void* h, unsigned n) {
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
-int orc_collision_stage(void* h) { ORC_TRY(collision_stage(*(Ctx*)h)); }
+int orc_collision_stage(void* h) { ORC_TRY(collision_stage(*(Ctx*)h, false)); }
 void orc_after_time_step(void* h) { after_time_step(*(Ctx*)h); }
 
 void orc_get_coloring(void* h, unsigned* colors, unsigned* num_colors) {
@@ -1764,8 +2123,8 @@ unsigned orc_num_pairs(void* h) { return (unsigned)((Ctx*)h)->pairs.size(); }
 // normal[3], barys[3], cp_local[3] (ascending key)
 unsigned orc_get_contacts(void* h, uint64_t* keys, unsigned* idx4, double* vec9) {
     Ctx& c = *(Ctx*)h;
-    for (size_t k = 0; k < c.contacts.size(); k++) {
-        const auto& d = c.contacts[k];
+    for (size_t k = 0; k < c.detected.size(); k++) {
+        const auto& d = c.detected[k];
         if (keys) keys[k] = d.key;
         if (idx4) { idx4[4 * k] = d.tri[0]; idx4[4 * k + 1] = d.tri[1]; idx4[4 * k + 2] = d.tri[2]; idx4[4 * k + 3] = d.rb; }
         if (vec9) {
@@ -1776,7 +2135,49 @@ unsigned orc_get_contacts(void* h, uint64_t* keys, unsigned* idx4, double* vec9)
             }
         }
     }
-    return (unsigned)c.contacts.size();
+    return (unsigned)c.detected.size();
+}
+
+// Dynamic contact state: [0] live contacts, [1] pool size (highest slot + 1),
+// [2] colors, [3] conflicted particles, [4] particles still dirty,
+// [5] dynamic adjacency entries
+void orc_dynamic_info(void* h, unsigned* out) {
+    Ctx& c = *(Ctx*)h;
+    out[0] = c.trc_count;
+    out[1] = (unsigned)c.trc.size();
+    out[2] = c.num_colors;
+    out[3] = (unsigned)c.touched_conflicted.size();
+    out[4] = (unsigned)c.dirty.size();
+    out[5] = (unsigned)c.dyn_ent.size();
+}
+
+// Contact pool slots [0, pool size): particles (4 per slot), active flag, and
+// 24 doubles per slot: n, t, b, barys, cp_local, k_start, k_n, k_t, k_b,
+// lam_n, lam_t, lam_b, C_n_prev, use_static + 2 unclamped
+void orc_get_trc(void* h, unsigned* p4, uint8_t* active, double* data) {
+    Ctx& c = *(Ctx*)h;
+    for (size_t s = 0; s < c.trc.size(); s++) {
+        const TriRigid& e = c.trc[s];
+        if (p4) for (int k = 0; k < 4; k++) p4[4 * s + k] = e.p[k];
+        if (active) active[s] = c.trc_active[s];
+        if (data) {
+            double* d = data + 24 * s;
+            const V3 v[5] = {e.n, e.t, e.b, e.barys, e.cp_local};
+            for (int i = 0; i < 5; i++) for (int j = 0; j < 3; j++) d[3 * i + j] = v[i][j];
+            d[15] = e.k_start; d[16] = e.k_n; d[17] = e.k_t; d[18] = e.k_b;
+            d[19] = e.lam_n; d[20] = e.lam_t; d[21] = e.lam_b; d[22] = e.cn_prev;
+            d[23] = (e.use_static ? 1 : 0) + (e.unclamped ? 2 : 0);
+        }
+    }
+}
+
+// test hook: the recoloring's round limit (6 in the reference)
+void orc_set_recolor_rounds(void* h, unsigned rounds) { ((Ctx*)h)->recolor_rounds = rounds; }
+
+// per-particle conflict flags of the last recoloring
+void orc_get_conflicted(void* h, uint8_t* out) {
+    Ctx& c = *(Ctx*)h;
+    for (unsigned p = 0; p < c.np(); p++) out[p] = c.conflicted.empty() ? 0 : c.conflicted[p];
 }
 void orc_get_lbvh(void* h, uint64_t* morton, unsigned* sorted, unsigned* left, unsigned* right, unsigned* parent,
                   unsigned* subtree, double* bounds, unsigned* root, unsigned* pairs) {

@@ -59,11 +59,16 @@ def lib():
             "orc_set_velocities": (None, [vp, C.c_uint, C.c_uint, dp, dp]),
             "orc_set_positions_raw": (None, [vp, C.c_uint, C.c_uint, dp]),
             "orc_set_rotations_raw": (None, [vp, C.c_uint, C.c_uint, dp]),
+            "orc_set_angular_velocities": (None, [vp, C.c_uint, C.c_uint, dp]),
             "orc_get_positions": (None, [vp, dp]),
             "orc_get_velocities": (None, [vp, dp]),
             "orc_get_rotations": (None, [vp, dp]),
             "orc_get_contacts": (C.c_uint, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint), dp]),
             "orc_get_angular_velocities": (None, [vp, dp]),
+            "orc_dynamic_info": (None, [vp, up]),
+            "orc_get_trc": (None, [vp, up, u8p, dp]),
+            "orc_get_conflicted": (None, [vp, u8p]),
+            "orc_set_recolor_rounds": (None, [vp, C.c_uint]),
             "orc_num_particles": (C.c_uint, [vp]),
             "orc_neo_hookean_add": (C.c_uint, [vp, C.c_uint, up, dp, dp, dp, dp, dp]),
             "orc_cosserat_rod_add": (C.c_uint, [vp, C.c_uint, up, dp, dp, dp]),
@@ -192,6 +197,10 @@ class Oracle:
         x = _d(positions, (-1, 3))
         self.L.orc_set_positions_raw(self.h, first, len(x), _p(x, C.c_double))
 
+    def set_angular_velocities(self, first, w):
+        w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1, 3)
+        self.L.orc_set_angular_velocities(self.h, first, len(w), _p(w, C.c_double))
+
     def set_rotations_raw(self, first, rotations):
         q = _d(rotations, (-1, 4))
         self.L.orc_set_rotations_raw(self.h, first, len(q), _p(q, C.c_double))
@@ -283,6 +292,36 @@ class Oracle:
             self.L.orc_get_contacts(self.h, _p(keys, C.c_uint64), _p(idx, C.c_uint), _p(vec, C.c_double))
         return {"key": keys, "tri": idx[:, :3], "rigid": idx[:, 3], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
                 "cp_local": vec[:, 6:9]}
+
+    def dynamic_info(self):
+        """Contact pool and recoloring state: live contacts, pool size, colors,
+        conflicted particles, particles still dirty, dynamic adjacency entries."""
+        out = np.zeros(6, dtype=np.uint32)
+        self.L.orc_dynamic_info(self.h, _p(out, C.c_uint))
+        return dict(zip(["live", "pool_size", "colors", "conflicted", "dirty", "entries"], (int(v) for v in out)))
+
+    def contact_pool(self):
+        """Triangle-rigid contact pool by slot: particles [s, 4], active [s],
+        and per slot n, t, b, barys, cp_local [s, 3], k (k_start, k_n, k_t,
+        k_b) [s, 4], lam (lam_n, lam_t, lam_b, C_n_prev) [s, 4], flags [s]
+        (1 static friction, 2 unclamped)."""
+        n = self.dynamic_info()["pool_size"]
+        p4 = np.zeros((n, 4), dtype=np.uint32)
+        act = np.zeros(n, dtype=np.uint8)
+        d = np.zeros((n, 24))
+        if n:
+            self.L.orc_get_trc(self.h, _p(p4, C.c_uint), _p(act, C.c_uint8), _p(d, C.c_double))
+        return {"particles": p4, "active": act.astype(bool), "n": d[:, 0:3], "t": d[:, 3:6], "b": d[:, 6:9],
+                "barys": d[:, 9:12], "cp_local": d[:, 12:15], "k": d[:, 15:19], "lam": d[:, 19:23],
+                "flags": d[:, 23].astype(np.uint8)}
+
+    def set_recolor_rounds(self, rounds):
+        self.L.orc_set_recolor_rounds(self.h, rounds)
+
+    def conflicted(self):
+        out = np.zeros(self.num_particles, dtype=np.uint8)
+        self.L.orc_get_conflicted(self.h, _p(out, C.c_uint8))
+        return out.astype(bool)
 
     def angular_velocities(self):
         out = np.zeros((self.num_particles, 3))

@@ -1,0 +1,123 @@
+"""Parity of the dynamic triangle-rigid contacts with the FP64 oracle: the
+merge of the narrow phase's detections into the contact pool
+(CollisionDetector::_handleDetectedCollisions, collision/CollisionDetector.cpp:
+265-482), the incremental recoloring (ColorList.hpp:381-522), the contact
+energies in the vertex blocks (TriangleRigidCollisionEnergySolver.hpp:14-118,
+CollisionConstraintEnergySolver.hpp:60-285) and the conflict buffering
+(VBDSolver.hpp:82-87,108-119,474-509).
+
+Scene: four rigid spheres dropped on a soft 4^3-cell tet cube with a fixed
+base.  In FP64 the pool (slots, particles), the colors and the conflicts are
+compared exactly every step, positions within 1e-8 of the bounding-box
+diagonal; with no recoloring rounds the conflict path runs every step."""
+import numpy as np
+import pytest
+
+from avbd_b200 import Context, scenes
+
+pytestmark = pytest.mark.gpu
+
+N_CUBE = 125
+
+
+def pair(oracle_lib, precision="fp64", rounds=None, tol=0.0, max_iters=0):
+    sc = scenes.spheres_on_cube(n=4, num_spheres=4, seed=0)
+    e = Context()
+    sc.load(e, precision=precision, residual_tolerance=tol, max_iters=max_iters)
+    e.finalize()
+    o = oracle_lib.Oracle()
+    sc.load(o, residual_tolerance=tol, max_iters=max_iters)
+    o.finalize()
+    if rounds is not None:
+        e.set_recolor_rounds(rounds)
+        o.set_recolor_rounds(rounds)
+    return sc, e, o
+
+
+def quat_err(a, b):
+    s = np.sign(np.sum(a * b, axis=1, keepdims=True))
+    s[s == 0] = 1
+    return np.abs(a - s * b).max()
+
+
+@pytest.mark.parametrize("rounds", [None, 0])
+def test_contacts_track_oracle_fp64(oracle_lib, rounds):
+    sc, e, o = pair(oracle_lib, "fp64", rounds)
+    d = sc.bbox_diagonal()
+    conflicts = 0
+    for step in range(60):
+        e.step(1)
+        o.step(1)
+        ie, io = e.dynamic_info(), o.dynamic_info()
+        assert ie == io, (step, ie, io)
+        conflicts += ie["conflicted"]
+        ce, nce = e.coloring()
+        co, nco = o.coloring()
+        assert nce == nco and (ce == co).all(), step
+        ex = np.abs(e.positions() - o.positions()).max() / d
+        assert ex < 1e-8, (step, ex)
+    assert quat_err(e.rotations(), o.rotations()) < 1e-7
+    pe, po = e.contact_pool(), o.contact_pool()
+    assert (pe["active"] == po["active"]).all()
+    act = po["active"]
+    assert act.any()
+    assert (pe["particles"][act] == po["particles"][act]).all()
+    for key in ("n", "t", "b", "barys", "cp_local"):
+        np.testing.assert_allclose(pe[key][act], po[key][act], rtol=0, atol=1e-7, err_msg=key)
+    np.testing.assert_allclose(pe["k"][act], po["k"][act], rtol=1e-6)
+    lam_scale = np.abs(po["lam"][act][:, :3]).max() + 1e-12
+    assert np.abs(pe["lam"][act][:, :3] - po["lam"][act][:, :3]).max() <= 1e-6 * lam_scale
+    assert (pe["flags"][act] == po["flags"][act]).all()
+    if rounds == 0:
+        assert conflicts > 0
+
+
+def test_contact_blocks_and_residual_match_oracle(oracle_lib):
+    """avbd_debug_block of a sphere and of triangle vertices in contact, and
+    the residual, after 12 steps of both."""
+    sc, e, o = pair(oracle_lib, "fp64")
+    e.step(12)
+    o.step(12)
+    pool = o.contact_pool()
+    act = np.nonzero(pool["active"])[0]
+    assert len(act)
+    parts = sorted({int(v) for s in act for v in pool["particles"][s]})
+    for p in parts[:6] + parts[-2:]:
+        Ge, He = e.debug_block(p)
+        Go, Ho = o.debug_block(p)
+        scale_h = np.abs(Ho).max()
+        scale_g = max(np.abs(Go).max(), scale_h * 1e-3)
+        assert np.abs(Ge - Go).max() <= 1e-6 * scale_g, (p, Ge, Go)
+        assert np.abs(He - Ho).max() <= 1e-6 * scale_h, (p, He, Ho)
+    re, ro = e.residual(), o.residual()
+    assert abs(re - ro) <= 1e-6 * ro, (re, ro)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp32"])
+def test_contacts_lower_precision_land_spheres(oracle_lib, precision):
+    """Mixed and FP32 runs form contacts and keep the spheres on the cube
+    (their detections may differ from FP64's near the margin)."""
+    sc, e, o = pair(oracle_lib, precision)
+    live = 0
+    for _ in range(6):
+        e.step(10)
+        live = max(live, e.dynamic_info()["live"])
+    x = e.positions()
+    assert np.isfinite(x).all()
+    assert live > 0
+    top = x[:N_CUBE, 1].max()
+    radii = np.array([a[1][0] for m, a, _ in sc.calls if m == "add_spheres"])
+    low = x[N_CUBE:, 1] - radii
+    assert np.all(low > top - 0.08) and np.all(low < top + 0.02), (low, top)
+
+
+def test_contacts_run_to_tolerance(oracle_lib):
+    """Per-scene run-to-tolerance with contacts: iteration counts and states
+    follow the oracle."""
+    sc, e, o = pair(oracle_lib, "fp64", tol=1e-3, max_iters=200)
+    for _ in range(20):
+        e.step(1)
+        o.step(1)
+    st = e.stats()
+    assert abs(st["iterations"] - o.iterations) <= 2 * 20, (st["iterations"], o.iterations)
+    assert np.abs(e.positions() - o.positions()).max() / sc.bbox_diagonal() < 1e-6

@@ -1,11 +1,14 @@
-"""Narrow phase on the GPU vs the FP64 oracle: spheres fall through the top
-of a tet cube (the contact energies of these detections are not part of the
-step, so they pass through) and then roll on the ground.  The LBVH with
-sphere primitives (rotated-box bounds, CollisionPrimitivePool.hpp:199-231)
-stays bit-exact, and the triangle-sphere detections
-(CollisionDetector::_triangleSDF_CCD) match: same keys, triangles and
-spheres, vectors to 1e-12 while the spheres do not spin and to 1e-9 once they
-roll (device and host sin/cos may differ in the last bit)."""
+"""Narrow phase on the GPU vs the FP64 oracle: two spheres hit the top of a
+coarse tet cube at 2-4 m/s (one step moves them 3-7 cm); their contact
+energies throw one far off and let the other through to the ground.  Such
+impacts amplify rounding differences between two solvers, so the engine's
+state (positions, velocities, rotations, angular velocities) is copied into
+the oracle before every detection.  From the same state the LBVH with sphere
+primitives (rotated-box bounds, CollisionPrimitivePool.hpp:199-231) is
+bit-exact, and the triangle-sphere detections
+(CollisionDetector::_triangleSDF_CCD) match: same keys, triangles and spheres,
+vectors to 1e-12 while the spheres do not spin and to 1e-9 once they roll
+(device and host sin/cos may differ in the last bit)."""
 import numpy as np
 import pytest
 
@@ -15,13 +18,12 @@ pytestmark = pytest.mark.gpu
 
 
 def scene(n=4, seed=3):
-    """Four spheres on a 2 x 2 grid over the cube's top face, moving apart
-    (sphere-sphere candidates would stop the reference), falling through the
-    top face and rolling on the ground afterwards."""
+    """Two spheres over opposite corners of the cube's top face, moving apart
+    (sphere-sphere candidates stop the reference)."""
     sc = scenes.cube_drop(n=n, iters=10, height=0.05, surface=True)
     rng = np.random.default_rng(seed)
     first = sc.num_particles
-    for k, (gx, gz) in enumerate([(0.25, 0.25), (0.75, 0.25), (0.25, 0.75), (0.75, 0.75)]):
+    for k, (gx, gz) in enumerate([(0.25, 0.25), (0.75, 0.75)]):
         r = rng.uniform(0.06, 0.1)
         p = (gx + rng.uniform(-0.05, 0.05), 1.05 + r + rng.uniform(0.0, 0.1), gz + rng.uniform(-0.05, 0.05))
         b = scenes.add_sphere(sc, r, 500.0, p)
@@ -51,9 +53,13 @@ def test_narrow_phase_matches_oracle(oracle_lib):
     sc.load(o)
     o.finalize()
     found, spinning = 0, False
+    sph = sc.meta["spheres"]
     for step in range(40):
         e.step(1)
-        o.step(1)
+        o.set_positions_raw(0, e.positions())
+        o.set_velocities(0, e.velocities())
+        o.set_rotations_raw(sph[0], e.rotations()[sph[0]:])
+        o.set_angular_velocities(sph[0], e.angular_velocities()[sph[0]:])
         e.collision_stage()
         o.collision_stage()
         w = o.angular_velocities()[sc.meta["spheres"]]
