@@ -93,6 +93,8 @@ SIGNATURES = {
     "avbd_get_contacts": [_vp, C.c_uint, _u64p, _up, _dp, _up],
     "avbd_dynamic_info": [_vp, _up],
     "avbd_get_contact_pool": [_vp, C.c_uint, _up, _u8p, _dp, _up],
+    "avbd_get_rod_contact_pool": [_vp, C.c_uint, _up, _u8p, _dp, _up],
+    "avbd_get_rod_contacts": [_vp, C.c_uint, _u64p, _up, _dp, _up],
     "avbd_debug_set_recolor_rounds": [_vp, C.c_uint],
     "avbd_debug_block": [_vp, C.c_uint, _dp, _dp, C.POINTER(C.c_int)],
     "avbd_residual": [_vp, _dp],

@@ -270,9 +270,10 @@ class Context:
         """Contact pool and recoloring state of the last step: live contacts,
         pool size, colors, conflicted particles, particles still dirty,
         dynamic adjacency entries."""
-        out = np.zeros(6, dtype=np.uint32)
+        out = np.zeros(8, dtype=np.uint32)
         check(self.L.avbd_dynamic_info(self.h, _up(out)))
-        return dict(zip(["live", "pool_size", "colors", "conflicted", "dirty", "entries"], (int(v) for v in out)))
+        return dict(zip(["live", "pool_size", "colors", "conflicted", "dirty", "entries", "rod_live", "rod_pool_size"],
+                        (int(v) for v in out)))
 
     def contact_pool(self):
         """Triangle-rigid contact pool by slot (layout of avbd_get_contact_pool)."""
@@ -287,6 +288,35 @@ class Context:
         return {"particles": p4, "active": act.astype(bool), "n": d[:, 0:3], "t": d[:, 3:6], "b": d[:, 6:9],
                 "barys": d[:, 9:12], "cp_local": d[:, 12:15], "k": d[:, 15:19], "lam": d[:, 19:23],
                 "flags": d[:, 23].astype(np.uint8)}
+
+    def rod_contact_pool(self):
+        """Triangle-rod contact pool by slot (layout of avbd_get_rod_contact_pool)."""
+        size = C.c_uint(0)
+        check(self.L.avbd_get_rod_contact_pool(self.h, 0, None, None, None, C.byref(size)))
+        n = size.value
+        p5 = np.zeros((n, 5), dtype=np.uint32)
+        act = np.zeros(n, dtype=np.uint8)
+        d = np.zeros((n, 25))
+        if n:
+            check(self.L.avbd_get_rod_contact_pool(self.h, n, _up(p5), _u8p(act), _dp(d), C.byref(size)))
+        return {"particles": p5, "active": act.astype(bool), "n": d[:, 0:3], "t": d[:, 3:6], "b": d[:, 6:9],
+                "barys": d[:, 9:12], "cp_local": d[:, 12:15], "s": d[:, 15], "k": d[:, 16:20], "lam": d[:, 20:24],
+                "flags": d[:, 24].astype(np.uint8)}
+
+    def rod_contacts(self):
+        """Triangle-rod contacts of the last collision stage, ascending key:
+        key [k], tri [k, 3], rod [k, 2], normal / barys / cp_local [k, 3], s [k]."""
+        cnt = C.c_uint(0)
+        check(self.L.avbd_get_rod_contacts(self.h, 0, None, None, None, C.byref(cnt)))
+        n = cnt.value
+        keys = np.zeros(n, dtype=np.uint64)
+        idx = np.zeros((n, 5), dtype=np.uint32)
+        vec = np.zeros((n, 10))
+        if n:
+            check(self.L.avbd_get_rod_contacts(self.h, n, keys.ctypes.data_as(C.POINTER(C.c_uint64)), _up(idx),
+                                               _dp(vec), C.byref(cnt)))
+        return {"key": keys, "tri": idx[:, :3], "rod": idx[:, 3:5], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
+                "cp_local": vec[:, 6:9], "s": vec[:, 9]}
 
     def set_recolor_rounds(self, rounds):
         check(self.L.avbd_debug_set_recolor_rounds(self.h, rounds))

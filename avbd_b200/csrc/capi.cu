@@ -747,6 +747,11 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     for (auto& g : c->ground)
         if (c->rot[g.p] != UINT32_MAX)
             return fail(AVBD_ERR_UNSUPPORTED, "ground energy on an oriented particle (use rigid-body ground)");
+    // a rod segment's contact frame interpolates its nodes' rotations
+    // (CollisionDetector::_triangleRod, collision/CollisionDetector.cpp:637-640)
+    for (auto& pr : c->prims)
+        if (pr.type == AVBD_SHAPE_ROD_SEGMENT && (c->rot[pr.idx[0]] == UINT32_MAX || c->rot[pr.idx[1]] == UINT32_MAX))
+            return fail(AVBD_ERR_INVALID_ARG, "rod segment primitive on a positional particle");
     for (auto& g : c->rground)
         if (g.shape != AVBD_SHAPE_SPHERE && g.shape != AVBD_SHAPE_ROD_SEGMENT)
             return fail(AVBD_ERR_UNSUPPORTED, "rigid-body ground contact needs a sphere or rod-segment shape");
@@ -898,13 +903,7 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
     if (!c->prims.empty()) {
         std::string err;
         if (int r2 = lbvh_allocate(c, err)) return fail(r2, err);
-        // triangle-sphere pairs give dynamic contact energies, managed per step
-        bool tri = false, sph = false;
-        for (auto& pr : c->prims) {
-            tri |= pr.type == AVBD_SHAPE_TRIANGLE;
-            sph |= pr.type == AVBD_SHAPE_SPHERE;
-        }
-        if (tri && sph)
+        if (c->lbvh.contact_capacity)  // triangles with spheres or rod segments: dynamic contacts
             if (int r2 = dyn_create(c, p_off, p_nbr, err)) return fail(r2, err);
     }
     c->stats.num_colors = nc;
@@ -975,7 +974,7 @@ void enqueue_chebyshev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double 
                        const SceneTol& T) {
     launch_chebyshev_dual<R>(c, s, k, omega, st, T);
     launch_chebyshev_rot<R>(c, s, k, omega, st, T);
-    if (c->dyn) launch_trc_after_iter<R>(c, s, st, T);
+    if (c->dyn) launch_contact_after_iter<R>(c, s, st, T);
 }
 
 template <typename R>
@@ -1432,13 +1431,21 @@ int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, doubl
     return device_error(c);
 }
 
-int avbd_get_contacts(avbd_ctx* c, unsigned capacity, uint64_t* keys, unsigned* idx4, double* vec9,
-                      unsigned* count) {
-    if (int r = check_ctx(c)) return r;
-    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
-    if (!count) return fail(AVBD_ERR_INVALID_ARG, "null count");
+}  // extern "C"
+
+namespace {
+
+// The narrow phase's detections of one DetectedCollisionType (2
+// triangle-sphere, 3 triangle-rod) in ascending key order.
+struct Detections {
+    std::vector<uint64_t> key;
+    std::vector<uint4> idx;
+    std::vector<uint32_t> idx5;
+    std::vector<double> vec;   // 10 per detection
+};
+
+int read_detections(avbd_ctx* c, unsigned type, Detections& out) {
     const LbvhState& L = c->lbvh;
-    *count = 0;
     if (!L.contact_capacity) return AVBD_OK;
     uint32_t n = 0;
     CUDA_OR_FAIL(cudaMemcpyAsync(&n, L.contact_count, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
@@ -1446,28 +1453,74 @@ int avbd_get_contacts(avbd_ctx* c, unsigned capacity, uint64_t* keys, unsigned* 
     if (n > L.contact_capacity) return fail(AVBD_ERR_CAPACITY, "more contacts than the contact buffer holds");
     std::vector<uint64_t> k(n);
     std::vector<uint4> ix(n);
-    std::vector<double> v(9ull * n);
+    std::vector<uint32_t> ix5(n);
+    std::vector<double> v(10ull * n);
     if (n) {
         CUDA_OR_FAIL(cudaMemcpyAsync(k.data(), L.contact_key, 8ull * n, cudaMemcpyDeviceToHost, c->stream));
         CUDA_OR_FAIL(cudaMemcpyAsync(ix.data(), L.contact_idx, 16ull * n, cudaMemcpyDeviceToHost, c->stream));
-        CUDA_OR_FAIL(cudaMemcpyAsync(v.data(), L.contact_vec, 72ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_OR_FAIL(cudaMemcpyAsync(ix5.data(), L.contact_idx5, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_OR_FAIL(cudaMemcpyAsync(v.data(), L.contact_vec, 80ull * n, cudaMemcpyDeviceToHost, c->stream));
         CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
     }
     // ascending key, as CollisionDetector::_handleDetectedCollisions orders them
-    std::vector<uint32_t> ord(n);
-    std::iota(ord.begin(), ord.end(), 0u);
+    std::vector<uint32_t> ord;
+    for (uint32_t j = 0; j < n; j++)
+        if ((k[j] >> 59) == type) ord.push_back(j);
     std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return k[a] < k[b]; });
-    *count = n;
-    for (uint32_t j = 0; j < n && j < capacity; j++) {
-        const uint32_t o = ord[j];
-        if (keys) keys[j] = k[o];
+    for (uint32_t o : ord) {
+        out.key.push_back(k[o]);
+        out.idx.push_back(make_uint4(c->perm[ix[o].x], c->perm[ix[o].y], c->perm[ix[o].z], c->perm[ix[o].w]));
+        out.idx5.push_back(type == 3 ? c->perm[ix5[o]] : 0u);
+        out.vec.insert(out.vec.end(), v.begin() + 10ull * o, v.begin() + 10ull * o + 10);
+    }
+    return AVBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int avbd_get_contacts(avbd_ctx* c, unsigned capacity, uint64_t* keys, unsigned* idx4, double* vec9,
+                      unsigned* count) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (!count) return fail(AVBD_ERR_INVALID_ARG, "null count");
+    *count = 0;
+    Detections D;
+    if (int r = read_detections(c, 2, D)) return r;
+    *count = (unsigned)D.key.size();
+    for (size_t j = 0; j < D.key.size() && j < capacity; j++) {
+        if (keys) keys[j] = D.key[j];
         if (idx4) {
-            idx4[4 * j] = c->perm[ix[o].x];
-            idx4[4 * j + 1] = c->perm[ix[o].y];
-            idx4[4 * j + 2] = c->perm[ix[o].z];
-            idx4[4 * j + 3] = c->perm[ix[o].w];
+            idx4[4 * j] = D.idx[j].x;
+            idx4[4 * j + 1] = D.idx[j].y;
+            idx4[4 * j + 2] = D.idx[j].z;
+            idx4[4 * j + 3] = D.idx[j].w;
         }
-        if (vec9) std::copy(v.begin() + 9ull * o, v.begin() + 9ull * o + 9, vec9 + 9ull * j);
+        if (vec9) std::copy(D.vec.begin() + 10 * j, D.vec.begin() + 10 * j + 9, vec9 + 9 * j);
+    }
+    return device_error(c);
+}
+
+int avbd_get_rod_contacts(avbd_ctx* c, unsigned capacity, uint64_t* keys, unsigned* idx5, double* vec10,
+                          unsigned* count) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (!count) return fail(AVBD_ERR_INVALID_ARG, "null count");
+    *count = 0;
+    Detections D;
+    if (int r = read_detections(c, 3, D)) return r;
+    *count = (unsigned)D.key.size();
+    for (size_t j = 0; j < D.key.size() && j < capacity; j++) {
+        if (keys) keys[j] = D.key[j];
+        if (idx5) {
+            idx5[5 * j] = D.idx[j].x;
+            idx5[5 * j + 1] = D.idx[j].y;
+            idx5[5 * j + 2] = D.idx[j].z;
+            idx5[5 * j + 3] = D.idx[j].w;
+            idx5[5 * j + 4] = D.idx5[j];
+        }
+        if (vec10) std::copy(D.vec.begin() + 10 * j, D.vec.begin() + 10 * j + 10, vec10 + 10 * j);
     }
     return device_error(c);
 }

@@ -1,11 +1,12 @@
-// contacts.cu -- dynamic triangle-rigid contacts: the contact handling of the
-// collision stage and the per-color solve around it.
+// contacts.cu -- dynamic contacts (triangle-rigid and triangle-rod): the
+// contact handling of the collision stage and the per-color solve around it.
 //
 // Reference behaviour followed:
 //   CollisionDetector::detectCollisionsAndRecolor_Parallel   collision/CollisionDetector.cpp:57-128
 //   CollisionDetector::_handleDetectedCollisions / _add / _update / _removeCollision
 //                                                            collision/CollisionDetector.cpp:265-482
 //   TriangleRigidCollisionEnergyPool::addEnergy              energy/collision/TriangleRigidCollisionEnergyPool.hpp:31-62
+//   TriangleRodCollisionEnergyPool::addEnergy                energy/collision/TriangleRodCollisionEnergyPool.hpp:29-66
 //   CollisionConstraintEnergyPool::addEnergy                 energy/collision/CollisionConstraintEnergyPool.hpp:48-69
 //   CollisionConstraintEnergySolver::updateCollisionFrame    energy/collision/CollisionConstraintEnergySolver.hpp:17-53
 //   Math::completeOrthonormalBasisGivenNormal                common/Math.hpp:323-327
@@ -36,31 +37,37 @@
 namespace avbd {
 
 struct DynHost {
-    // ---- triangle-rigid contact pool (FP64 host mirror, reference particle ids)
+    // ---- contact pools (FP64 host mirror, reference particle ids):
+    // pool[0] triangle-rigid, pool[1] triangle-rod
     struct Rec {
-        unsigned p[4];
+        unsigned p[5];  // triangle x3, rigid body / rod nodes
         double n[3], t[3], b[3], bar[3], cpl[3];
+        double s;       // along the rod segment
         double k[4];    // k_n, k_t, k_b, k_start
         double lam[4];  // lam_n, lam_t, lam_b, C_n_prev
         double mu_s, mu_k;
         uint8_t flag;   // ContactFlags
     };
-    unsigned cap = 0;
-    std::vector<Rec> rec;
-    std::vector<uint8_t> active;
-    std::vector<unsigned> slots;   // free-slot stack
-    unsigned top = 0, count = 0, size = 0;
+    struct Pool {
+        std::vector<Rec> rec;
+        std::vector<uint8_t> active;
+        std::vector<unsigned> slots;   // free-slot stack
+        unsigned top = 0, count = 0, size = 0;
+    };
+    unsigned cap = 0;  // slots per pool on the device
+    Pool pool[2];
     struct Det {
         uint64_t key;
-        unsigned tri[3], rb;
-        double n[3], bar[3], cpl[3];
+        int pool;       // 0: DetectedCollisionType::TriangleRigid (2), 1: TriangleRod (3)
+        unsigned tri[3], p4[2];   // rigid body, or the rod's two nodes
+        double n[3], bar[3], cpl[3], s;
         unsigned e_idx;
     };
     std::vector<Det> cur, prev;
     // ---- adjacency and coloring (reference particle ids)
     std::vector<unsigned> p_off, p_nbr;          // static neighbours
     std::vector<unsigned> dyn_off, dnb_off, dnb; // dynamic entries per particle, dynamic neighbours
-    std::vector<uint32_t> dyn_ent_ext;           // slot << 2 | local
+    std::vector<uint32_t> dyn_ent_ext;           // slot << 4 | pool << 3 | local
     std::vector<unsigned> color, slab_color;
     unsigned num_colors = 0;
     std::vector<unsigned> last_dirty, dirty, next_dirty, touched_frame, cand, touched_conflicted;
@@ -77,8 +84,8 @@ struct DynHost {
     // ---- staging
     std::vector<uint64_t> h_key;
     std::vector<uint4> h_idx;
+    std::vector<uint32_t> h_idx5;
     std::vector<double> h_vec;
-    std::vector<unsigned char> h_pool;           // downloaded k / lam / flag rows
     unsigned long long contacts_added = 0, contacts_removed = 0;
 };
 
@@ -135,25 +142,25 @@ void update_frame(DynHost::Rec& e, const double nn[3]) {
 
 // TombstonePool: the stack grows on demand; a slot never reached holds its
 // own index, as the reference's iota-initialised stack does
-int pool_alloc(DynHost& D, unsigned& slot) {
-    if (D.top == D.slots.size()) D.slots.push_back((unsigned)D.slots.size());
-    slot = D.slots[D.top];
-    if (slot >= D.cap) return set_error(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
-    D.top++;
-    if (slot >= D.rec.size()) {
-        D.rec.resize(slot + 1);
-        D.active.resize(slot + 1, 0);
+int pool_alloc(DynHost::Pool& P, unsigned cap, unsigned& slot) {
+    if (P.top == P.slots.size()) P.slots.push_back((unsigned)P.slots.size());
+    slot = P.slots[P.top];
+    if (slot >= cap) return set_error(AVBD_ERR_CAPACITY, "Pool has exceeded capacity");
+    P.top++;
+    if (slot >= P.rec.size()) {
+        P.rec.resize(slot + 1);
+        P.active.resize(slot + 1, 0);
     }
-    D.active[slot] = 1;
-    D.count++;
-    D.size = std::max(D.size, slot + 1);
+    P.active[slot] = 1;
+    P.count++;
+    P.size = std::max(P.size, slot + 1);
     return AVBD_OK;
 }
-int pool_free(DynHost& D, unsigned slot) {
-    if (slot >= D.active.size() || !D.active[slot]) return set_error(AVBD_ERR_STATE, "freeSlot called on inactive slot");
-    D.active[slot] = 0;
-    D.count--;
-    D.slots[--D.top] = slot;
+int pool_free(DynHost::Pool& P, unsigned slot) {
+    if (slot >= P.active.size() || !P.active[slot]) return set_error(AVBD_ERR_STATE, "freeSlot called on inactive slot");
+    P.active[slot] = 0;
+    P.count--;
+    P.slots[--P.top] = slot;
     return AVBD_OK;
 }
 
@@ -165,15 +172,22 @@ void mark_dirty(DynHost& D, unsigned p) {
     }
 }
 
+// _addCollision: k_start from the smallest mass of the contact's particles,
+// frame from the normal, all its particles dirty
 int add_contact(avbd_ctx* c, DynHost& D, DynHost::Det& d) {
-    const double mn = std::min({c->mass[d.tri[0]], c->mass[d.tri[1]], c->mass[d.tri[2]], c->mass[d.rb]});
+    const int np = d.pool == POOL_TRI_ROD ? 5 : 4;
+    unsigned ps[5] = {d.tri[0], d.tri[1], d.tri[2], d.p4[0], d.p4[1]};
+    double mn = c->mass[ps[0]];
+    for (int k = 1; k < np; k++) mn = std::min(mn, c->mass[ps[k]]);
     const double ks = mn / (c->params.dt * c->params.dt);
+    DynHost::Pool& P = D.pool[d.pool];
     unsigned slot;
-    if (int r = pool_alloc(D, slot)) return r;
-    DynHost::Rec& e = D.rec[slot];
+    if (int r = pool_alloc(P, D.cap, slot)) return r;
+    DynHost::Rec& e = P.rec[slot];
     e = DynHost::Rec{};
-    e.p[0] = d.tri[0]; e.p[1] = d.tri[1]; e.p[2] = d.tri[2]; e.p[3] = d.rb;
+    for (int k = 0; k < 5; k++) e.p[k] = k < np ? ps[k] : 0;
     for (int i = 0; i < 3; i++) { e.n[i] = d.n[i]; e.bar[i] = d.bar[i]; e.cpl[i] = d.cpl[i]; }
+    e.s = d.s;
     normal_basis(d.n, e.t, e.b);
     e.k[0] = e.k[1] = e.k[2] = e.k[3] = ks;
     e.lam[0] = e.lam[1] = e.lam[2] = e.lam[3] = 0;
@@ -181,22 +195,24 @@ int add_contact(avbd_ctx* c, DynHost& D, DynHost::Det& d) {
     e.mu_k = 0.2;
     e.flag = CF_ACTIVE;
     d.e_idx = slot;
-    for (int k = 0; k < 3; k++) mark_dirty(D, d.tri[k]);
-    mark_dirty(D, d.rb);
+    for (int k = 0; k < np; k++) mark_dirty(D, ps[k]);
     D.csr_dirty = true;
     D.contacts_added++;
     return AVBD_OK;
 }
 
+// _updateCollision: new barycentrics, body-frame point (and s), frame update
 void update_contact(DynHost& D, const DynHost::Det& d) {
-    DynHost::Rec& e = D.rec[d.e_idx];
+    DynHost::Rec& e = D.pool[d.pool].rec[d.e_idx];
     for (int i = 0; i < 3; i++) { e.cpl[i] = d.cpl[i]; e.bar[i] = d.bar[i]; }
+    e.s = d.s;
     update_frame(e, d.n);
 }
 
 int remove_contact(DynHost& D, const DynHost::Det& d) {
-    if (int r = pool_free(D, d.e_idx)) return r;
-    D.rec[d.e_idx].flag = 0;
+    DynHost::Pool& P = D.pool[d.pool];
+    if (int r = pool_free(P, d.e_idx)) return r;
+    P.rec[d.e_idx].flag = 0;
     D.csr_dirty = true;
     D.contacts_removed++;
     return AVBD_OK;
@@ -231,11 +247,15 @@ int handle_detections(avbd_ctx* c, DynHost& D) {
 void build_dynamic_adjacency(DynHost& D, unsigned n) {
     D.dyn_off.assign(n + 1, 0);
     D.dnb_off.assign(n + 1, 0);
-    for (unsigned s = 0; s < D.size; s++) {
-        if (!D.active[s]) continue;
-        for (int k = 0; k < 4; k++) {
-            D.dyn_off[D.rec[s].p[k] + 1]++;
-            D.dnb_off[D.rec[s].p[k] + 1] += 3;
+    for (int pl = 0; pl < 2; pl++) {
+        const DynHost::Pool& P = D.pool[pl];
+        const int np = pl == POOL_TRI_ROD ? 5 : 4;
+        for (unsigned s = 0; s < P.size; s++) {
+            if (!P.active[s]) continue;
+            for (int k = 0; k < np; k++) {
+                D.dyn_off[P.rec[s].p[k] + 1]++;
+                D.dnb_off[P.rec[s].p[k] + 1] += np - 1;
+            }
         }
     }
     for (unsigned p = 0; p < n; p++) {
@@ -245,14 +265,18 @@ void build_dynamic_adjacency(DynHost& D, unsigned n) {
     D.dyn_ent_ext.assign(D.dyn_off[n], 0);
     D.dnb.assign(D.dnb_off[n], 0);
     std::vector<unsigned> ec(D.dyn_off.begin(), D.dyn_off.end() - 1), nc(D.dnb_off.begin(), D.dnb_off.end() - 1);
-    for (unsigned s = 0; s < D.size; s++) {
-        if (!D.active[s]) continue;
-        const DynHost::Rec& e = D.rec[s];
-        for (unsigned k = 0; k < 4; k++) {
-            const unsigned p = e.p[k];
-            D.dyn_ent_ext[ec[p]++] = (s << 2) | k;
-            for (int k2 = 0; k2 < 4; k2++)
-                if ((unsigned)k2 != k) D.dnb[nc[p]++] = e.p[k2];
+    for (int pl = 0; pl < 2; pl++) {  // DynamicEnergyType order: triangle-rigid, triangle-rod
+        const DynHost::Pool& P = D.pool[pl];
+        const unsigned np = pl == POOL_TRI_ROD ? 5 : 4;
+        for (unsigned s = 0; s < P.size; s++) {
+            if (!P.active[s]) continue;
+            const DynHost::Rec& e = P.rec[s];
+            for (unsigned k = 0; k < np; k++) {
+                const unsigned p = e.p[k];
+                D.dyn_ent_ext[ec[p]++] = (s << 4) | ((unsigned)pl << 3) | k;
+                for (unsigned k2 = 0; k2 < np; k2++)
+                    if (k2 != k) D.dnb[nc[p]++] = e.p[k2];
+            }
         }
     }
 }
@@ -367,19 +391,33 @@ void build_lists(avbd_ctx* c, DynHost& D) {
     }
 }
 
+// the step-start hook of every live contact of both pools: thread i < size0
+// serves pool 0 slot i, the rest pool 1
 template <typename R>
-__global__ void k_trc_after_step(DevState<R> s, unsigned size) {
-    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= size || !(s.trc_flag[k] & CF_ACTIVE)) return;
-    trc_after_step<R>(s, k);
+__global__ void k_contact_after_step(DevState<R> s, unsigned size0, unsigned size1) {
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    int pool = 0;
+    if (k >= size0) {
+        k -= size0;
+        pool = 1;
+        if (k >= size1) return;
+    }
+    if (!(s.cp[pool].flag[k] & CF_ACTIVE)) return;
+    dyn_after_step<R>(s, pool, k);
 }
 
 template <typename R>
-__global__ void k_trc_after_iter(DevState<R> s, unsigned size, SceneTol T) {
-    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= size || !(s.trc_flag[k] & CF_ACTIVE)) return;
-    if (T.active && !T.active[T.scene[s.trc_p[k].w]]) return;
-    trc_after_iter<R>(s, k);
+__global__ void k_contact_after_iter(DevState<R> s, unsigned size0, unsigned size1, SceneTol T) {
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    int pool = 0;
+    if (k >= size0) {
+        k -= size0;
+        pool = 1;
+        if (k >= size1) return;
+    }
+    if (!(s.cp[pool].flag[k] & CF_ACTIVE)) return;
+    if (T.active && !T.active[T.scene[s.cp[pool].p[k].w]]) return;
+    dyn_after_iter<R>(s, pool, k);
 }
 
 // _commitConflictedInColor: buffered positions of the color's conflicted
@@ -411,19 +449,24 @@ int alloc_state(avbd_ctx* c, DevState<R>& s, DynHost& D, std::string& err) {
         c->allocations.push_back(*p);
         return true;
     };
-    D.ent_cap = 4 * cap;
-    if (!alloc((void**)&s.trc_p, sizeof(uint4) * cap) || !alloc((void**)&s.trc_n, sizeof(V4) * cap) ||
-        !alloc((void**)&s.trc_t, sizeof(V4) * cap) || !alloc((void**)&s.trc_b, sizeof(V4) * cap) ||
-        !alloc((void**)&s.trc_bar, sizeof(V4) * cap) || !alloc((void**)&s.trc_cpl, sizeof(V4) * cap) ||
-        !alloc((void**)&s.trc_k, sizeof(V4) * cap) || !alloc((void**)&s.trc_lam, sizeof(V4) * cap) ||
-        !alloc((void**)&s.trc_flag, cap) || !alloc((void**)&s.dyn_begin, sizeof(uint32_t) * (n + 1)) ||
+    D.ent_cap = 4 * cap + 5 * cap;  // entries of a full triangle-rigid and a full triangle-rod pool
+    for (int pl = 0; pl < 2; pl++) {
+        ContactPoolDev<R>& P = s.cp[pl];
+        if (!alloc((void**)&P.p, sizeof(uint4) * cap) || !alloc((void**)&P.p5, sizeof(uint32_t) * cap) ||
+            !alloc((void**)&P.n, sizeof(V4) * cap) || !alloc((void**)&P.t, sizeof(V4) * cap) ||
+            !alloc((void**)&P.b, sizeof(V4) * cap) || !alloc((void**)&P.bar, sizeof(V4) * cap) ||
+            !alloc((void**)&P.cpl, sizeof(V4) * cap) || !alloc((void**)&P.k, sizeof(V4) * cap) ||
+            !alloc((void**)&P.lam, sizeof(V4) * cap) || !alloc((void**)&P.flag, cap))
+            return AVBD_ERR_CUDA;
+        P.cap = cap;
+        cudaMemsetAsync(P.flag, 0, cap, c->stream);
+    }
+    if (!alloc((void**)&s.dyn_begin, sizeof(uint32_t) * (n + 1)) ||
         !alloc((void**)&s.dyn_ent, sizeof(uint32_t) * D.ent_cap) || !alloc((void**)&s.dyn_skip, n) ||
         !alloc((void**)&s.conflicted, n) || !alloc((void**)&s.buffered, sizeof(V4) * n) ||
         !alloc((void**)&D.d_lists, sizeof(uint32_t) * 2 * (size_t)n))
         return AVBD_ERR_CUDA;
-    s.trc_cap = cap;
     cudaStream_t st = c->stream;
-    cudaMemsetAsync(s.trc_flag, 0, cap, st);
     cudaMemsetAsync(s.dyn_begin, 0, sizeof(uint32_t) * (n + 1), st);
     cudaMemsetAsync(s.dyn_skip, 0, n, st);
     cudaMemsetAsync(s.conflicted, 0, n, st);
@@ -442,16 +485,16 @@ int alloc_state(avbd_ctx* c, DevState<R>& s, DynHost& D, std::string& err) {
         if (e_ != cudaSuccess) return set_error(AVBD_ERR_CUDA, cudaGetErrorString(e_));     \
     } while (0)
 
-// reads the device's k / lam / flag of slots [0, size) into the host mirror
+// reads the device's k / lam / flag of slots [0, size) of one pool into the host mirror
 template <typename R>
-int download_pool(DevState<R>& s, DynHost& D, cudaStream_t st) {
+int download_pool(const ContactPoolDev<R>& S, DynHost::Pool& D, cudaStream_t st) {
     using V4 = typename Vec4Of<R>::T;
     if (D.size == 0) return AVBD_OK;
     std::vector<V4> k(D.size), lam(D.size);
     std::vector<uint8_t> f(D.size);
-    DYN_CUDA(cudaMemcpyAsync(k.data(), s.trc_k, sizeof(V4) * D.size, cudaMemcpyDeviceToHost, st));
-    DYN_CUDA(cudaMemcpyAsync(lam.data(), s.trc_lam, sizeof(V4) * D.size, cudaMemcpyDeviceToHost, st));
-    DYN_CUDA(cudaMemcpyAsync(f.data(), s.trc_flag, D.size, cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaMemcpyAsync(k.data(), S.k, sizeof(V4) * D.size, cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaMemcpyAsync(lam.data(), S.lam, sizeof(V4) * D.size, cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaMemcpyAsync(f.data(), S.flag, D.size, cudaMemcpyDeviceToHost, st));
     DYN_CUDA(cudaStreamSynchronize(st));
     for (unsigned i = 0; i < D.size; i++) {
         if (!D.active[i]) continue;
@@ -464,11 +507,12 @@ int download_pool(DevState<R>& s, DynHost& D, cudaStream_t st) {
 }
 
 template <typename R>
-int upload_pool(avbd_ctx* c, DevState<R>& s, DynHost& D, cudaStream_t st) {
+int upload_pool(avbd_ctx* c, ContactPoolDev<R>& S, const DynHost::Pool& D, cudaStream_t st) {
     using V4 = typename Vec4Of<R>::T;
     const unsigned m = D.size;
     if (m == 0) return AVBD_OK;
     std::vector<uint4> p(m);
+    std::vector<uint32_t> p5(m, 0);
     std::vector<V4> vn(m), vt(m), vb(m), vbar(m), vcpl(m), vk(m), vlam(m);
     std::vector<uint8_t> f(m);
     auto v4 = [](const double a[3], double w) {
@@ -484,7 +528,8 @@ int upload_pool(avbd_ctx* c, DevState<R>& s, DynHost& D, cudaStream_t st) {
             continue;
         }
         p[i] = make_uint4(c->inv[e.p[0]], c->inv[e.p[1]], c->inv[e.p[2]], c->inv[e.p[3]]);
-        vn[i] = v4(e.n, 0);
+        p5[i] = c->inv[e.p[4]];
+        vn[i] = v4(e.n, e.s);
         vt[i] = v4(e.t, 0);
         vb[i] = v4(e.b, 0);
         vbar[i] = v4(e.bar, e.mu_s);
@@ -493,15 +538,16 @@ int upload_pool(avbd_ctx* c, DevState<R>& s, DynHost& D, cudaStream_t st) {
         vlam[i] = v4(e.lam, e.lam[3]);
         f[i] = e.flag;
     }
-    DYN_CUDA(cudaMemcpyAsync(s.trc_p, p.data(), sizeof(uint4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_n, vn.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_t, vt.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_b, vb.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_bar, vbar.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_cpl, vcpl.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_k, vk.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_lam, vlam.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(s.trc_flag, f.data(), m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.p, p.data(), sizeof(uint4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.p5, p5.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.n, vn.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.t, vt.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.b, vb.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.bar, vbar.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.cpl, vcpl.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.k, vk.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.lam, vlam.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.flag, f.data(), m, cudaMemcpyHostToDevice, st));
     // the host vectors are pageable: the copies complete before the call returns
     DYN_CUDA(cudaStreamSynchronize(st));
     return AVBD_OK;
@@ -515,7 +561,7 @@ int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vecto
     const unsigned n = (unsigned)c->perm.size();
     DynHost* D = new DynHost();
     // a merge may add this stage's contacts before it frees the last stage's,
-    // so the pool holds up to twice the narrow phase's capacity
+    // so each pool holds up to twice the narrow phase's capacity
     D->cap = 2 * c->lbvh.contact_capacity;
     D->p_off = p_off;
     D->p_nbr = p_nbr;
@@ -565,19 +611,23 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     (void)k;
     DynHost& D = *c->dyn;
     LbvhState& L = c->lbvh;
-    // detections of the narrow phase and the pool's multipliers
+    // detections of the narrow phase and the pools' multipliers
     uint32_t cnt = 0;
     DYN_CUDA(cudaMemcpyAsync(&cnt, L.contact_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    if (int r = download_pool<R>(s, D, st)) return r;  // synchronizes the stream
+    for (int pl = 0; pl < 2; pl++)
+        if (int r = download_pool<R>(s.cp[pl], D.pool[pl], st)) return r;
+    DYN_CUDA(cudaStreamSynchronize(st));
     if (cnt > L.contact_capacity)
-        return set_error(AVBD_ERR_CAPACITY, "triangle-sphere contacts exceed the narrow phase's capacity");
+        return set_error(AVBD_ERR_CAPACITY, "narrow-phase contacts exceed the contact buffer's capacity");
     D.h_key.resize(cnt);
     D.h_idx.resize(cnt);
-    D.h_vec.resize(9ull * cnt);
+    D.h_idx5.resize(cnt);
+    D.h_vec.resize(10ull * cnt);
     if (cnt) {
         DYN_CUDA(cudaMemcpyAsync(D.h_key.data(), L.contact_key, sizeof(uint64_t) * cnt, cudaMemcpyDeviceToHost, st));
         DYN_CUDA(cudaMemcpyAsync(D.h_idx.data(), L.contact_idx, sizeof(uint4) * cnt, cudaMemcpyDeviceToHost, st));
-        DYN_CUDA(cudaMemcpyAsync(D.h_vec.data(), L.contact_vec, sizeof(double) * 9 * cnt, cudaMemcpyDeviceToHost, st));
+        DYN_CUDA(cudaMemcpyAsync(D.h_idx5.data(), L.contact_idx5, sizeof(uint32_t) * cnt, cudaMemcpyDeviceToHost, st));
+        DYN_CUDA(cudaMemcpyAsync(D.h_vec.data(), L.contact_vec, sizeof(double) * 10 * cnt, cudaMemcpyDeviceToHost, st));
         DYN_CUDA(cudaStreamSynchronize(st));
     }
     D.prev.swap(D.cur);
@@ -585,15 +635,18 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     for (uint32_t i = 0; i < cnt; i++) {
         DynHost::Det& d = D.cur[i];
         d.key = D.h_key[i];
+        d.pool = (d.key >> 59) == 3u ? POOL_TRI_ROD : POOL_TRI_RIGID;  // DetectedCollisionType in the top 5 bits
         d.tri[0] = c->perm[D.h_idx[i].x];
         d.tri[1] = c->perm[D.h_idx[i].y];
         d.tri[2] = c->perm[D.h_idx[i].z];
-        d.rb = c->perm[D.h_idx[i].w];
+        d.p4[0] = c->perm[D.h_idx[i].w];
+        d.p4[1] = d.pool == POOL_TRI_ROD ? c->perm[D.h_idx5[i]] : 0u;
         for (int j = 0; j < 3; j++) {
-            d.n[j] = D.h_vec[9ull * i + j];
-            d.bar[j] = D.h_vec[9ull * i + 3 + j];
-            d.cpl[j] = D.h_vec[9ull * i + 6 + j];
+            d.n[j] = D.h_vec[10ull * i + j];
+            d.bar[j] = D.h_vec[10ull * i + 3 + j];
+            d.cpl[j] = D.h_vec[10ull * i + 6 + j];
         }
+        d.s = D.h_vec[10ull * i + 9];
         d.e_idx = 0;
     }
     // the narrow phase appends in any order; the reference radix-sorts by key
@@ -605,7 +658,8 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     build_lists(c, D);
 
     // uploads: pool records, dynamic adjacency (engine order), flags, lists
-    if (int r = upload_pool<R>(c, s, D, st)) return r;
+    for (int pl = 0; pl < 2; pl++)
+        if (int r = upload_pool<R>(c, s.cp[pl], D.pool[pl], st)) return r;
     if (D.csr_dirty) {
         D.dyn_begin.assign(n + 1, 0);
         for (unsigned i = 0; i < n; i++) {
@@ -638,8 +692,9 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
                                  st));
     DYN_CUDA(cudaStreamSynchronize(st));
     // the contacts' step-start hook, at the positions of the step start
-    if (D.size) {
-        k_trc_after_step<R><<<nblk(D.size, 128), 128, 0, st>>>(s, D.size);
+    const unsigned s0 = D.pool[0].size, s1 = D.pool[1].size;
+    if (s0 + s1) {
+        k_contact_after_step<R><<<nblk(s0 + s1, 128), 128, 0, st>>>(s, s0, s1);
         count_launch(c);
     }
     return AVBD_OK;
@@ -667,10 +722,11 @@ void dyn_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned 
 }
 
 template <typename R>
-void launch_trc_after_iter(avbd_ctx* c, DevState<R>& s, cudaStream_t st, const SceneTol& T) {
-    const unsigned m = c->dyn ? c->dyn->size : 0;
-    if (!m) return;
-    k_trc_after_iter<R><<<nblk(m, 128), 128, 0, st>>>(s, m, T);
+void launch_contact_after_iter(avbd_ctx* c, DevState<R>& s, cudaStream_t st, const SceneTol& T) {
+    if (!c->dyn) return;
+    const unsigned s0 = c->dyn->pool[0].size, s1 = c->dyn->pool[1].size;
+    if (!(s0 + s1)) return;
+    k_contact_after_iter<R><<<nblk(s0 + s1, 128), 128, 0, st>>>(s, s0, s1, T);
     count_launch(c);
 }
 
@@ -681,37 +737,42 @@ using namespace avbd;
 
 extern "C" {
 
-int avbd_dynamic_info(avbd_ctx* c, unsigned out[6]) {
+int avbd_dynamic_info(avbd_ctx* c, unsigned out[8]) {
     if (!c || !out) return set_error(AVBD_ERR_INVALID_ARG, "null argument");
-    std::fill(out, out + 6, 0u);
+    std::fill(out, out + 8, 0u);
     if (!c->dyn) return AVBD_OK;
     const DynHost& D = *c->dyn;
-    out[0] = D.count;
-    out[1] = D.size;
+    out[0] = D.pool[0].count;
+    out[1] = D.pool[0].size;
     out[2] = D.num_colors;
     out[3] = (unsigned)D.touched_conflicted.size();
     out[4] = (unsigned)D.dirty.size();
     out[5] = (unsigned)D.dyn_ent_ext.size();
+    out[6] = D.pool[1].count;
+    out[7] = D.pool[1].size;
     return AVBD_OK;
 }
 
-int avbd_get_contact_pool(avbd_ctx* c, unsigned capacity, unsigned* p4, uint8_t* active, double* data24,
-                          unsigned* size) {
+// pool `pl` by slot into p (np per slot), active, data (24 or 25 per slot)
+static int get_pool(avbd_ctx* c, int pl, unsigned capacity, unsigned* p, uint8_t* active, double* data,
+                    unsigned* size) {
     if (!c || !size) return set_error(AVBD_ERR_INVALID_ARG, "null argument");
     *size = 0;
     if (!c->dyn) return AVBD_OK;
-    DynHost& D = *c->dyn;
+    DynHost::Pool& D = c->dyn->pool[pl];
     if (cudaSetDevice(c->device) != cudaSuccess) return set_error(AVBD_ERR_CUDA, "cudaSetDevice");
     const bool d64 = c->solver.precision != AVBD_PRECISION_FP32;
-    if (int r = d64 ? download_pool<double>(c->d, D, c->stream) : download_pool<float>(c->f, D, c->stream)) return r;
+    if (int r = d64 ? download_pool<double>(c->d.cp[pl], D, c->stream) : download_pool<float>(c->f.cp[pl], D, c->stream))
+        return r;
+    const int np = pl == POOL_TRI_ROD ? 5 : 4, nd = pl == POOL_TRI_ROD ? 25 : 24;
     *size = D.size;
     for (unsigned i = 0; i < D.size && i < capacity; i++) {
         const DynHost::Rec& e = D.rec[i];
-        if (p4)
-            for (int k = 0; k < 4; k++) p4[4 * i + k] = e.p[k];
+        if (p)
+            for (int k = 0; k < np; k++) p[np * i + k] = e.p[k];
         if (active) active[i] = D.active[i];
-        if (data24) {
-            double* o = data24 + 24ull * i;
+        if (data) {
+            double* o = data + (size_t)nd * i;
             for (int j = 0; j < 3; j++) {
                 o[j] = e.n[j];
                 o[3 + j] = e.t[j];
@@ -719,20 +780,32 @@ int avbd_get_contact_pool(avbd_ctx* c, unsigned capacity, unsigned* p4, uint8_t*
                 o[9 + j] = e.bar[j];
                 o[12 + j] = e.cpl[j];
             }
-            o[15] = e.k[3];
-            o[16] = e.k[0];
-            o[17] = e.k[1];
-            o[18] = e.k[2];
-            for (int j = 0; j < 4; j++) o[19 + j] = e.lam[j];
-            o[23] = ((e.flag & CF_USE_STATIC) ? 1 : 0) + ((e.flag & CF_UNCLAMPED) ? 2 : 0);
+            int q = 15;
+            if (pl == POOL_TRI_ROD) o[q++] = e.s;  // the rod record carries s before k
+            o[q] = e.k[3];
+            o[q + 1] = e.k[0];
+            o[q + 2] = e.k[1];
+            o[q + 3] = e.k[2];
+            for (int j = 0; j < 4; j++) o[q + 4 + j] = e.lam[j];
+            o[q + 8] = ((e.flag & CF_USE_STATIC) ? 1 : 0) + ((e.flag & CF_UNCLAMPED) ? 2 : 0);
         }
     }
     return AVBD_OK;
 }
 
+int avbd_get_contact_pool(avbd_ctx* c, unsigned capacity, unsigned* p4, uint8_t* active, double* data24,
+                          unsigned* size) {
+    return get_pool(c, POOL_TRI_RIGID, capacity, p4, active, data24, size);
+}
+
+int avbd_get_rod_contact_pool(avbd_ctx* c, unsigned capacity, unsigned* p5, uint8_t* active, double* data25,
+                              unsigned* size) {
+    return get_pool(c, POOL_TRI_ROD, capacity, p5, active, data25, size);
+}
+
 int avbd_debug_set_recolor_rounds(avbd_ctx* c, unsigned rounds) {
     if (!c) return set_error(AVBD_ERR_INVALID_ARG, "null context");
-    if (!c->dyn) return set_error(AVBD_ERR_STATE, "no dynamic contacts (finalize a context with triangles and spheres)");
+    if (!c->dyn) return set_error(AVBD_ERR_STATE, "no dynamic contacts (finalize a context with triangles and spheres or rod segments)");
     c->dyn->rounds = rounds;
     return AVBD_OK;
 }
@@ -745,7 +818,7 @@ namespace avbd {
     template int dyn_manage<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                     \
     template void dyn_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, cudaStream_t,      \
                                      const SceneTol&);                                                         \
-    template void launch_trc_after_iter<R>(avbd_ctx*, DevState<R>&, cudaStream_t, const SceneTol&);
+    template void launch_contact_after_iter<R>(avbd_ctx*, DevState<R>&, cudaStream_t, const SceneTol&);
 INST(float)
 INST(double)
 #undef INST

@@ -41,6 +41,24 @@ static_assert(sizeof(IncRec<double>) == 112, "FP64 incidence record must be 112 
 enum VertexFlags : uint8_t { VF_FIXED = 1, VF_ORIENTED = 2, VF_GROUND = 4 };
 enum GroundFlags : uint8_t { GF_USE_STATIC = 1, GF_UNCLAMPED = 2 };
 
+// One dynamic contact pool on the device, by slot (see DevState::cp).
+template <typename R>
+struct ContactPoolDev {
+    using V4 = typename Vec4Of<R>::T;
+    unsigned cap = 0;                // slots allocated
+    uint4* p = nullptr;              // internal vertex ids: triangle x3, rigid body / first rod node
+    uint32_t* p5 = nullptr;          // second rod node (triangle-rod pool)
+    V4* n = nullptr;                 // contact frame: normal (w: s along the segment, triangle-rod),
+    V4* t = nullptr;                 //   tangent,
+    V4* b = nullptr;                 //   binormal
+    V4* bar = nullptr;               // barycentrics of the triangle point, mu_s in w
+    V4* cpl = nullptr;               // contact point in the body (or interpolated rod) frame, mu_k in w
+    V4* k = nullptr;                 // k_n, k_t, k_b, k_start
+    V4* lam = nullptr;               // lam_n, lam_t, lam_b, C_n_prev
+    uint8_t* flag = nullptr;         // ContactFlags
+};
+enum ContactPoolType { POOL_TRI_RIGID = 0, POOL_TRI_ROD = 1 };
+
 // Device arrays of one precision.  All per-vertex arrays use the internal
 // (color-major) vertex order.
 template <typename R>
@@ -93,20 +111,12 @@ struct DevState {
     V4* jrq = nullptr;               // reference rotation (quaternion)
     uint8_t* oflag = nullptr;        // per rotation slot, OrientedFlags
 
-    // ---- triangle-rigid contacts (TriangleRigidCollisionEnergyPool), by pool
-    // slot; the host manages the pool between steps (contacts.cu)
-    unsigned trc_cap = 0;            // slots allocated on the device
-    uint4* trc_p = nullptr;          // internal vertex ids: triangle x3, rigid body
-    V4* trc_n = nullptr;             // contact frame: normal, tangent, binormal
-    V4* trc_t = nullptr;
-    V4* trc_b = nullptr;
-    V4* trc_bar = nullptr;           // barycentrics of the triangle point, mu_s in w
-    V4* trc_cpl = nullptr;           // contact point in the body frame, mu_k in w
-    V4* trc_k = nullptr;             // k_n, k_t, k_b, k_start
-    V4* trc_lam = nullptr;           // lam_n, lam_t, lam_b, C_n_prev
-    uint8_t* trc_flag = nullptr;     // ContactFlags
-    // dynamic adjacency per internal vertex: entries (slot << 2 | local);
-    // null when the context has no triangle-sphere pairs
+    // ---- dynamic contacts: cp[0] triangle-rigid (TriangleRigidCollisionEnergyPool),
+    // cp[1] triangle-rod (TriangleRodCollisionEnergyPool), by pool slot; the
+    // host manages the pools between steps (contacts.cu)
+    ContactPoolDev<R> cp[2];
+    // dynamic adjacency per internal vertex, entries (slot << 4 | pool << 3 |
+    // local), by pool then slot; null when the context has no dynamic contacts
     uint32_t* dyn_begin = nullptr;   // n + 1
     uint32_t* dyn_ent = nullptr;
     uint8_t* dyn_skip = nullptr;     // 1: has contacts or a new color, solved from its color's list, not its slab
@@ -176,11 +186,13 @@ struct LbvhState {
     double* vd = nullptr;
     unsigned hist_blocks = 0;
     uint32_t* obj = nullptr;        // object id of each primitive
-    // narrow-phase detections (triangle-sphere), allocated when spheres exist
+    // narrow-phase detections, allocated when triangles meet spheres or rod segments
     unsigned contact_capacity = 0;
-    uint64_t* contact_key = nullptr;
-    uint4* contact_idx = nullptr;   // triangle's three vertices, sphere particle (internal order)
-    double* contact_vec = nullptr;  // normal, barycentrics, contact point in the sphere frame
+    uint64_t* contact_key = nullptr;  // DetectedCollision key: type 2 triangle-sphere, 3 triangle-rod
+    uint4* contact_idx = nullptr;   // triangle's three vertices, sphere particle / first rod node (internal order)
+    uint32_t* contact_idx5 = nullptr;  // second rod node
+    double* contact_vec = nullptr;  // 10 per contact: normal, barycentrics, contact point in the body
+                                    // (or interpolated rod) frame, s along the segment
     uint32_t* contact_count = nullptr;
 };
 
@@ -307,7 +319,7 @@ template <typename R>
 void dyn_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned color, cudaStream_t st,
                      const SceneTol& T);
 template <typename R>
-void launch_trc_after_iter(avbd_ctx* c, DevState<R>& s, cudaStream_t st, const SceneTol& T);
+void launch_contact_after_iter(avbd_ctx* c, DevState<R>& s, cudaStream_t st, const SceneTol& T);
 unsigned dyn_num_colors(const avbd_ctx* c);
 // the positional vertices solved from lists (all colors), for the residual pass
 void dyn_positional_list(const avbd_ctx* c, const uint32_t** list, unsigned* count);

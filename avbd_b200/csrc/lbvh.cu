@@ -397,12 +397,14 @@ int lbvh_allocate(avbd_ctx* c, std::string& err) {
     std::vector<uint4> pidx(n);
     std::vector<double> radius(n);
     std::vector<uint32_t> obj(n);
-    unsigned spheres = 0;
+    unsigned spheres = 0, segments = 0, triangles = 0;
     for (unsigned i = 0; i < n; i++) {
         const HostPrim& p = c->prims[i];
         type[i] = p.type;
         obj[i] = p.object_id;
         spheres += p.type == AVBD_SHAPE_SPHERE;
+        segments += p.type == AVBD_SHAPE_ROD_SEGMENT;
+        triangles += p.type == AVBD_SHAPE_TRIANGLE;
         pidx[i] = make_uint4(c->inv[p.idx[0]], p.type == AVBD_SHAPE_SPHERE ? 0 : c->inv[p.idx[1]],
                              p.type == AVBD_SHAPE_TRIANGLE ? c->inv[p.idx[2]] : 0, 0);
         radius[i] = p.radius;
@@ -429,11 +431,12 @@ int lbvh_allocate(avbd_ctx* c, std::string& err) {
         !alloc((void**)&L.range, sizeof(uint2) * std::max(1u, n - 1)) ||
         !alloc((void**)&L.obj, sizeof(uint32_t) * n))
         return AVBD_ERR_CUDA;
-    if (spheres) {  // room for 64 triangle contacts per sphere
-        L.contact_capacity = std::max(1024u, 64u * spheres);
+    if (triangles && (spheres || segments)) {  // room for 64 triangle contacts per sphere, 16 per segment
+        L.contact_capacity = std::max(1024u, 64u * spheres + 16u * segments);
         if (!alloc((void**)&L.contact_key, sizeof(uint64_t) * L.contact_capacity) ||
             !alloc((void**)&L.contact_idx, sizeof(uint4) * L.contact_capacity) ||
-            !alloc((void**)&L.contact_vec, sizeof(double) * 9 * L.contact_capacity) ||
+            !alloc((void**)&L.contact_idx5, sizeof(uint32_t) * L.contact_capacity) ||
+            !alloc((void**)&L.contact_vec, sizeof(double) * 10 * L.contact_capacity) ||
             !alloc((void**)&L.contact_count, sizeof(uint32_t)))
             return AVBD_ERR_CUDA;
         cudaMemsetAsync(L.contact_count, 0, sizeof(uint32_t), c->stream);

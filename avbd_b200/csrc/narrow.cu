@@ -1,10 +1,12 @@
 // narrow.cu -- narrow phase of the collision stage: the broad phase's
 // candidate leaf pairs are mapped to primitives, same-object pairs sharing a
-// vertex are skipped, and triangle-sphere pairs run the continuous collision
+// vertex are skipped; triangle-sphere pairs run the continuous collision
 // test of CollisionDetector::_triangleSDF_CCD (collision/CollisionDetector.cpp:
 // 689-876; Pelletier-Guenette 2025): alternating golden-section searches in
 // time and on the triangle for the first contact of the moving triangle with
-// the moving sphere during the step.  One thread per candidate pair.
+// the moving sphere during the step; triangle-rod-segment pairs the
+// closest-point test of CollisionDetector::_triangleRod (:601-666) at the
+// step-start positions.  One thread per candidate pair.
 //
 // Compiled without FMA contraction, in FP64, in the reference's operation
 // order: detections equal the FP64 oracle's (sin/cos of a rotating sphere may
@@ -138,6 +140,154 @@ AVBD_D bool tri_sphere_ccd(const Body& B, const D3 p[3], const D3 vv[3], double 
     return sd < margin;
 }
 
+// Math::closestPoint_PointTriangle (common/Math.hpp:446-500), Ericson's regions
+AVBD_D D3 closest_point_triangle(D3 p, D3 a, D3 b, D3 c) {
+    const D3 ab = b - a, ac = c - a, ap = p - a;
+    const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+    if (d1 <= 0 && d2 <= 0) return a;
+    const D3 bp = p - b;
+    const double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 >= 0 && d4 <= d3) return b;
+    const D3 cp = p - c;
+    const double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+    if (d6 >= 0 && d5 <= d6) return c;
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0 && d1 >= 0 && d3 <= 0) return a + (d1 / (d1 - d3)) * ab;
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0) return a + (d2 / (d2 - d6)) * ac;
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) return b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b);
+    const double den = 1.0 / (va + vb + vc);
+    const double v = vb * den, w = vc * den;
+    return a + v * ab + w * ac;
+}
+
+AVBD_D double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }  // std::clamp
+
+// Math::closestPoint_SegmentSegment (common/Math.hpp:508-560): s on (p1, q1), t on (p2, q2)
+AVBD_D void closest_segment_segment(D3 p1, D3 q1, D3 p2, D3 q2, double& s, double& t) {
+    const D3 d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+    const double a = dot3(d1, d1), e = dot3(d2, d2), f = dot3(d2, r);
+    const double EPS = 1e-8;
+    if (a <= EPS && e <= EPS) {
+        s = t = 0.0;
+        return;
+    }
+    if (a <= EPS) {
+        s = 0.0;
+        t = clamp01(f / e);
+    } else {
+        const double cc = dot3(d1, r);
+        if (e <= EPS) {
+            t = 0.0;
+            s = clamp01(-cc / a);
+        } else {
+            const double b = dot3(d1, d2);
+            const double den = a * e - b * b;
+            s = den != 0.0 ? clamp01((b * f - cc * e) / den) : 0.0;
+            t = (b * s + f) / e;
+            if (t < 0.0) {
+                t = 0.0;
+                s = clamp01(-cc / a);
+            } else if (t > 1.0) {
+                t = 1.0;
+                s = clamp01((b - cc) / a);
+            }
+        }
+    }
+}
+
+// Math::pointInTriangle (common/Math.hpp:562-591)
+AVBD_D bool point_in_triangle(D3 p, D3 a, D3 b, D3 c) {
+    const D3 v0 = b - a, v1 = c - a, v2 = p - a;
+    const double d00 = dot3(v0, v0), d01 = dot3(v0, v1), d11 = dot3(v1, v1), d20 = dot3(v2, v0), d21 = dot3(v2, v1);
+    const double den = d00 * d11 - d01 * d01;
+    if (fabs(den) < 1e-12) return false;
+    const double v = (d11 * d20 - d01 * d21) / den;
+    const double w = (d00 * d21 - d01 * d20) / den;
+    const double u = 1.0 - v - w;
+    return u >= -1e-8 && v >= -1e-8 && w >= -1e-8;
+}
+
+// Math::closestPoint_SegmentTriangle (common/Math.hpp:593-681): the crossing
+// point, else the closest of the three edge tests and the two end points.
+// The edge test measures the distance to the edge point at the segment's
+// parameter s, (1-s) q0 + s q1, as the reference does.
+AVBD_D void closest_segment_triangle(D3 p0, D3 p1, D3 a, D3 b, D3 c, double& s_out, D3& bary, double& dist) {
+    const double EPS = 1e-8;
+    const D3 dir = p1 - p0;
+    const D3 nrm = cross3(b - a, c - a);
+    s_out = 0.0;
+    bary = mk3(1.0, 0.0, 0.0);
+    dist = 1.7976931348623157e308;  // std::numeric_limits<double>::max()
+    if (dot3(nrm, nrm) > EPS) {
+        const double den = dot3(nrm, dir);
+        if (fabs(den) > EPS) {
+            const double s = dot3(nrm, a - p0) / den;
+            if (s >= 0.0 && s <= 1.0) {
+                const D3 p = p0 + s * dir;
+                if (point_in_triangle(p, a, b, c)) {
+                    s_out = s;
+                    bary = barycentric(p, a, b, c);
+                    dist = 0.0;
+                    return;
+                }
+            }
+        }
+    }
+    const D3 q0s[3] = {a, a, b}, q1s[3] = {b, c, c};
+    const int i0s[3] = {0, 0, 1}, i1s[3] = {1, 2, 2};
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+        double s, t;
+        closest_segment_segment(p0, p1, q0s[e], q1s[e], s, t);
+        const D3 cp = (1 - s) * p0 + s * p1;
+        const D3 cq = (1 - s) * q0s[e] + s * q1s[e];
+        const D3 dd = cp - cq;
+        const double d2 = dot3(dd, dd);
+        if (d2 < dist * dist) {
+            s_out = s;
+            double bb[3] = {0.0, 0.0, 0.0};
+            bb[i0s[e]] = 1 - t;
+            bb[i1s[e]] = t;
+            bary = mk3(bb[0], bb[1], bb[2]);
+            dist = sqrt(d2);
+        }
+    }
+    const D3 c0 = closest_point_triangle(p0, a, b, c);
+    const D3 e0 = p0 - c0;
+    const double d0 = dot3(e0, e0);
+    if (d0 < dist * dist) {
+        s_out = 0.0;
+        bary = barycentric(c0, a, b, c);
+        dist = sqrt(d0);
+    }
+    const D3 c1 = closest_point_triangle(p1, a, b, c);
+    const D3 e1 = p1 - c1;
+    const double d1 = dot3(e1, e1);
+    if (d1 < dist * dist) {
+        s_out = 1.0;
+        bary = barycentric(c1, a, b, c);
+        dist = sqrt(d1);
+    }
+}
+
+// CollisionDetector::_triangleRod (collision/CollisionDetector.cpp:601-666)
+AVBD_D bool tri_rod_contact(const D3 v[3], D3 s1, D3 s2, DQ q1, DQ q2, double radius, double margin, D3& normal,
+                            D3& bary, double& s, D3& cp_local) {
+    double dist;
+    closest_segment_triangle(s1, s2, v[0], v[1], v[2], s, bary, dist);
+    if (!(dist < radius + margin)) return false;
+    const D3 cl = (1 - s) * s1 + s * s2;
+    const D3 ct = bary.x * v[0] + bary.y * v[1] + bary.z * v[2];
+    const D3 d = ct - cl;
+    const double m = norm3(d);
+    normal = m > 1e-8 ? mk3(d.x / m, d.y / m, d.z / m) : mk3(1.0, 0.0, 0.0);
+    const DQ qm = plus_s3(q1, s * minus_s3(q2, q1));
+    cp_local = qrot_inv(qm, radius * normal);
+    return true;
+}
+
 // DetectedCollision::generateKey (collision/DetectedCollision.hpp:43-66)
 AVBD_D uint64_t collision_key(unsigned type, unsigned a, unsigned b, unsigned code) {
     if (a > b) { unsigned t = a; a = b; b = t; }
@@ -171,7 +321,33 @@ __global__ void __launch_bounds__(128) k_narrow(DevState<R> s, LbvhState L, doub
             if (share) continue;
         }
         if (L.type[a] > L.type[b]) { unsigned t = a; a = b; b = t; }
-        if (!(L.type[a] == AVBD_SHAPE_TRIANGLE && L.type[b] == AVBD_SHAPE_SPHERE)) continue;
+        if (L.type[a] != AVBD_SHAPE_TRIANGLE) continue;
+        if (L.type[b] == AVBD_SHAPE_ROD_SEGMENT) {
+            const uint4 it = L.pidx[a], ir = L.pidx[b];
+            const D3 v[3] = {ld3<R>(s.x, it.x), ld3<R>(s.x, it.y), ld3<R>(s.x, it.z)};
+            const typename Vec4Of<R>::T qa = s.q[s.rot[ir.x]], qb = s.q[s.rot[ir.y]];
+            const DQ q1{(double)qa.x, (double)qa.y, (double)qa.z, (double)qa.w};
+            const DQ q2{(double)qb.x, (double)qb.y, (double)qb.z, (double)qb.w};
+            D3 nrm, bar, cp;
+            double sp;
+            if (!tri_rod_contact(v, ld3<R>(s.x, ir.x), ld3<R>(s.x, ir.y), q1, q2, L.radius[b], margin, nrm, bar, sp, cp))
+                continue;
+            const unsigned k = atomicAdd(L.contact_count, 1u);
+            if (k >= L.contact_capacity) {
+                atomicExch(err, (int)AVBD_ERR_CAPACITY);
+                continue;
+            }
+            L.contact_key[k] = collision_key(3u, a, b, 0u);  // DetectedCollisionType::TriangleRod
+            L.contact_idx[k] = make_uint4(it.x, it.y, it.z, ir.x);
+            L.contact_idx5[k] = ir.y;
+            double* o = L.contact_vec + 10ull * k;
+            o[0] = nrm.x; o[1] = nrm.y; o[2] = nrm.z;
+            o[3] = bar.x; o[4] = bar.y; o[5] = bar.z;
+            o[6] = cp.x; o[7] = cp.y; o[8] = cp.z;
+            o[9] = sp;
+            continue;
+        }
+        if (L.type[b] != AVBD_SHAPE_SPHERE) continue;
         const uint4 it = L.pidx[a];
         const unsigned rb = L.pidx[b].x, slot = s.rot[rb];
         Body B;
@@ -192,10 +368,12 @@ __global__ void __launch_bounds__(128) k_narrow(DevState<R> s, LbvhState L, doub
         }
         L.contact_key[k] = collision_key(2u, a, b, 0u);  // DetectedCollisionType::TriangleRigid
         L.contact_idx[k] = make_uint4(it.x, it.y, it.z, rb);
-        double* o = L.contact_vec + 9ull * k;
+        L.contact_idx5[k] = 0;
+        double* o = L.contact_vec + 10ull * k;
         o[0] = nrm.x; o[1] = nrm.y; o[2] = nrm.z;
         o[3] = bar.x; o[4] = bar.y; o[5] = bar.z;
         o[6] = cp.x; o[7] = cp.y; o[8] = cp.z;
+        o[9] = 0.0;
     }
 }
 

@@ -397,9 +397,13 @@ __global__ void __launch_bounds__(128) k_solve_rod(DevState<R> s, unsigned begin
     uint8_t f = s.oflag[slot];
     if (f & OF_RGROUND) accumulate_rground<R>(s, slot, x, q, B);
     if (f & OF_JOINT) accumulate_joint<R>(s, slot, x, q, B);
-    // dynamic energies (VBDSolver.hpp:397-446): the body's triangle-rigid contacts
+    // dynamic energies (VBDSolver.hpp:397-446): the node's triangle-rigid then
+    // triangle-rod contacts, each in slot order
     if (s.dyn_begin)
-        for (unsigned k = s.dyn_begin[p]; k < s.dyn_begin[p + 1]; k++) trc_accumulate6<R>(s, s.dyn_ent[k] >> 2, B);
+        for (unsigned k = s.dyn_begin[p]; k < s.dyn_begin[p + 1]; k++) {
+            const uint32_t en = s.dyn_ent[k];
+            dyn_accumulate6<R>(s, dyn_pool(en), dyn_slot(en), dyn_local(en), B);
+        }
     typename Vec4Of<R>::T y4 = s.y[p];
     R m = y4.w;
     V3<R> I = xyz(s.Iv[slot]);

@@ -369,11 +369,12 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
     if (active && lane == 0) {
         if (GROUND && (fl & VF_GROUND)) accumulate_ground<P, HT>(s, p, xi, B);
         if constexpr (DYN) {
-            // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid contacts in slot order
+            // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid then
+            // triangle-rod contacts, each in slot order
             const unsigned e = s.dyn_begin[p + 1];
             for (unsigned k = s.dyn_begin[p]; k < e; k++) {
                 const uint32_t en = s.dyn_ent[k];
-                trc_accumulate3<P, HT>(s, en >> 2, en & 3u, B);
+                dyn_accumulate3<P, HT>(s, dyn_pool(en), dyn_slot(en), dyn_local(en), B);
             }
         }
         typename Vec4Of<P>::T y4 = s.y[p];

@@ -321,6 +321,32 @@ def spheres_on_cube(n: int = 4, num_spheres: int = 4, seed: int = 0, iters: int 
     return sc
 
 
+def rods_on_cube(n: int = 4, num_rods: int = 3, segments: int = 8, seed: int = 0, iters: int = 20,
+                 rho: float = 0.5, dt: float = 1.0 / 60.0, size: float = 1.0, E_cube: float = 1e6,
+                 nu_cube: float = 0.4, rod_length: float = 0.5, rod_radius: float = 0.01, drop: float = 0.002,
+                 speed: float = 0.2) -> Scene:
+    """Cosserat rods dropped flat on a soft tet cube: a cube of n^3 cells
+    (bottom face fixed, surface triangles as collision primitives) and
+    `num_rods` straight rods of `segments` elements (radius 1 cm, E 1e7, nu
+    0.25, rho 1000) lying along x at seeded z over the top face, `drop` above
+    it and falling at `speed`, each its own object with rigid-body ground
+    contact.  Their segments' contacts with the cube's surface are the
+    triangle-rod contact energies of the collision stage."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(name=f"cube{n}_rods{num_rods}x{segments}", dt=dt, solver_iters=iters, iter_acceleration=rho)
+    add_tet_cube(sc, n, size=size, E=E_cube, nu=nu_cube, density=1000.0, fix_bottom=True, surface=True,
+                 object_id=0)
+    for r in range(num_rods):
+        z = (r + 0.5) / num_rods * size + rng.uniform(-0.05, 0.05) * size / num_rods
+        x0 = 0.5 * (size - rod_length) + rng.uniform(-0.05, 0.05)
+        base = add_rod(sc, segments, rod_length, rod_radius, 1e7, 0.25, 1000.0,
+                       (x0, size + rod_radius + drop, z), (0.0, 90.0, 0.0), (0.0, 0.0, 0.0), base_joint=False,
+                       ground=True, collide=True, object_id=1 + r)
+        vel = np.tile([0.0, -speed, 0.0], (segments + 1, 1))
+        sc.record("set_velocities", base, vel, vel)
+    return sc
+
+
 def rods_and_spheres(num_rods: int = 256, segments: int = 100, num_spheres: int = 64, seed: int = 0,
                      iters: int = 20, rho: float = 0.5, dt: float = 1.0 / 60.0, length: float = 1.0,
                      helix_radius: float = 0.02, spacing: float = 0.1) -> Scene:

@@ -270,17 +270,30 @@ AVBD_API int avbd_get_candidate_pairs(avbd_ctx* ctx, unsigned capacity, unsigned
 AVBD_API int avbd_get_contacts(avbd_ctx* ctx, unsigned capacity, uint64_t* keys, unsigned* idx4, double* vec9,
                                unsigned* count);
 
+/* Triangle-rod-segment contacts found by the last collision stage's narrow
+ * phase (CollisionDetector::_triangleRod, collision/CollisionDetector.cpp:
+ * 601-666, with Math::closestPoint_SegmentTriangle, common/Math.hpp:593-681),
+ * in ascending key order.  Per contact: keys[k]; idx5 = the triangle's three
+ * particle slots and the segment's two nodes; vec10 = contact normal (world,
+ * centreline to triangle), barycentrics on the triangle, contact point in
+ * the rod frame interpolated at s, and s along the segment.  Up to
+ * `capacity` contacts are written (pointers may be NULL); *count receives
+ * the number found. */
+AVBD_API int avbd_get_rod_contacts(avbd_ctx* ctx, unsigned capacity, uint64_t* keys, unsigned* idx5,
+                                   double* vec10, unsigned* count);
+
 /* Dynamic contact state after the last step's collision stage (contexts
- * with triangle and sphere primitives; zeros otherwise): out[0] live
- * triangle-rigid contacts, out[1] pool size (highest slot + 1,
+ * with triangles and spheres or rod segments; zeros otherwise): out[0] live
+ * triangle-rigid contacts, out[1] their pool size (highest slot + 1,
  * TombstonePool::totalSize, common/TombstonePool.hpp:53), out[2] colors after
  * the incremental recoloring (ColorList::incrementalRecoloring,
  * common/ColorList.hpp:381-474), out[3] conflicted particles
  * (ColorList::finalizeConflicts, :476-522), out[4] particles left dirty for
  * the next stage, out[5] dynamic adjacency entries
  * (DynamicParticleAdjacency::buildAdjacency,
- * common/DynamicParticleAdjacency.hpp:33-118). */
-AVBD_API int avbd_dynamic_info(avbd_ctx* ctx, unsigned out[6]);
+ * common/DynamicParticleAdjacency.hpp:33-118), out[6] live triangle-rod
+ * contacts, out[7] their pool size. */
+AVBD_API int avbd_dynamic_info(avbd_ctx* ctx, unsigned out[8]);
 
 /* The triangle-rigid contact pool (TriangleRigidCollisionEnergyPool,
  * energy/collision/TriangleRigidCollisionEnergyPool.hpp:10-78) by slot, slots
@@ -293,6 +306,15 @@ AVBD_API int avbd_dynamic_info(avbd_ctx* ctx, unsigned out[6]);
  * the pool size. */
 AVBD_API int avbd_get_contact_pool(avbd_ctx* ctx, unsigned capacity, unsigned* p4, uint8_t* active, double* data24,
                                    unsigned* size);
+
+/* The triangle-rod contact pool (TriangleRodCollisionEnergyPool,
+ * energy/collision/TriangleRodCollisionEnergyPool.hpp:9-86) by slot, as
+ * avbd_get_contact_pool: p5 = the triangle's three particle slots and the
+ * segment's two nodes; data25 = normal, tangent, binormal, barycentrics,
+ * contact point in the interpolated rod frame (3 each), s, k_start, k_n, k_t,
+ * k_b, lambda_n, lambda_t, lambda_b, C_n_prev, flags. */
+AVBD_API int avbd_get_rod_contact_pool(avbd_ctx* ctx, unsigned capacity, unsigned* p5, uint8_t* active,
+                                       double* data25, unsigned* size);
 
 /* Test hook: the round limit of the incremental recoloring (6 in the
  * reference, ColorList.hpp:384).  Fewer rounds leave more particles

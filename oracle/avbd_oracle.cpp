@@ -307,6 +307,37 @@ struct Joint {
 // TriangleRigidCollisionEnergyInfo (energy/collision/TriangleRigidCollisionEnergyPool.hpp:10-16):
 // p[0..2] the triangle's vertices, p[3] the rigid body
 struct TriRigid : Contact { unsigned p[4]; V3 barys, cp_local; };
+// TriangleRodCollisionEnergyInfo (energy/collision/TriangleRodCollisionEnergyPool.hpp:9-15):
+// p[0..2] the triangle's vertices, p[3], p[4] the rod segment's nodes
+struct TriRod : Contact { unsigned p[5]; V3 barys, cp_local; double s = 0; };
+
+// TombstonePool::allocSlot / freeSlot (common/TombstonePool.hpp:56-103).  The
+// stack grows on demand; a slot never reached holds its own index, as the
+// reference's iota-initialised stack does.  freeSlot's lowering of
+// highest_index runs while the freed slot is still active, so it never
+// lowers; the live slots are always a subset of [0, size()).
+struct SlotPool {
+    std::vector<uint8_t> active;
+    std::vector<unsigned> slots;
+    unsigned top = 0, count = 0;
+    unsigned size() const { return (unsigned)active.size(); }
+    unsigned alloc() {
+        if (top == slots.size()) slots.push_back((unsigned)slots.size());
+        unsigned slot = slots[top++];
+        if (slot >= active.size()) active.resize(slot + 1, 0);
+        active[slot] = 1;
+        count++;
+        return slot;
+    }
+    void free(unsigned slot) {
+        if (slot >= active.size() || !active[slot]) throw std::runtime_error("freeSlot called on inactive slot");
+        active[slot] = 0;
+        count--;
+        slots[--top] = slot;
+    }
+};
+enum DynamicType : uint8_t { DYN_TRI_RIGID = 0, DYN_TRI_ROD = 1 };   // DynamicEnergyType order
+struct DynEnt { uint8_t type; unsigned slot; uint16_t local; };
 struct Prim { uint8_t type; unsigned idx[3]; uint8_t np; unsigned object_id; double radius; };
 struct Entry { uint8_t type; unsigned idx; uint16_t local; };
 
@@ -363,18 +394,22 @@ struct Ctx {
     unsigned root = 0;
     std::vector<std::pair<unsigned, unsigned>> pairs;
     // detected triangle-sphere contacts of the last collision stage, ascending key
-    struct Detected { uint64_t key; unsigned tri[3], rb; V3 normal, barys, cp_local; unsigned e_idx = 0; };
+    // type 2 (TriangleRigid): rb = sphere particle; type 3 (TriangleRod): rod[2], s
+    struct Detected {
+        uint64_t key; unsigned type = 2; unsigned tri[3], rb = 0, rod[2] = {0, 0};
+        V3 normal, barys, cp_local; double s = 0; unsigned e_idx = 0;
+    };
     std::vector<Detected> detected;                 // narrow-phase output of the last stage
     std::vector<Detected> contacts, prev_contacts;  // managed detections with their pool slots
 
-    // TriangleRigidCollisionEnergyPool over a TombstonePool (common/TombstonePool.hpp:13-103)
+    // TriangleRigid / TriangleRodCollisionEnergyPool, each over a TombstonePool
     std::vector<TriRigid> trc;
-    std::vector<uint8_t> trc_active;
-    std::vector<unsigned> trc_slots;        // free-slot stack
-    unsigned trc_top = 0, trc_high = 0, trc_count = 0;
+    SlotPool trc_pool;
+    std::vector<TriRod> trd;
+    SlotPool trd_pool;
     // DynamicParticleAdjacency (common/DynamicParticleAdjacency.hpp:17-118)
     std::vector<unsigned> dyn_off;          // np + 1
-    std::vector<std::pair<unsigned, uint16_t>> dyn_ent;   // (slot, local)
+    std::vector<DynEnt> dyn_ent;            // per particle by type, then slot
     std::vector<unsigned> dnb_off, dnb;
     // ColorList incremental recoloring state (common/ColorList.hpp:62-90)
     std::vector<unsigned> last_dirty, dirty, next_dirty, touched_frame, cand_color, touched_conflicted;
@@ -694,6 +729,63 @@ static void trc_accumulate(const Ctx& c, const TriRigid& e, unsigned local, doub
     }
 }
 
+// TriangleRodCollisionConstraintSolver::evaluateConstraint
+// (energy/collision/TriangleRodCollisionEnergySolver.hpp:14-50): the rod point
+// is p_mid + q_mid cp_local, with p_mid and q_mid interpolated at s along the
+// segment (q_mid = q1 (+) s (q2 (-) q1))
+static void trd_eval(const Ctx& c, const TriRod& e, double& Cn, double& Ct, double& Cb) {
+    V3 cp_tri = e.barys.x * c.x[e.p[0]] + e.barys.y * c.x[e.p[1]] + e.barys.z * c.x[e.p[2]];
+    Q4 q1 = c.q[c.rot[e.p[3]]], q2 = c.q[c.rot[e.p[4]]];
+    Q4 qm = plus_s3(q1, e.s * minus_s3(q2, q1));
+    V3 pm = (1 - e.s) * c.x[e.p[3]] + e.s * c.x[e.p[4]];
+    V3 d = (pm + qrot(qm, e.cp_local)) - cp_tri;
+    Cn = dot(e.n, d); Ct = dot(e.t, d); Cb = dot(e.b, d);
+}
+
+// TriangleRodCollisionConstraintSolver::constraintGradientHessian
+// (energy/collision/TriangleRodCollisionEnergySolver.hpp:52-149).  Triangle
+// vertices as for the rigid contact.  Rod node 3 / 4: translation gradient
+// (1 - s) n / s n; rotation gradient -n^T (-R S) dR_s/dR with
+// dR_s/dR = Exp(s dq)^T - s J_r(s dq) J_r^-1(dq)^T for node 3 and
+// s J_r(s dq) J_r^-1(dq) for node 4 (dq = q2 (-) q1, R = R(q_mid),
+// S = skew(cp_local)); tangent and binormal gradients and all constraint
+// Hessians are zero (Gauss-Newton).
+template <int DOF>
+static void trd_accumulate(const Ctx& c, const TriRod& e, unsigned local, double H[DOF][DOF], double G[DOF]) {
+    double Cn, Ct, Cb;
+    trd_eval(c, e, Cn, Ct, Cb);
+    double gn[DOF] = {}, gt[DOF] = {}, gb[DOF] = {};
+    if constexpr (DOF == 6) {
+        Q4 q1 = c.q[c.rot[e.p[3]]], q2 = c.q[c.rot[e.p[4]]];
+        V3 qd = minus_s3(q2, q1);
+        Q4 qm = plus_s3(q1, e.s * qd);
+        M3 R = qmat(qm);
+        M3 Rl = (-1.0) * (R * skew(e.cp_local));
+        M3 gam_inv = inv_right_jac(qd);
+        M3 gam = right_jac(e.s * qd);
+        M3 dR;
+        double sc;
+        if (local == 3) {
+            dR = exp_so3(e.s * qd).T() - e.s * (gam * gam_inv.T());
+            sc = 1 - e.s;
+        } else if (local == 4) {
+            dR = e.s * (gam * gam_inv);
+            sc = e.s;
+        } else {
+            throw std::runtime_error("TriangleRigidCollisionEnergySolver::constraintGradientHessian local_idx out of bounds!");
+        }
+        M3 M = Rl * dR;
+        for (int i = 0; i < 3; i++) gn[i] = sc * e.n[i];
+        for (int j = 0; j < 3; j++) gn[3 + j] = -(e.n.x * M.a[0][j] + e.n.y * M.a[1][j] + e.n.z * M.a[2][j]);
+        contact_accumulate<6>(e, Cn, Ct, Cb, gn, gt, gb, nullptr, nullptr, nullptr, (double(*)[6])H, G);
+    } else {
+        if (local >= 3) throw std::runtime_error("TriangleRigidCollisionEnergySolver::constraintGradientHessian local_idx out of bounds!");
+        double br = e.barys[local];
+        for (int i = 0; i < 3; i++) { gn[i] = -br * e.n[i]; gt[i] = -br * e.t[i]; gb[i] = -br * e.b[i]; }
+        contact_accumulate<DOF>(e, Cn, Ct, Cb, gn, gt, gb, nullptr, nullptr, nullptr, H, G);
+    }
+}
+
 // OneSidedFixedJointConstraintSolver::evaluateConstraint
 // (energy/joint/OneSidedFixedJointEnergySolver.hpp:16-34)
 static void joint_eval(const Ctx& c, const Joint& e, double C[6]) {
@@ -793,10 +885,14 @@ static void accumulate_block(const Ctx& c, unsigned p, double H[DOF][DOF], doubl
                 break;
         }
     }
-    // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid contacts in slot order
+    // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid, then
+    // triangle-rod contacts, each in slot order
     if (!c.dyn_off.empty())
-        for (unsigned k = c.dyn_off[p]; k < c.dyn_off[p + 1]; k++)
-            trc_accumulate<DOF>(c, c.trc[c.dyn_ent[k].first], c.dyn_ent[k].second, H, G);
+        for (unsigned k = c.dyn_off[p]; k < c.dyn_off[p + 1]; k++) {
+            const DynEnt& en = c.dyn_ent[k];
+            if (en.type == DYN_TRI_RIGID) trc_accumulate<DOF>(c, c.trc[en.slot], en.local, H, G);
+            else trd_accumulate<DOF>(c, c.trd[en.slot], en.local, H, G);
+        }
 }
 
 // VBDSolver::_solveParticle<DOF> assembly and solve (simulation/VBDSolver.hpp:449-510)
@@ -974,11 +1070,17 @@ static void after_time_step(Ctx& c) {
         contact_after_step(e, Cn);
     }
     // TriangleRigidCollisionEnergySolver::updateAfterTimeStep over the live slots
-    for (unsigned i = 0; i < c.trc.size(); i++) {
-        if (!c.trc_active[i]) continue;
+    for (unsigned i = 0; i < c.trc_pool.size(); i++) {
+        if (!c.trc_pool.active[i]) continue;
         double Cn, Ct, Cb;
         trc_eval(c, c.trc[i], Cn, Ct, Cb);
         contact_after_step(c.trc[i], Cn);
+    }
+    for (unsigned i = 0; i < c.trd_pool.size(); i++) {
+        if (!c.trd_pool.active[i]) continue;
+        double Cn, Ct, Cb;
+        trd_eval(c, c.trd[i], Cn, Ct, Cb);
+        contact_after_step(c.trd[i], Cn);
     }
     for (auto& e : c.joints) joint_after_step(c, e, c.joint_k_start);
 }
@@ -1000,11 +1102,17 @@ static void after_iteration(Ctx& c) {
         rground_eval(c, e, Cn, Ct, Cb);
         contact_after_iter(e, Cn, Ct, Cb);
     }
-    for (unsigned i = 0; i < c.trc.size(); i++) {
-        if (!c.trc_active[i] || !scene_on(c, c.trc[i].p[3])) continue;
+    for (unsigned i = 0; i < c.trc_pool.size(); i++) {
+        if (!c.trc_pool.active[i] || !scene_on(c, c.trc[i].p[3])) continue;
         double Cn, Ct, Cb;
         trc_eval(c, c.trc[i], Cn, Ct, Cb);
         contact_after_iter(c.trc[i], Cn, Ct, Cb);
+    }
+    for (unsigned i = 0; i < c.trd_pool.size(); i++) {
+        if (!c.trd_pool.active[i] || !scene_on(c, c.trd[i].p[3])) continue;
+        double Cn, Ct, Cb;
+        trd_eval(c, c.trd[i], Cn, Ct, Cb);
+        contact_after_iter(c.trd[i], Cn, Ct, Cb);
     }
     for (auto& e : c.joints)
         if (scene_on(c, e.p)) joint_after_iter(c, e);
@@ -1528,6 +1636,142 @@ static inline uint64_t collision_key(unsigned type, unsigned a, unsigned b, unsi
     return (k << 7) | (code & 127u);
 }
 
+// Math::closestPoint_PointTriangle (common/Math.hpp:446-500), Ericson's regions
+static V3 closest_point_triangle(V3 p, V3 a, V3 b, V3 c) {
+    V3 ab = b - a, ac = c - a, ap = p - a;
+    double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0 && d2 <= 0) return a;
+    V3 bp = p - b;
+    double d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0 && d4 <= d3) return b;
+    V3 cp = p - c;
+    double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0 && d5 <= d6) return c;
+    double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0 && d1 >= 0 && d3 <= 0) return a + (d1 / (d1 - d3)) * ab;
+    double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0) return a + (d2 / (d2 - d6)) * ac;
+    double va = d3 * d6 - d5 * d4;
+    if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) return b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b);
+    double den = 1.0 / (va + vb + vc);
+    double v = vb * den, w = vc * den;
+    return a + v * ab + w * ac;
+}
+
+static inline double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }   // std::clamp
+
+// Math::closestPoint_SegmentSegment (common/Math.hpp:508-560), Ericson's
+// ClosestPtSegmentSegment: s on (p1, q1), t on (p2, q2)
+static void closest_segment_segment(V3 p1, V3 q1, V3 p2, V3 q2, double& s, double& t) {
+    V3 d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+    double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    const double EPS = 1e-8;
+    if (a <= EPS && e <= EPS) { s = t = 0.0; return; }
+    if (a <= EPS) {
+        s = 0.0;
+        t = clamp01(f / e);
+    } else {
+        double cc = dot(d1, r);
+        if (e <= EPS) {
+            t = 0.0;
+            s = clamp01(-cc / a);
+        } else {
+            double b = dot(d1, d2);
+            double den = a * e - b * b;
+            s = den != 0.0 ? clamp01((b * f - cc * e) / den) : 0.0;
+            t = (b * s + f) / e;
+            if (t < 0.0) { t = 0.0; s = clamp01(-cc / a); }
+            else if (t > 1.0) { t = 1.0; s = clamp01((b - cc) / a); }
+        }
+    }
+}
+
+// Math::pointInTriangle (common/Math.hpp:562-591)
+static bool point_in_triangle(V3 p, V3 a, V3 b, V3 c) {
+    V3 v0 = b - a, v1 = c - a, v2 = p - a;
+    double d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+    double den = d00 * d11 - d01 * d01;
+    if (std::fabs(den) < 1e-12) return false;
+    double v = (d11 * d20 - d01 * d21) / den;
+    double w = (d00 * d21 - d01 * d20) / den;
+    double u = 1.0 - v - w;
+    const double EPS = 1e-8;
+    return u >= -EPS && v >= -EPS && w >= -EPS;
+}
+
+// Math::closestPoint_SegmentTriangle (common/Math.hpp:593-681): the segment's
+// crossing of the triangle, else the closest of the three edge tests and the
+// two end points.  The edge test measures its distance to (1-s) q0 + s q1,
+// the edge point at the SEGMENT's parameter, as the reference does.
+static void closest_segment_triangle(V3 p0, V3 p1, V3 a, V3 b, V3 c, double& s_out, V3& bary, double& dist) {
+    const double EPS = 1e-8;
+    V3 dir = p1 - p0;
+    V3 nrm = cross(b - a, c - a);
+    s_out = 0.0;
+    bary = V3(1, 0, 0);
+    dist = std::numeric_limits<double>::max();
+    if (sqnorm(nrm) > EPS) {
+        double den = dot(nrm, dir);
+        if (std::fabs(den) > EPS) {
+            double s = dot(nrm, a - p0) / den;
+            if (s >= 0.0 && s <= 1.0) {
+                V3 p = p0 + s * dir;
+                if (point_in_triangle(p, a, b, c)) {
+                    s_out = s;
+                    bary = barycentric(p, a, b, c);
+                    dist = 0.0;
+                    return;
+                }
+            }
+        }
+    }
+    auto edge = [&](V3 q0, V3 q1, int i0, int i1) {
+        double s, t;
+        closest_segment_segment(p0, p1, q0, q1, s, t);
+        V3 cp = (1 - s) * p0 + s * p1;
+        V3 cq = (1 - s) * q0 + s * q1;
+        double d2 = sqnorm(cp - cq);
+        if (d2 < dist * dist) {
+            s_out = s;
+            bary = V3(0, 0, 0);
+            bary[i0] = 1 - t;
+            bary[i1] = t;
+            dist = std::sqrt(d2);
+        }
+    };
+    edge(a, b, 0, 1);
+    edge(a, c, 0, 2);
+    edge(b, c, 1, 2);
+    V3 c0 = closest_point_triangle(p0, a, b, c);
+    double d0 = sqnorm(p0 - c0);
+    if (d0 < dist * dist) { s_out = 0.0; bary = barycentric(c0, a, b, c); dist = std::sqrt(d0); }
+    V3 c1 = closest_point_triangle(p1, a, b, c);
+    double d1 = sqnorm(p1 - c1);
+    if (d1 < dist * dist) { s_out = 1.0; bary = barycentric(c1, a, b, c); dist = std::sqrt(d1); }
+}
+
+// CollisionDetector::_triangleRod (collision/CollisionDetector.cpp:601-666):
+// contact when the centreline's distance to the triangle is below radius +
+// margin; the normal points from the centreline point to the triangle point,
+// the rod point is radius * normal in the frame interpolated at s.
+static bool tri_rod_contact(const Ctx& c, const Prim& T, const Prim& R, V3& normal, V3& barys, double& s,
+                            V3& cp_local) {
+    V3 v1 = c.x[T.idx[0]], v2 = c.x[T.idx[1]], v3 = c.x[T.idx[2]];
+    V3 s1 = c.x[R.idx[0]], s2 = c.x[R.idx[1]];
+    double dist;
+    closest_segment_triangle(s1, s2, v1, v2, v3, s, barys, dist);
+    if (!(dist < R.radius + c.margin)) return false;
+    V3 cl = (1 - s) * s1 + s * s2;
+    V3 ct = barys.x * v1 + barys.y * v2 + barys.z * v3;
+    V3 d = ct - cl;
+    double m = norm(d);
+    normal = m > 1e-8 ? d / m : V3(1, 0, 0);
+    Q4 q1 = c.q[c.rot[R.idx[0]]], q2 = c.q[c.rot[R.idx[1]]];
+    Q4 qm = plus_s3(q1, s * minus_s3(q2, q1));
+    cp_local = qrot_inv(qm, R.radius * normal);
+    return true;
+}
+
 // CollisionDetector::_narrowPhaseCollisionDetection + _processPotentialCollision
 // (collision/CollisionDetector.cpp:132-215) for the pairs this engine
 // supports: same-object primitives sharing a vertex are skipped,
@@ -1556,8 +1800,18 @@ static void narrow_phase(Ctx& c) {
             Ctx::Detected d;
             if (tri_sphere_ccd(c, P, Q, d.normal, d.barys, d.cp_local)) {
                 d.key = collision_key(2, ia, ib, 0);
+                d.type = 2;
                 d.tri[0] = P.idx[0]; d.tri[1] = P.idx[1]; d.tri[2] = P.idx[2];
                 d.rb = Q.idx[0];
+                c.detected.push_back(d);
+            }
+        } else if (P.type == 0 && Q.type == 1) {
+            Ctx::Detected d;
+            if (tri_rod_contact(c, P, Q, d.normal, d.barys, d.s, d.cp_local)) {
+                d.key = collision_key(3, ia, ib, 0);   // DetectedCollisionType::TriangleRod
+                d.type = 3;
+                d.tri[0] = P.idx[0]; d.tri[1] = P.idx[1]; d.tri[2] = P.idx[2];
+                d.rod[0] = Q.idx[0]; d.rod[1] = Q.idx[1];
                 c.detected.push_back(d);
             }
         }
@@ -1608,30 +1862,6 @@ static void update_frame(Contact& e, V3 nn) {
     e.lam_b = dot(f, e.b);
 }
 
-// TombstonePool::allocSlot / freeSlot (common/TombstonePool.hpp:56-103).  The
-// stack grows on demand; a slot never reached holds its own index, as the
-// reference's iota-initialised stack does.  freeSlot's lowering of
-// highest_index runs while the freed slot is still active, so it never
-// lowers; the live slots are always a subset of [0, size).
-static unsigned trc_alloc(Ctx& c) {
-    if (c.trc_top == c.trc_slots.size()) c.trc_slots.push_back((unsigned)c.trc_slots.size());
-    unsigned slot = c.trc_slots[c.trc_top++];
-    if (slot >= c.trc.size()) {
-        c.trc.resize(slot + 1);
-        c.trc_active.resize(slot + 1, 0);
-    }
-    c.trc_active[slot] = 1;
-    c.trc_count++;
-    c.trc_high = std::max(c.trc_high, slot);
-    return slot;
-}
-static void trc_free(Ctx& c, unsigned slot) {
-    if (slot >= c.trc_active.size() || !c.trc_active[slot]) throw std::runtime_error("freeSlot called on inactive slot");
-    c.trc_active[slot] = 0;
-    c.trc_count--;
-    c.trc_slots[--c.trc_top] = slot;
-}
-
 // ColorList::markParticleDirty (common/ColorList.hpp:365-378)
 static void mark_dirty(Ctx& c, unsigned p) {
     if (c.last_dirty[p] != 0) {
@@ -1647,7 +1877,8 @@ static void add_contact(Ctx& c, Ctx::Detected& d) {
     double ks = mn / (c.dt * c.dt);
     V3 t, b;
     normal_basis(d.normal, t, b);
-    unsigned slot = trc_alloc(c);
+    unsigned slot = c.trc_pool.alloc();
+    if (slot >= c.trc.size()) c.trc.resize(slot + 1);
     TriRigid& e = c.trc[slot];
     e = TriRigid{};
     // CollisionConstraintEnergyPool::addEnergy (energy/collision/CollisionConstraintEnergyPool.hpp:48-69)
@@ -1665,12 +1896,57 @@ static void add_contact(Ctx& c, Ctx::Detected& d) {
     mark_dirty(c, d.rb);
 }
 
-// CollisionDetector::_updateCollision, TriangleRigid case (collision/CollisionDetector.cpp:474-481)
-static void update_contact(Ctx& c, const Ctx::Detected& d) {
-    TriRigid& e = c.trc[d.e_idx];
-    e.cp_local = d.cp_local;
+// CollisionDetector::_addCollision, TriangleRod case (collision/CollisionDetector.cpp:379-418)
+static void add_rod_contact(Ctx& c, Ctx::Detected& d) {
+    double mn = std::min({c.m[d.tri[0]], c.m[d.tri[1]], c.m[d.tri[2]], c.m[d.rod[0]], c.m[d.rod[1]]});
+    double ks = mn / (c.dt * c.dt);
+    V3 t, b;
+    normal_basis(d.normal, t, b);
+    unsigned slot = c.trd_pool.alloc();
+    if (slot >= c.trd.size()) c.trd.resize(slot + 1);
+    TriRod& e = c.trd[slot];
+    e = TriRod{};
+    e.lam_n = e.lam_t = e.lam_b = 0;
+    e.k_start = e.k_n = e.k_t = e.k_b = ks;
+    e.cn_prev = 0;
+    e.mu_s = 0.4; e.mu_k = 0.2;
+    e.use_static = false; e.unclamped = false;
+    for (int k = 0; k < 3; k++) e.p[k] = d.tri[k];
+    e.p[3] = d.rod[0]; e.p[4] = d.rod[1];
+    e.n = d.normal; e.t = t; e.b = b;
     e.barys = d.barys;
-    update_frame(e, d.normal);
+    e.s = d.s;
+    e.cp_local = d.cp_local;
+    d.e_idx = slot;
+    for (int k = 0; k < 3; k++) mark_dirty(c, d.tri[k]);
+    mark_dirty(c, d.rod[0]);
+    mark_dirty(c, d.rod[1]);
+}
+
+// CollisionDetector::_updateCollision (collision/CollisionDetector.cpp:460-491)
+static void update_contact(Ctx& c, const Ctx::Detected& d) {
+    if (d.type == 2) {
+        TriRigid& e = c.trc[d.e_idx];
+        e.cp_local = d.cp_local;
+        e.barys = d.barys;
+        update_frame(e, d.normal);
+    } else {
+        TriRod& e = c.trd[d.e_idx];
+        e.s = d.s;
+        e.cp_local = d.cp_local;
+        e.barys = d.barys;
+        update_frame(e, d.normal);
+    }
+}
+
+static void add_any(Ctx& c, Ctx::Detected& d) {
+    if (d.type == 2) add_contact(c, d);
+    else add_rod_contact(c, d);
+}
+// CollisionDetector::_removeCollision (collision/CollisionDetector.cpp:421-458)
+static void remove_any(Ctx& c, const Ctx::Detected& d) {
+    if (d.type == 2) c.trc_pool.free(d.e_idx);
+    else c.trd_pool.free(d.e_idx);
 }
 
 // CollisionDetector::_handleDetectedCollisions (collision/CollisionDetector.cpp:265-318):
@@ -1683,9 +1959,9 @@ static void handle_detections(Ctx& c) {
     size_t i = 0, j = 0;
     while (i < cur.size() && j < prev.size()) {
         if (cur[i].key < prev[j].key) {
-            add_contact(c, cur[i++]);
+            add_any(c, cur[i++]);
         } else if (cur[i].key > prev[j].key) {
-            trc_free(c, prev[j++].e_idx);
+            remove_any(c, prev[j++]);
         } else {
             cur[i].e_idx = prev[j].e_idx;
             update_contact(c, cur[i]);
@@ -1693,34 +1969,40 @@ static void handle_detections(Ctx& c) {
             j++;
         }
     }
-    for (; i < cur.size(); i++) add_contact(c, cur[i]);
-    for (; j < prev.size(); j++) trc_free(c, prev[j].e_idx);
+    for (; i < cur.size(); i++) add_any(c, cur[i]);
+    for (; j < prev.size(); j++) remove_any(c, prev[j]);
 }
 
 // DynamicParticleAdjacency::buildAdjacency (common/DynamicParticleAdjacency.hpp:33-118):
-// per particle its contact entries in slot order; neighbours with repeats
+// per particle its contact entries, triangle-rigid then triangle-rod, each in
+// slot order; neighbours with repeats
 static void build_dynamic_adjacency(Ctx& c) {
     const unsigned n = c.np();
     c.dyn_off.assign(n + 1, 0);
     c.dnb_off.assign(n + 1, 0);
-    for (unsigned s = 0; s < c.trc.size(); s++) {
-        if (!c.trc_active[s]) continue;
-        for (int k = 0; k < 4; k++) { c.dyn_off[c.trc[s].p[k] + 1]++; c.dnb_off[c.trc[s].p[k] + 1] += 3; }
-    }
+    auto count = [&](const unsigned* ps, int np_) {
+        for (int k = 0; k < np_; k++) { c.dyn_off[ps[k] + 1]++; c.dnb_off[ps[k] + 1] += np_ - 1; }
+    };
+    for (unsigned s = 0; s < c.trc_pool.size(); s++)
+        if (c.trc_pool.active[s]) count(c.trc[s].p, 4);
+    for (unsigned s = 0; s < c.trd_pool.size(); s++)
+        if (c.trd_pool.active[s]) count(c.trd[s].p, 5);
     for (unsigned p = 0; p < n; p++) { c.dyn_off[p + 1] += c.dyn_off[p]; c.dnb_off[p + 1] += c.dnb_off[p]; }
-    c.dyn_ent.assign(c.dyn_off[n], {0u, (uint16_t)0});
+    c.dyn_ent.assign(c.dyn_off[n], DynEnt{0, 0u, (uint16_t)0});
     c.dnb.assign(c.dnb_off[n], 0);
     std::vector<unsigned> ec(c.dyn_off.begin(), c.dyn_off.end() - 1), nc(c.dnb_off.begin(), c.dnb_off.end() - 1);
-    for (unsigned s = 0; s < c.trc.size(); s++) {
-        if (!c.trc_active[s]) continue;
-        const TriRigid& e = c.trc[s];
-        for (int k = 0; k < 4; k++) {
-            unsigned p = e.p[k];
-            c.dyn_ent[ec[p]++] = {s, (uint16_t)k};
-            for (int k2 = 0; k2 < 4; k2++)
-                if (k2 != k) c.dnb[nc[p]++] = e.p[k2];
+    auto scatter = [&](uint8_t type, unsigned slot, const unsigned* ps, int np_) {
+        for (int k = 0; k < np_; k++) {
+            unsigned p = ps[k];
+            c.dyn_ent[ec[p]++] = DynEnt{type, slot, (uint16_t)k};
+            for (int k2 = 0; k2 < np_; k2++)
+                if (k2 != k) c.dnb[nc[p]++] = ps[k2];
         }
-    }
+    };
+    for (unsigned s = 0; s < c.trc_pool.size(); s++)
+        if (c.trc_pool.active[s]) scatter(DYN_TRI_RIGID, s, c.trc[s].p, 4);
+    for (unsigned s = 0; s < c.trd_pool.size(); s++)
+        if (c.trd_pool.active[s]) scatter(DYN_TRI_ROD, s, c.trd[s].p, 5);
 }
 
 // ForEachNeighbor (common/ColorList.hpp:41-60): static, then dynamic neighbours
@@ -2066,6 +2348,9 @@ unsigned orc_add_spheres(void* h, unsigned n, const unsigned* p, const double* r
 int orc_finalize(void* h, int reference_dsatur) {
     Ctx& c = *(Ctx*)h;
     ORC_TRY({
+        for (const Prim& pr : c.prims)
+            if (pr.type == 1 && (!c.oriented(pr.idx[0]) || !c.oriented(pr.idx[1])))
+                throw std::runtime_error("rod segment primitive on a positional particle");
         build_adjacency(c);
         if (reference_dsatur) dsatur_reference(c); else dsatur_fast(c);
         if (c.num_colors > 256) throw std::runtime_error("Ran out of colors!");
@@ -2123,8 +2408,11 @@ unsigned orc_num_pairs(void* h) { return (unsigned)((Ctx*)h)->pairs.size(); }
 // normal[3], barys[3], cp_local[3] (ascending key)
 unsigned orc_get_contacts(void* h, uint64_t* keys, unsigned* idx4, double* vec9) {
     Ctx& c = *(Ctx*)h;
-    for (size_t k = 0; k < c.detected.size(); k++) {
-        const auto& d = c.detected[k];
+    std::vector<Ctx::Detected> sph;
+    for (const auto& d : c.detected)
+        if (d.type == 2) sph.push_back(d);
+    for (size_t k = 0; k < sph.size(); k++) {
+        const auto& d = sph[k];
         if (keys) keys[k] = d.key;
         if (idx4) { idx4[4 * k] = d.tri[0]; idx4[4 * k + 1] = d.tri[1]; idx4[4 * k + 2] = d.tri[2]; idx4[4 * k + 3] = d.rb; }
         if (vec9) {
@@ -2135,20 +2423,70 @@ unsigned orc_get_contacts(void* h, uint64_t* keys, unsigned* idx4, double* vec9)
             }
         }
     }
-    return (unsigned)c.detected.size();
+    return (unsigned)sph.size();
 }
 
-// Dynamic contact state: [0] live contacts, [1] pool size (highest slot + 1),
-// [2] colors, [3] conflicted particles, [4] particles still dirty,
-// [5] dynamic adjacency entries
+// triangle-rod contacts of the last collision stage: key, tri[3] + rod[2],
+// normal[3], barys[3], cp_local[3], s (ascending key)
+unsigned orc_get_rod_contacts(void* h, uint64_t* keys, unsigned* idx5, double* vec10) {
+    Ctx& c = *(Ctx*)h;
+    unsigned k = 0;
+    for (const auto& d : c.detected) {
+        if (d.type != 3) continue;
+        if (keys) keys[k] = d.key;
+        if (idx5) {
+            for (int i = 0; i < 3; i++) idx5[5 * k + i] = d.tri[i];
+            idx5[5 * k + 3] = d.rod[0];
+            idx5[5 * k + 4] = d.rod[1];
+        }
+        if (vec10) {
+            for (int i = 0; i < 3; i++) {
+                vec10[10 * k + i] = d.normal[i];
+                vec10[10 * k + 3 + i] = d.barys[i];
+                vec10[10 * k + 6 + i] = d.cp_local[i];
+            }
+            vec10[10 * k + 9] = d.s;
+        }
+        k++;
+    }
+    return k;
+}
+
+// Dynamic contact state: [0] live triangle-rigid contacts, [1] their pool
+// size (highest slot + 1), [2] colors, [3] conflicted particles, [4]
+// particles still dirty, [5] dynamic adjacency entries, [6] live
+// triangle-rod contacts, [7] their pool size
 void orc_dynamic_info(void* h, unsigned* out) {
     Ctx& c = *(Ctx*)h;
-    out[0] = c.trc_count;
-    out[1] = (unsigned)c.trc.size();
+    out[0] = c.trc_pool.count;
+    out[1] = c.trc_pool.size();
     out[2] = c.num_colors;
     out[3] = (unsigned)c.touched_conflicted.size();
     out[4] = (unsigned)c.dirty.size();
     out[5] = (unsigned)c.dyn_ent.size();
+    out[6] = c.trd_pool.count;
+    out[7] = c.trd_pool.size();
+}
+
+// Triangle-rod pool slots [0, pool size): particles (5 per slot), active flag,
+// and 25 doubles per slot: n, t, b, barys, cp_local, s, k_start, k_n, k_t,
+// k_b, lam_n, lam_t, lam_b, C_n_prev, use_static + 2 unclamped
+void orc_get_trd(void* h, unsigned* p5, uint8_t* active, double* data) {
+    Ctx& c = *(Ctx*)h;
+    for (size_t s = 0; s < c.trd_pool.size(); s++) {
+        const TriRod& e = c.trd[s];
+        if (p5) for (int k = 0; k < 5; k++) p5[5 * s + k] = e.p[k];
+        if (active) active[s] = c.trd_pool.active[s];
+        if (data) {
+            double* d = data + 25 * s;
+            const V3 v[5] = {e.n, e.t, e.b, e.barys, e.cp_local};
+            for (int i = 0; i < 5; i++) for (int j = 0; j < 3; j++) d[3 * i + j] = v[i][j];
+            d[15] = e.s;
+            d[16] = e.k_start; d[17] = e.k_n; d[18] = e.k_t; d[19] = e.k_b;
+            d[20] = e.lam_n; d[21] = e.lam_t; d[22] = e.lam_b; d[23] = e.cn_prev;
+            d[24] = (e.use_static ? 1 : 0) + (e.unclamped ? 2 : 0);
+        }
+    }
 }
 
 // Contact pool slots [0, pool size): particles (4 per slot), active flag, and
@@ -2156,10 +2494,10 @@ void orc_dynamic_info(void* h, unsigned* out) {
 // lam_n, lam_t, lam_b, C_n_prev, use_static + 2 unclamped
 void orc_get_trc(void* h, unsigned* p4, uint8_t* active, double* data) {
     Ctx& c = *(Ctx*)h;
-    for (size_t s = 0; s < c.trc.size(); s++) {
+    for (size_t s = 0; s < c.trc_pool.size(); s++) {
         const TriRigid& e = c.trc[s];
         if (p4) for (int k = 0; k < 4; k++) p4[4 * s + k] = e.p[k];
-        if (active) active[s] = c.trc_active[s];
+        if (active) active[s] = c.trc_pool.active[s];
         if (data) {
             double* d = data + 24 * s;
             const V3 v[5] = {e.n, e.t, e.b, e.barys, e.cp_local};

@@ -67,6 +67,8 @@ def lib():
             "orc_get_angular_velocities": (None, [vp, dp]),
             "orc_dynamic_info": (None, [vp, up]),
             "orc_get_trc": (None, [vp, up, u8p, dp]),
+            "orc_get_trd": (None, [vp, up, u8p, dp]),
+            "orc_get_rod_contacts": (C.c_uint, [vp, C.POINTER(C.c_uint64), up, dp]),
             "orc_get_conflicted": (None, [vp, u8p]),
             "orc_set_recolor_rounds": (None, [vp, C.c_uint]),
             "orc_num_particles": (C.c_uint, [vp]),
@@ -296,9 +298,10 @@ class Oracle:
     def dynamic_info(self):
         """Contact pool and recoloring state: live contacts, pool size, colors,
         conflicted particles, particles still dirty, dynamic adjacency entries."""
-        out = np.zeros(6, dtype=np.uint32)
+        out = np.zeros(8, dtype=np.uint32)
         self.L.orc_dynamic_info(self.h, _p(out, C.c_uint))
-        return dict(zip(["live", "pool_size", "colors", "conflicted", "dirty", "entries"], (int(v) for v in out)))
+        return dict(zip(["live", "pool_size", "colors", "conflicted", "dirty", "entries", "rod_live", "rod_pool_size"],
+                        (int(v) for v in out)))
 
     def contact_pool(self):
         """Triangle-rigid contact pool by slot: particles [s, 4], active [s],
@@ -317,6 +320,32 @@ class Oracle:
 
     def set_recolor_rounds(self, rounds):
         self.L.orc_set_recolor_rounds(self.h, rounds)
+
+    def rod_contact_pool(self):
+        """Triangle-rod contact pool by slot: particles [s, 5], active [s], and
+        per slot n, t, b, barys, cp_local [s, 3], s [s], k [s, 4], lam [s, 4],
+        flags [s]."""
+        n = self.dynamic_info()["rod_pool_size"]
+        p5 = np.zeros((n, 5), dtype=np.uint32)
+        act = np.zeros(n, dtype=np.uint8)
+        d = np.zeros((n, 25))
+        if n:
+            self.L.orc_get_trd(self.h, _p(p5, C.c_uint), _p(act, C.c_uint8), _p(d, C.c_double))
+        return {"particles": p5, "active": act.astype(bool), "n": d[:, 0:3], "t": d[:, 3:6], "b": d[:, 6:9],
+                "barys": d[:, 9:12], "cp_local": d[:, 12:15], "s": d[:, 15], "k": d[:, 16:20], "lam": d[:, 20:24],
+                "flags": d[:, 24].astype(np.uint8)}
+
+    def rod_contacts(self):
+        """Triangle-rod contacts of the last collision stage, ascending key:
+        key [k], tri [k, 3], rod [k, 2], normal / barys / cp_local [k, 3], s [k]."""
+        n = self.L.orc_get_rod_contacts(self.h, None, None, None)
+        keys = np.zeros(n, dtype=np.uint64)
+        idx = np.zeros((n, 5), dtype=np.uint32)
+        vec = np.zeros((n, 10))
+        if n:
+            self.L.orc_get_rod_contacts(self.h, _p(keys, C.c_uint64), _p(idx, C.c_uint), _p(vec, C.c_double))
+        return {"key": keys, "tri": idx[:, :3], "rod": idx[:, 3:5], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
+                "cp_local": vec[:, 6:9], "s": vec[:, 9]}
 
     def conflicted(self):
         out = np.zeros(self.num_particles, dtype=np.uint8)
