@@ -85,6 +85,8 @@ static void free_device(avbd_ctx* c) {
     c->d_scene_mg2 = nullptr;
     c->d_scene_iters = nullptr;
     c->d_tol_count = nullptr;
+    c->d_solve_ranges = nullptr;
+    c->solve_range_off.clear();
     mlp_device_free(c->ws_mlp);
     c->ws_mlp = nullptr;
     c->d_ws_feat = c->d_ws_x0 = nullptr;
@@ -896,6 +898,39 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
             (rc = dalloc(c, &c->d_scene_iters, S)) || (rc = dalloc(c, &c->d_tol_count, 1)))
             return rc;
         CUDA_OR_FAIL(cudaMemcpyAsync(c->d_scene, sid.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
+        // the solved part of each color slab is ordered scene by scene
+        std::vector<uint4> ranges;
+        for (unsigned k = 0; k < nc; k++) {
+            unsigned b = c->color_begin[k];
+            const unsigned e = b + c->color_solve[k];
+            while (b < e) {
+                unsigned q = b;
+                while (q < e && sid[q] == sid[b]) q++;
+                ranges.push_back(make_uint4(b, q - b, sid[b], 0));
+                b = q;
+            }
+        }
+        // pieces of at most solve_chunk vertices for the sweeps (AVBD_SOLVE_CHUNK
+        // overrides; 0 launches whole slabs)
+        if (const char* env = getenv("AVBD_SOLVE_CHUNK")) c->solve_chunk = (unsigned)atoi(env);
+        c->solve_range_off.assign(nc + 1, 0);
+        std::vector<uint4> pieces;
+        if (c->solve_chunk) {
+            unsigned r = 0;
+            for (unsigned k = 0; k < nc; k++) {
+                c->solve_range_off[k] = (unsigned)pieces.size();
+                for (; r < ranges.size() && ranges[r].x < c->color_begin[k] + c->color_solve[k]; r++)
+                    for (unsigned o = 0; o < ranges[r].y; o += c->solve_chunk)
+                        pieces.push_back(make_uint4(ranges[r].x + o, std::min(c->solve_chunk, ranges[r].y - o),
+                                                    ranges[r].z, 0));
+            }
+            c->solve_range_off[nc] = (unsigned)pieces.size();
+        }
+        if (!pieces.empty()) {
+            if ((rc = dalloc(c, &c->d_solve_ranges, pieces.size()))) return rc;
+            CUDA_OR_FAIL(cudaMemcpyAsync(c->d_solve_ranges, pieces.data(), sizeof(uint4) * pieces.size(),
+                                         cudaMemcpyHostToDevice, c->stream));
+        }
         CUDA_OR_FAIL(cudaMemcpyAsync(c->d_scene_mg2, mg2.data(), sizeof(double) * S, cudaMemcpyHostToDevice, c->stream));
         CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
     }
@@ -961,7 +996,10 @@ void enqueue_sweep(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_
         return;
     }
     for (unsigned col = 0; col < c->num_colors; col++) {
-        if (c->color_solve[col])
+        if (c->color_solve[col] && T.active && c->d_solve_ranges) {  // run-to-tolerance: per-scene pieces
+            const unsigned r0 = c->solve_range_off[col], r1 = c->solve_range_off[col + 1];
+            launch_solve_color<R>(c, s, k, 0, 0, st, T, nullptr, c->d_solve_ranges + r0, r1 - r0);
+        } else if (c->color_solve[col])
             launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st, T);
         if (c->color_orient[col])
             launch_solve_rod<R>(c, s, k, c->color_begin[col] + c->color_solve[col], c->color_orient[col], st, T, 0,

@@ -257,6 +257,13 @@ struct avbd_ctx {
     double* d_scene_mg2 = nullptr;
     uint32_t* d_scene_iters = nullptr;
     int* d_tol_count = nullptr;
+    // (first internal vertex, count, scene) pieces of at most solve_chunk
+    // vertices of each scene's solved vertices in each color slab, color by
+    // color (offsets solve_range_off): the sweeps and the residual pass of
+    // run-to-tolerance steps launch one block per piece
+    uint4* d_solve_ranges = nullptr;
+    std::vector<unsigned> solve_range_off;
+    unsigned solve_chunk = 512;
     unsigned long long host_iterations = 0;  // scene-iterations of fixed-iteration steps
 
     // CUDA graph of one full step (fixed-iteration mode)
@@ -332,9 +339,11 @@ template <typename R>
 void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
 // list: when given, the count vertices of list (internal ids) instead of the
 // slab [begin, begin + count)
+// ranges: when given, (first vertex, count, scene) pieces of the slab, one block each
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, const SceneTol& T = SceneTol(), const uint32_t* list = nullptr);
+                        cudaStream_t st, const SceneTol& T = SceneTol(), const uint32_t* list = nullptr,
+                        const uint4* ranges = nullptr, unsigned nranges = 0);
 template <typename R>
 void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
                            const SceneTol& T = SceneTol());

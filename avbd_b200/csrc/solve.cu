@@ -299,13 +299,10 @@ struct SolveMinBlocks {
 // color changed by the recoloring, launched over per-color lists; the slab
 // launches (DYN false) skip those vertices and carry no dynamic code.
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
-__global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
-                                                   unsigned begin, unsigned count, Consts<P> c,
-                                                   unsigned long long* counters, double* out, SceneTol T,
-                                                   const float4* __restrict__ aux, const uint32_t* __restrict__ list) {
-    unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned gi = tid / LANES;
-    unsigned lane = tid % LANES;
+__device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS>* __restrict__ inc, unsigned begin,
+                                           unsigned count, unsigned gi, unsigned lane, const Consts<P>& c,
+                                           unsigned long long* counters, double* out, const SceneTol& T,
+                                           const float4* __restrict__ aux, const uint32_t* __restrict__ list) {
     bool active = gi < count;
     unsigned p = list ? (active ? list[gi] : 0u) : begin + (active ? gi : 0);
     uint8_t fl = active ? s.flags[p] : 0;
@@ -483,6 +480,33 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
     }
 }
 
+// ranges: when given, block b serves the vertices [x, x + y) of scene z
+// (a piece of one scene's part of a color slab) and returns at once when the
+// scene is not iterating (solve) or not a residual candidate (residual):
+// with per-scene run-to-tolerance most scenes drop out of the later
+// iterations, and a block of them then costs one check.  Otherwise thread
+// groups map to vertices [begin, begin + count) (or to list).
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
+__global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
+                                                   unsigned begin, unsigned count, Consts<P> c,
+                                                   unsigned long long* counters, double* out, SceneTol T,
+                                                   const float4* __restrict__ aux, const uint32_t* __restrict__ list,
+                                                   const uint4* __restrict__ ranges) {
+    const unsigned lane = threadIdx.x % LANES;
+    if (ranges) {
+        const uint4 rg = ranges[blockIdx.x];
+        const uint8_t* gate = MODE == MODE_SOLVE ? T.active : T.cand;
+        if (gate && !gate[rg.z]) return;
+        for (unsigned base = 0; base < rg.y; base += blockDim.x / LANES)
+            tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, rg.x, rg.y, base + threadIdx.x / LANES, lane,
+                                                                  c, counters, out, T, aux, list);
+        return;
+    }
+    const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+    tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, begin, count, tid / LANES, lane, c, counters, out, T,
+                                                          aux, list);
+}
+
 // Chebyshev acceleration of every particle fused with the ground-contact dual
 // update that follows it (CollisionConstraintEnergySolver::updateAfterIteration);
 // a ground energy reads only its own particle, so the fusion is exact.
@@ -607,22 +631,23 @@ void launch_tet_eprev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStre
 
 template <typename P, typename RS, typename HT, int LANES, int MODE, bool DYN = false>
 static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
-                           unsigned count, cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list) {
+                           unsigned count, cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list,
+                           const uint4* ranges = nullptr, unsigned nranges = 0) {
     unsigned threads = count * LANES;
-    unsigned blocks = nblocks(threads, 256);
+    unsigned blocks = ranges ? nranges : nblocks(threads, 256);
     if (blocks == 0) return;
     bool damp = c->damping, ground = !c->ground.empty();
     auto kc = mkc<P>(k);
     auto* ctr = c->d_counters;
     const float4* aux = reinterpret_cast<const float4*>(c->ws_prev_arg);
     if (damp && ground)
-        k_solve_tet<P, RS, HT, LANES, true, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
+        k_solve_tet<P, RS, HT, LANES, true, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list, ranges);
     else if (damp)
-        k_solve_tet<P, RS, HT, LANES, true, false, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
+        k_solve_tet<P, RS, HT, LANES, true, false, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list, ranges);
     else if (ground)
-        k_solve_tet<P, RS, HT, LANES, false, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
+        k_solve_tet<P, RS, HT, LANES, false, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list, ranges);
     else
-        k_solve_tet<P, RS, HT, LANES, false, false, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list);
+        k_solve_tet<P, RS, HT, LANES, false, false, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list, ranges);
     count_launch(c);
 }
 
@@ -632,7 +657,29 @@ static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, c
 // uses 8.
 template <typename P, typename RS, typename HT, int MODE>
 static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k, unsigned begin,
-                          unsigned count, cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list) {
+                          unsigned count, cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list,
+                          const uint4* ranges = nullptr, unsigned nranges = 0) {
+    if constexpr (MODE == MODE_RESIDUAL) {  // tolerance residual: the sweeps' per-scene pieces, all colors
+        if (!list && T.cand && T.ex && c->d_solve_ranges) {
+            ranges = c->d_solve_ranges;
+            nranges = c->solve_range_off.back();
+        }
+    }
+    if constexpr (MODE == MODE_SOLVE || MODE == MODE_RESIDUAL) {
+        if (ranges) {
+            const uint4* rg = ranges;
+            const unsigned nr = nranges;
+            switch (c->lanes) {
+                case 1: solve_dispatch<P, RS, HT, 1, MODE>(c, s, inc, k, 0, 0, st, out, T, nullptr, rg, nr); break;
+                case 2: solve_dispatch<P, RS, HT, 2, MODE>(c, s, inc, k, 0, 0, st, out, T, nullptr, rg, nr); break;
+                case 4: solve_dispatch<P, RS, HT, 4, MODE>(c, s, inc, k, 0, 0, st, out, T, nullptr, rg, nr); break;
+                case 16: solve_dispatch<P, RS, HT, 16, MODE>(c, s, inc, k, 0, 0, st, out, T, nullptr, rg, nr); break;
+                case 32: solve_dispatch<P, RS, HT, 32, MODE>(c, s, inc, k, 0, 0, st, out, T, nullptr, rg, nr); break;
+                default: solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, 0, 0, st, out, T, nullptr, rg, nr); break;
+            }
+            return;
+        }
+    }
     if constexpr (MODE == MODE_DEBUG) {
         if (c->dyn) solve_dispatch<P, RS, HT, 8, MODE, true>(c, s, inc, k, begin, count, st, out, T, list);
         else solve_dispatch<P, RS, HT, 8, MODE>(c, s, inc, k, begin, count, st, out, T, list);
@@ -655,22 +702,25 @@ static void solve_lanes_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, co
 // state and gradient, float records and Hessian.
 template <int MODE>
 static void solve_lanes(avbd_ctx* c, DevState<float>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list = nullptr) {
-    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out, T, list);
+                        cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list = nullptr,
+                        const uint4* ranges = nullptr, unsigned nranges = 0) {
+    solve_lanes_t<float, float, float, MODE>(c, s, s.inc, k, begin, count, st, out, T, list, ranges, nranges);
 }
 template <int MODE>
 static void solve_lanes(avbd_ctx* c, DevState<double>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list = nullptr) {
+                        cudaStream_t st, double* out, const SceneTol& T, const uint32_t* list = nullptr,
+                        const uint4* ranges = nullptr, unsigned nranges = 0) {
     if (c->solver.precision == AVBD_PRECISION_MIXED)
-        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out, T, list);
+        solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out, T, list, ranges, nranges);
     else
-        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out, T, list);
+        solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out, T, list, ranges, nranges);
 }
 
 template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
-                        cudaStream_t st, const SceneTol& T, const uint32_t* list) {
-    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr, T, list);
+                        cudaStream_t st, const SceneTol& T, const uint32_t* list, const uint4* ranges,
+                        unsigned nranges) {
+    solve_lanes<MODE_SOLVE>(c, s, k, begin, count, st, nullptr, T, list, ranges, nranges);
 }
 
 template <typename R>
@@ -851,7 +901,7 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
     template void launch_begin_step<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);               \
     template void launch_tet_eprev<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                \
     template void launch_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,         \
-                                        cudaStream_t, const SceneTol&, const uint32_t*);                        \
+                                        cudaStream_t, const SceneTol&, const uint32_t*, const uint4*, unsigned); \
     template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t,    \
                                            const SceneTol&);                                                    \
     template void launch_velocity<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                 \
