@@ -1085,8 +1085,15 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
         c->lanes = l;
         for (int rep = 0; rep < 2; rep++) {  // rep 0 warms up, rep 1 is timed
             if (rep == 1) CUDA_OR_FAIL(cudaEventRecord(a, st));
-            for (unsigned col = 0; col < c->num_colors; col++)
-                if (c->color_solve[col]) launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st);
+            for (unsigned col = 0; col < c->num_colors; col++) {
+                if (!c->color_solve[col]) continue;
+                if (c->solver.residual_tolerance > 0 && c->d_solve_ranges) {  // the launches a step will use
+                    const unsigned r0 = c->solve_range_off[col], r1 = c->solve_range_off[col + 1];
+                    launch_solve_color<R>(c, s, k, 0, 0, st, SceneTol(), nullptr, c->d_solve_ranges + r0, r1 - r0);
+                } else {
+                    launch_solve_color<R>(c, s, k, c->color_begin[col], c->color_solve[col], st);
+                }
+            }
             if (rep == 1) CUDA_OR_FAIL(cudaEventRecord(b, st));
         }
         CUDA_OR_FAIL(cudaEventSynchronize(b));

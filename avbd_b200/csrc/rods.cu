@@ -21,6 +21,10 @@ namespace avbd {
 namespace {
 
 constexpr double JOINT_K_START = 1e4;  // OneSidedFixedJointEnergyPool.hpp:27
+// threads per block of the 6-DOF solve (one node each).  A color of the
+// 256-rod workload has ~13 K nodes; 32, 64 and 128 measured the same step
+// time there: each node's serial FP64 chain, not the SM spread, bounds it.
+constexpr int ROD_BLOCK = 128;
 
 template <typename R>
 struct Block6 {
@@ -374,7 +378,7 @@ __global__ void __launch_bounds__(256) k_begin_step_rot(DevState<R> s, R dt, R g
 enum { RMODE_SOLVE = 0, RMODE_RESIDUAL = 1, RMODE_DEBUG = 2 };
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128) k_solve_rod(DevState<R> s, unsigned begin, unsigned count, R dt, double g,
+__global__ void __launch_bounds__(ROD_BLOCK) k_solve_rod(DevState<R> s, unsigned begin, unsigned count, R dt, double g,
                                                    double* out, SceneTol T, const uint32_t* __restrict__ list) {
     unsigned gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= count) return;
@@ -544,11 +548,11 @@ void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned
                       cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list) {
     if (count == 0) return;
     if (mode == RMODE_RESIDUAL)
-        k_solve_rod<R, RMODE_RESIDUAL><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_RESIDUAL><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     else if (mode == RMODE_DEBUG)
-        k_solve_rod<R, RMODE_DEBUG><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_DEBUG><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     else
-        k_solve_rod<R, RMODE_SOLVE><<<nblk(count, 128), 128, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_SOLVE><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     count_launch(c);
 }
 
