@@ -8,7 +8,7 @@ every step runs AVBD iterations until the residual R <= 1e-4 (at most
 --max-iters).  One step of the batch counts as `scenes` scene-steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--workload batch_cubes|rods_spheres]
+                    [--workload batch_cubes|rods_spheres|contacts]
 
 The batched-cubes line times two arms on identically built contexts: plain
 AVBD (the adaptive inertial guess) and the learned warm start (the fused
@@ -20,6 +20,15 @@ latency of one batch step (CUDA events around every step).
 `--workload rods_spheres` measures the rod scene instead: 256 Cosserat rods
 of 100 segments hanging from one-sided fixed joints plus 64 rigid spheres,
 all with rigid-body ground contact, 20 iterations per step, FP32 (steps/s).
+
+`--workload contacts` measures the dynamic contacts: 24 Cosserat rods of 32
+segments dropped flat on a 32^3-cell tet cube (35,937 vertices, 196,608 tets,
+12,288 surface triangles) resting on the ground; every step runs the LBVH
+broad phase over triangles and rod segments, the triangle-rod narrow phase,
+the contact pool merge (up to ~3,900 live contacts), the incremental
+recoloring and the contact energies inside 20 iterations, FP32 (steps/s).
+(Spheres on such a cube drift into each other within tens of steps, and
+the reference throws on sphere-sphere candidates.)
 
 Prints one JSON line.  `value` is scene-steps/s over all ranks with the state
 resident in HBM; `e2e` repeats the measurement through the C-ABI with the
@@ -61,14 +70,14 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", default=None, choices=["fp32", "mixed", "fp64"],
-                   help="default: mixed for batch_cubes, fp32 for rods_spheres")
-    p.add_argument("--workload", default="batch_cubes", choices=["batch_cubes", "rods_spheres"])
+                   help="default: mixed for batch_cubes, fp32 for rods_spheres and contacts")
+    p.add_argument("--workload", default="batch_cubes", choices=["batch_cubes", "rods_spheres", "contacts"])
     p.add_argument("--warmstart", default="learned", choices=["learned", "none"],
                    help="batch_cubes: time the learned warm start beside plain AVBD (value = learned)")
     p.add_argument("--weights", default=os.path.join(ROOT, "avbd_b200", "data", "warmstart_mlp.npz"))
     a = p.parse_args()
     if a.precision is None:
-        a.precision = "fp32" if a.workload == "rods_spheres" else "mixed"
+        a.precision = "mixed" if a.workload == "batch_cubes" else "fp32"
     return a
 
 
@@ -78,6 +87,8 @@ class Workload:
     def __init__(self, args, seed):
         from avbd_b200 import scenes
         self.rods = args.workload == "rods_spheres"
+        self.contacts = args.workload == "contacts"
+        self.single = self.rods or self.contacts   # one scene, fixed iterations, working set within L2
         if self.rods:
             self.scene = scenes.rods_and_spheres(seed=seed)
             self.name = "rods256x100_spheres64"
@@ -85,6 +96,14 @@ class Workload:
             self.unit = "steps/s"
             self.tol, self.max_iters = 0.0, 0
             self.method = "plain AVBD, 20 fixed iterations per step"
+        elif self.contacts:
+            self.scene = scenes.rods_on_cube(n=32, num_rods=24, segments=32, rod_length=0.9, seed=seed)
+            self.name = "cube32_rods24x32_contacts"
+            self.units = 1
+            self.unit = "steps/s"
+            self.tol, self.max_iters = 0.0, 0
+            self.method = ("plain AVBD with triangle-rod contacts (narrow phase, contact pool, "
+                           "incremental recoloring), 20 fixed iterations per step")
         else:
             self.scene = scenes.batched_cubes(num_scenes=args.scenes, seed=seed)
             self.name = f"batch{args.scenes}_cubes"
@@ -96,8 +115,8 @@ class Workload:
     def sample(self, args, seed):
         """The bounded sample the CPU baseline times, and its unit count."""
         from avbd_b200 import scenes
-        if self.rods:
-            return self.scene, 1, "the same rod scene"
+        if self.single:
+            return self.scene, 1, "the same scene"
         S = args.cpu_sample_scenes
         return (scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=range(S)), S,
                 f"{S} of {args.scenes} scenes of the same batch")
@@ -133,6 +152,8 @@ class Clocks:
         self.path = None
 
     def start(self):
+        """Starts the sampler and returns once it has written its first sample,
+        so its start-up (hundreds of ms) stays out of the timed region."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -141,6 +162,12 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -322,7 +349,7 @@ def run_engine(args):
     sc = wl.scene
     n = sc.num_particles
     stream = torch.cuda.Stream(device=local)
-    learned = not wl.rods and args.warmstart == "learned"
+    learned = not wl.single and args.warmstart == "learned"
     params = warmstart.load_params(args.weights) if learned else None
 
     def build():
@@ -336,7 +363,7 @@ def run_engine(args):
     el = build() if learned else None                # learned warm start, same scenes
     ee = build()                                     # the timed arm again, for the end-to-end run
     setup_s = time.time() - t0
-    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if wl.rods else None
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev) if wl.single else None
 
     for e in (ep, el, ee):
         if e is not None:
@@ -413,7 +440,7 @@ def run_engine(args):
                        "tets_per_gpu": sc.num_tets, "residual_tolerance": wl.tol, "max_iters": wl.max_iters,
                        "method": method, "arms": arms, "precision": args.precision,
                        "l2": (f"L2 flushed (256 MB write) before every timed step; {solve_bytes / 2 / 1e6:.1f} MB "
-                              "of solve data per iteration" if wl.rods else
+                              "of solve data per iteration" if wl.single else
                               f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration"),
                        "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
             "clocks": clk, "gpu_launches": cnt["kernel_launches"],
