@@ -377,37 +377,68 @@ __global__ void __launch_bounds__(256) k_begin_step_rot(DevState<R> s, R dt, R g
 
 enum { RMODE_SOLVE = 0, RMODE_RESIDUAL = 1, RMODE_DEBUG = 2 };
 
-template <typename R, int MODE>
+// LANES threads per node.  The rod elements (at most two) and the node's
+// dynamic contact terms (triangle-rigid then triangle-rod, each in slot order,
+// VBDSolver.hpp:397-446) are spread over the lanes and summed by shuffles;
+// the first lane adds the rigid-ground and joint terms and solves.  One lane
+// serves the static slabs; the lists of vertices with contacts use 8, since a
+// rod node may carry many contacts, each a chain of rotation and Jacobian
+// functions.
+template <typename R, int MODE, int LANES>
 __global__ void __launch_bounds__(ROD_BLOCK) k_solve_rod(DevState<R> s, unsigned begin, unsigned count, R dt, double g,
                                                    double* out, SceneTol T, const uint32_t* __restrict__ list) {
-    unsigned gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= count) return;
-    unsigned p = list ? list[gi] : begin + gi;
-    uint8_t fl = s.flags[p];
-    if (!(fl & VF_ORIENTED) || (fl & VF_FIXED)) return;
+    const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned gi = tid / LANES, lane = tid % LANES;
+    if (LANES == 1 && gi >= count) return;
+    // with several lanes no thread returns before the shuffles, which need the whole warp
+    bool active = gi < count;
+    const unsigned p = active ? (list ? list[gi] : begin + gi) : 0u;
+    const uint8_t fl = active ? s.flags[p] : 0;
+    if (!(fl & VF_ORIENTED) || (fl & VF_FIXED)) active = false;
     // a recolored vertex is solved from its new color's list, not its slab
-    if (MODE == RMODE_SOLVE && !list && s.dyn_skip && s.dyn_skip[p]) return;
-    if (MODE == RMODE_SOLVE && T.active && !T.active[T.scene[p]]) return;
-    if (MODE == RMODE_RESIDUAL && T.cand && !T.cand[T.scene[p]]) return;
-    unsigned slot = s.rot[p];
-    V3<R> x = xyz(s.x[p]);
-    Q4<R> q = q_of(s.q[slot]);
+    if (MODE == RMODE_SOLVE && active && !list && s.dyn_skip && s.dyn_skip[p]) active = false;
+    if (MODE == RMODE_SOLVE && active && T.active && !T.active[T.scene[p]]) active = false;
+    if (MODE == RMODE_RESIDUAL && active && T.cand && !T.cand[T.scene[p]]) active = false;
+    if (LANES == 1 && !active) return;
     Block6<R> B;
     b6_zero(B);
-    for (unsigned k = s.rod_begin[p]; k < s.rod_begin[p + 1]; k++) {
-        unsigned e = s.rod_inc[k];
-        accumulate_rod<R>(s, e >> 1, e & 1u, B);
+    if (active) {
+        const unsigned re = s.rod_begin[p + 1];
+        for (unsigned k = s.rod_begin[p] + lane; k < re; k += LANES) {
+            const unsigned e = s.rod_inc[k];
+            accumulate_rod<R>(s, e >> 1, e & 1u, B);
+        }
+        if (s.dyn_begin) {
+            const unsigned de = s.dyn_begin[p + 1];
+            for (unsigned k = s.dyn_begin[p] + lane; k < de; k += LANES) {
+                const uint32_t en = s.dyn_ent[k];
+                dyn_accumulate6<R>(s, dyn_pool(en), dyn_slot(en), dyn_local(en), B);
+            }
+        }
     }
+    if constexpr (LANES > 1) {
+        // rod and contact blocks are symmetric: the gradient and upper triangle travel
+#pragma unroll
+        for (int m = LANES / 2; m >= 1; m >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 6; i++) B.g[i] += __shfl_xor_sync(0xffffffffu, B.g[i], m);
+#pragma unroll
+            for (int a = 0; a < 6; a++)
+#pragma unroll
+                for (int b = a; b < 6; b++) B.h[a][b] += __shfl_xor_sync(0xffffffffu, B.h[a][b], m);
+        }
+#pragma unroll
+        for (int a = 0; a < 6; a++)
+#pragma unroll
+            for (int b = a + 1; b < 6; b++) B.h[b][a] = B.h[a][b];
+        if (!active || lane != 0) return;
+    }
+    const unsigned slot = s.rot[p];
+    const V3<R> x = xyz(s.x[p]);
+    const Q4<R> q = q_of(s.q[slot]);
     uint8_t f = s.oflag[slot];
     if (f & OF_RGROUND) accumulate_rground<R>(s, slot, x, q, B);
     if (f & OF_JOINT) accumulate_joint<R>(s, slot, x, q, B);
-    // dynamic energies (VBDSolver.hpp:397-446): the node's triangle-rigid then
-    // triangle-rod contacts, each in slot order
-    if (s.dyn_begin)
-        for (unsigned k = s.dyn_begin[p]; k < s.dyn_begin[p + 1]; k++) {
-            const uint32_t en = s.dyn_ent[k];
-            dyn_accumulate6<R>(s, dyn_pool(en), dyn_slot(en), dyn_local(en), B);
-        }
     typename Vec4Of<R>::T y4 = s.y[p];
     R m = y4.w;
     V3<R> I = xyz(s.Iv[slot]);
@@ -547,12 +578,15 @@ template <typename R>
 void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
                       cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list) {
     if (count == 0) return;
+    // nodes with contacts (lists; the debug pass) take 8 lanes, the static slabs one
     if (mode == RMODE_RESIDUAL)
-        k_solve_rod<R, RMODE_RESIDUAL><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_RESIDUAL, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     else if (mode == RMODE_DEBUG)
-        k_solve_rod<R, RMODE_DEBUG><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_DEBUG, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+    else if (list)
+        k_solve_rod<R, RMODE_SOLVE, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     else
-        k_solve_rod<R, RMODE_SOLVE><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_SOLVE, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
     count_launch(c);
 }
 

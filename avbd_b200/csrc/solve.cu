@@ -344,6 +344,18 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
             k = kn;
         }
     }
+    if constexpr (DYN) {
+        // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid then
+        // triangle-rod contacts, each in slot order, spread over the lanes
+        // (a contact term is a chain of rotation and Jacobian functions)
+        if (active) {
+            const unsigned e = s.dyn_begin[p + 1];
+            for (unsigned k = s.dyn_begin[p] + lane; k < e; k += LANES) {
+                const uint32_t en = s.dyn_ent[k];
+                dyn_accumulate3<P, HT>(s, dyn_pool(en), dyn_slot(en), dyn_local(en), B);
+            }
+        }
+    }
     reduce_block<LANES>(B);
     if constexpr (MODE == MODE_FEATURES) {
 #pragma unroll
@@ -365,15 +377,6 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
     double r2 = 0.0, mg2 = 0.0;
     if (active && lane == 0) {
         if (GROUND && (fl & VF_GROUND)) accumulate_ground<P, HT>(s, p, xi, B);
-        if constexpr (DYN) {
-            // dynamic energies (VBDSolver.hpp:397-446): triangle-rigid then
-            // triangle-rod contacts, each in slot order
-            const unsigned e = s.dyn_begin[p + 1];
-            for (unsigned k = s.dyn_begin[p]; k < e; k++) {
-                const uint32_t en = s.dyn_ent[k];
-                dyn_accumulate3<P, HT>(s, dyn_pool(en), dyn_slot(en), dyn_local(en), B);
-            }
-        }
         typename Vec4Of<P>::T y4 = s.y[p];
         P m = y4.w;
         P cm = m * c.inv_dt2;
