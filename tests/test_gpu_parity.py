@@ -201,6 +201,26 @@ def test_per_scene_tolerance_batch_fp64(oracle_lib):
     assert rel_err(e, o, sc) < 1e-7
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_piece_launches_match_slab_launches(monkeypatch, precision):
+    """Run-to-tolerance sweeps launch one block per (color, scene) piece of
+    at most 512 vertices (fewer here, to cut scenes into several pieces);
+    AVBD_SOLVE_CHUNK=0 launches whole slabs.  Both update the same vertices
+    with the same arithmetic: the states and iteration counts agree."""
+    sc = scenes.batched_cubes(num_scenes=6, seed=3, n_min=3, n_max=7)
+    runs = {}
+    for chunk in ("40", "0"):
+        monkeypatch.setenv("AVBD_SOLVE_CHUNK", chunk)
+        e = Context()
+        sc.load(e, precision=precision, residual_tolerance=1e-4, max_iters=150)
+        e.finalize()
+        e.step(5)
+        runs[chunk] = (e.positions(), e.stats()["iterations"])
+    (xa, ia), (xb, ib) = runs["40"], runs["0"]
+    assert abs(ia - ib) <= 2, (ia, ib)
+    assert np.abs(xa - xb).max() / sc.bbox_diagonal() < 1e-7
+
+
 def test_stats_and_no_fallback_on_c1(oracle_lib):
     sc = scenes.cube_fixed_bottom(8)
     e, _ = pair(sc, oracle_lib, "fp32")
