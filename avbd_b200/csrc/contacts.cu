@@ -86,7 +86,6 @@ struct DynHost {
     std::vector<uint4> h_idx;
     std::vector<uint32_t> h_idx5;
     std::vector<double> h_vec;
-    unsigned long long contacts_added = 0, contacts_removed = 0;
 };
 
 namespace {
@@ -197,7 +196,6 @@ int add_contact(avbd_ctx* c, DynHost& D, DynHost::Det& d) {
     d.e_idx = slot;
     for (int k = 0; k < np; k++) mark_dirty(D, ps[k]);
     D.csr_dirty = true;
-    D.contacts_added++;
     return AVBD_OK;
 }
 
@@ -214,7 +212,6 @@ int remove_contact(DynHost& D, const DynHost::Det& d) {
     if (int r = pool_free(P, d.e_idx)) return r;
     P.rec[d.e_idx].flag = 0;
     D.csr_dirty = true;
-    D.contacts_removed++;
     return AVBD_OK;
 }
 
