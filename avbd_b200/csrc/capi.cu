@@ -85,6 +85,11 @@ static void free_device(avbd_ctx* c) {
     c->d_scene_mg2 = nullptr;
     c->d_scene_iters = nullptr;
     c->d_tol_count = nullptr;
+    c->d_tol_it = nullptr;
+    c->d_tol_omega = nullptr;
+    c->d_omega_tab = nullptr;
+    c->omega_tab_n = 0;
+    c->graph_tol = false;
     c->d_solve_ranges = nullptr;
     c->solve_range_off.clear();
     mlp_device_free(c->ws_mlp);
@@ -136,6 +141,7 @@ int avbd_create(avbd_ctx** out, int device, unsigned particles_capacity, unsigne
         return fail(AVBD_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
     c->stream = c->own_stream;
+    if (const char* g = getenv("AVBD_GRAPH")) c->use_graph = atoi(g) != 0;  // 0: no CUDA graphs
     *out = c;
     return AVBD_OK;
 }
@@ -895,7 +901,8 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
         if ((rc = dalloc(c, &c->d_scene, n)) || (rc = dalloc(c, &c->d_scene_active, S)) ||
             (rc = dalloc(c, &c->d_scene_cand, S)) || (rc = dalloc(c, &c->d_scene_r2, S)) ||
             (rc = dalloc(c, &c->d_scene_ex, S)) || (rc = dalloc(c, &c->d_scene_mg2, S)) ||
-            (rc = dalloc(c, &c->d_scene_iters, S)) || (rc = dalloc(c, &c->d_tol_count, 1)))
+            (rc = dalloc(c, &c->d_scene_iters, S)) || (rc = dalloc(c, &c->d_tol_count, 1)) ||
+            (rc = dalloc(c, &c->d_tol_it, 1)) || (rc = dalloc(c, &c->d_tol_omega, 1)))
             return rc;
         CUDA_OR_FAIL(cudaMemcpyAsync(c->d_scene, sid.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, c->stream));
         // the solved part of each color slab is ordered scene by scene
@@ -1116,22 +1123,144 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     return AVBD_OK;
 }
 
+// Records the run-to-tolerance step as one CUDA graph: the step start, a
+// conditional while node whose body is one iteration (sweep, Chebyshev,
+// in-sweep decision, candidates' exact residual, stop decision, loop
+// control), then the velocity update.  The iteration index and its Chebyshev
+// weight live in device memory, so a step needs no host round trip; the loop
+// runs the iterations of the host-driven loop, in the same order, with the
+// same weights.
+template <typename R>
+int build_tol_graph(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, unsigned max_it, double tol,
+                    const SceneTol& solveT, const SceneTol& resT) {
+    if (c->omega_tab_n < max_it) {
+        if (c->d_omega_tab) {
+            CUDA_OR_FAIL(cudaStreamSynchronize(st));
+            cudaFree(c->d_omega_tab);
+            c->allocations.erase(std::find(c->allocations.begin(), c->allocations.end(), (void*)c->d_omega_tab));
+            c->d_omega_tab = nullptr;
+            c->omega_tab_n = 0;
+        }
+        if (int r = dalloc(c, &c->d_omega_tab, max_it)) return r;
+        c->omega_tab_n = max_it;
+    }
+    std::vector<double> tab(max_it);
+    double w = 1;
+    for (unsigned i = 0; i < max_it; i++) tab[i] = w = omega_at(i, c->solver.iter_acceleration, w);
+    CUDA_OR_FAIL(cudaMemcpyAsync(c->d_omega_tab, tab.data(), sizeof(double) * max_it, cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaStreamSynchronize(st));
+
+    SceneTol loopT = solveT;
+    loopT.omega = c->d_tol_omega;
+    const unsigned long long before = c->stats.kernel_launches;
+    cudaGraph_t g = nullptr;
+    CUDA_OR_FAIL(cudaGraphCreate(&g, 0));
+    auto abandon = [&](const char* what, cudaError_t e) {
+        cudaGraph_t partial = nullptr;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+            cudaStreamEndCapture(st, &partial);
+        cudaGraphDestroy(g);
+        c->stats.kernel_launches = before;
+        return fail(AVBD_ERR_CUDA, std::string(what) + cudaGetErrorString(e));
+    };
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    // step start and the per-scene bookkeeping
+    cudaError_t e = cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    enqueue_begin<R>(c, s, k, st);  // no host step without dynamic contacts: cannot fail
+    launch_tol_init(c, st);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    std::vector<cudaGraphNode_t> tail(deps, deps + ndeps);
+    e = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    // the iteration loop
+    cudaGraphConditionalHandle h;
+    e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return abandon("conditional handle: ", e);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t loop;
+    e = cudaGraphAddNode(&loop, g, tail.data(), tail.size(), &np);
+    if (e != cudaSuccess) return abandon("conditional node: ", e);
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, mode);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    const unsigned long long body0 = c->stats.kernel_launches;
+    enqueue_sweep<R>(c, s, k, st, loopT);
+    enqueue_chebyshev<R>(c, s, k, 1.0, st, loopT);
+    launch_tol_decide_a(c, tol, st);
+    enqueue_residual<R>(c, s, k, nullptr, st, resT);
+    launch_tol_decide_b(c, tol, max_it, st);
+    const unsigned body_launches = (unsigned)(c->stats.kernel_launches - body0);
+    launch_tol_loop_next(c, h, max_it, body_launches, st);
+    e = cudaStreamEndCapture(st, &body);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    // step end
+    e = cudaStreamBeginCaptureToGraph(st, g, &loop, nullptr, 1, mode);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    enqueue_velocity<R>(c, s, k, st);
+    e = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess) return abandon("graph capture: ", e);
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        c->graph = nullptr;
+        c->stats.kernel_launches = before;
+        return fail(AVBD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    // launches counted per graph launch on the host; the loop body's are
+    // counted on the device by the loop control kernel
+    c->launches_per_step = c->stats.kernel_launches - before - body_launches;
+    c->stats.kernel_launches = before;
+    c->graph_tol = true;
+    c->graph_dirty = false;
+    return AVBD_OK;
+}
+
 template <typename R>
 int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
     StepConsts k = consts(c);
     cudaStream_t st = c->stream;
-    if (c->solver.residual_tolerance > 0) {
+    // a step with dynamic contacts runs host work between its launches: no graph
+    const bool capturable =
+        c->use_graph && !c->dyn && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+    const bool tol_mode = c->solver.residual_tolerance > 0;
+    if (c->graph && (c->graph_dirty || c->graph_tol != tol_mode || !capturable)) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    if (tol_mode) {
         // Run-to-tolerance, scene by scene: a scene iterates until its own
         // residual R_s <= tol (or max_iters), exactly as it would alone in a
         // context.  The in-sweep residual the solve accumulates for free marks
         // candidate scenes; only those pay for the exact post-iteration
         // residual that decides the stop.  Converged scenes are skipped by the
-        // solve, Chebyshev and dual kernels.  One host read per iteration (the
-        // count of scenes still iterating) ends the loop.
+        // solve, Chebyshev and dual kernels.  The iteration loop runs on the
+        // device (a conditional while node of the step's graph); without a
+        // graph, one host read per iteration (the count of scenes still
+        // iterating) ends it.
         const unsigned max_it = c->solver.max_iters ? c->solver.max_iters : 1000;
         const double tol = c->solver.residual_tolerance;
         SceneTol solveT{c->d_scene, c->d_scene_active, nullptr, c->d_scene_r2, nullptr};
         SceneTol resT{c->d_scene, nullptr, c->d_scene_cand, nullptr, c->d_scene_ex};
+        if (capturable) {
+            if (!c->graph)
+                if (int r = build_tol_graph<R>(c, s, k, st, max_it, tol, solveT, resT)) return r;
+            for (unsigned t = 0; t < n_steps; t++) {
+                CUDA_OR_FAIL(cudaGraphLaunch(c->graph, st));
+                c->stats.kernel_launches += c->launches_per_step;
+            }
+            CUDA_OR_FAIL(cudaGetLastError());
+            return AVBD_OK;
+        }
         for (unsigned t = 0; t < n_steps; t++) {
             if (int r = enqueue_begin<R>(c, s, k, st)) return r;
             launch_tol_init(c, st);
@@ -1153,13 +1282,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         CUDA_OR_FAIL(cudaGetLastError());
         return AVBD_OK;
     }
-    // a step with dynamic contacts runs host work between its launches: no graph
-    bool capturable = c->use_graph && !c->dyn && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
-    if (capturable && (c->graph_dirty || !c->graph)) {
-        if (c->graph) {
-            cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
-        }
+    if (capturable && !c->graph) {
         unsigned long long before = c->stats.kernel_launches;
         cudaGraph_t g;
         CUDA_OR_FAIL(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -1171,6 +1294,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         if (e != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         c->launches_per_step = c->stats.kernel_launches - before;
         c->stats.kernel_launches = before;
+        c->graph_tol = false;
         c->graph_dirty = false;
     }
     for (unsigned t = 0; t < n_steps; t++) {
@@ -1236,8 +1360,9 @@ int avbd_collision_stage(avbd_ctx* c) {
 int avbd_get_stats(avbd_ctx* c, avbd_stats* out) {
     if (int r = check_ctx(c)) return r;
     if (!out) return fail(AVBD_ERR_INVALID_ARG, "null stats");
+    unsigned long long loop_launches = 0;  // launched by device-driven iteration loops
     if (c->finalized) {
-        unsigned long long h[5] = {0, 0, 0, 0, 0};
+        unsigned long long h[6] = {0, 0, 0, 0, 0, 0};
         CUDA_OR_FAIL(cudaMemcpyAsync(h, c->d_counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
         if (c->lbvh.pair_count) {
             uint32_t pc = 0;
@@ -1250,6 +1375,7 @@ int avbd_get_stats(avbd_ctx* c, avbd_stats* out) {
         c->stats.iterations = c->host_iterations + h[1];
         c->stats.capped_scene_steps = h[3];
         c->stats.warmstart_applied = h[4];
+        loop_launches = h[5];
         if (c->solver.residual_tolerance > 0 && h[2]) {
             // largest confirmed per-scene residual of the last step (order-preserving encoding)
             unsigned long long u = h[2];
@@ -1260,6 +1386,7 @@ int avbd_get_stats(avbd_ctx* c, avbd_stats* out) {
         }
     }
     *out = c->stats;
+    out->kernel_launches += loop_launches;
     return AVBD_OK;
 }
 

@@ -140,6 +140,8 @@ struct SceneTol {
     const uint8_t* cand = nullptr;    // exact residual only for these scenes
     double* r2 = nullptr;             // per-scene sum of in-sweep block residuals^2
     double* ex = nullptr;             // per-scene sum of exact block residuals^2
+    const double* omega = nullptr;    // Chebyshev weight of this iteration in device memory
+                                      // (device-driven iteration loop), else the launch argument
 };
 
 // Scalar arguments of a step.
@@ -257,6 +259,13 @@ struct avbd_ctx {
     double* d_scene_mg2 = nullptr;
     uint32_t* d_scene_iters = nullptr;
     int* d_tol_count = nullptr;
+    // device-driven iteration loop of run-to-tolerance steps (one CUDA graph
+    // with a conditional while node): iteration index, Chebyshev weight of the
+    // current iteration and the weights of iterations 0..omega_tab_n-1
+    uint32_t* d_tol_it = nullptr;
+    double* d_tol_omega = nullptr;
+    double* d_omega_tab = nullptr;
+    unsigned omega_tab_n = 0;
     // (first internal vertex, count, scene) pieces of at most solve_chunk
     // vertices of each scene's solved vertices in each color slab, color by
     // color (offsets solve_range_off): the sweeps and the residual pass of
@@ -266,9 +275,11 @@ struct avbd_ctx {
     unsigned solve_chunk = 512;
     unsigned long long host_iterations = 0;  // scene-iterations of fixed-iteration steps
 
-    // CUDA graph of one full step (fixed-iteration mode)
+    // CUDA graph of one full step: fixed iterations, or (graph_tol) the
+    // run-to-tolerance step whose iteration loop is a conditional while node
     cudaGraphExec_t graph = nullptr;
     bool graph_dirty = true;
+    bool graph_tol = false;
     bool use_graph = true;
     int lanes = 8;                      // threads per vertex in the tet solve
     int block = 256;
@@ -370,6 +381,8 @@ void launch_store_rot(const DevState<R>& s, int which, double* dst, const uint32
 void launch_tol_init(avbd_ctx* c, cudaStream_t st);
 void launch_tol_decide_a(avbd_ctx* c, double tol, cudaStream_t st);
 void launch_tol_decide_b(avbd_ctx* c, double tol, unsigned max_it, cudaStream_t st);
+void launch_tol_loop_next(avbd_ctx* c, cudaGraphConditionalHandle h, unsigned max_it, unsigned body_launches,
+                          cudaStream_t st);
 template <typename R>
 void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st);
 template <typename R>

@@ -508,6 +508,7 @@ __global__ void __launch_bounds__(256) k_chebyshev_rot(DevState<R> s, R omega, S
     uint8_t fl = s.flags[p];
     if (!(fl & VF_ORIENTED)) return;
     if (T.active && !T.active[T.scene[p]]) return;
+    if (T.omega) omega = (R)*T.omega;
     unsigned slot = s.rot[p];
     typename Vec4Of<R>::T x4 = s.x[p], l4 = s.xl[p], ll4 = s.xll[p];
     V3<R> xn = omega * (xyz(x4) - xyz(ll4)) + xyz(ll4);

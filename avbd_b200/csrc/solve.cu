@@ -520,6 +520,7 @@ __global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega, 
     uint8_t fl = s.flags[p];
     if (fl & VF_ORIENTED) return;
     if (T.active && !T.active[T.scene[p]]) return;
+    if (T.omega) omega = (R)*T.omega;
     typename Vec4Of<R>::T x4 = s.x[p], l4 = s.xl[p], ll4 = s.xll[p];
     V3<R> x = xyz(x4), ll = xyz(ll4);
     V3<R> xn = omega * (x - ll) + ll;
@@ -755,9 +756,13 @@ void launch_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* o
 
 // ------------------------------------------- per-scene run-to-tolerance
 __global__ void k_tol_init(uint8_t* active, uint8_t* cand, double* r2, double* ex, uint32_t* iters, unsigned S,
-                           unsigned long long* maxr) {
+                           unsigned long long* maxr, uint32_t* it, double* omega, const double* omega_tab) {
     unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s == 0) *maxr = 0ull;
+    if (s == 0) {
+        *maxr = 0ull;
+        *it = 0;
+        if (omega_tab) *omega = omega_tab[0];
+    }
     if (s >= S) return;
     active[s] = 1;
     cand[s] = 0;
@@ -816,7 +821,8 @@ __global__ void k_tol_decide_b(uint8_t* active, uint8_t* cand, double* ex, const
 void launch_tol_init(avbd_ctx* c, cudaStream_t st) {
     unsigned S = c->num_scenes;
     k_tol_init<<<nblocks(S, 256), 256, 0, st>>>(c->d_scene_active, c->d_scene_cand, c->d_scene_r2, c->d_scene_ex,
-                                                c->d_scene_iters, S, c->d_counters + 2);
+                                                c->d_scene_iters, S, c->d_counters + 2, c->d_tol_it, c->d_tol_omega,
+                                                c->d_omega_tab);
     count_launch(c);
 }
 
@@ -836,6 +842,27 @@ void launch_tol_decide_b(avbd_ctx* c, double tol, unsigned max_it, cudaStream_t 
                                                     c->params.g_accel * c->params.g_accel, max_it, c->d_tol_count,
                                                     c->d_counters + 2);
     count_launch(c);
+}
+
+// End of one iteration of the device-driven loop: counts it and continues the
+// while node while scenes are still iterating.  iters of a scene reach max_it
+// within max_it iterations, so n_active is 0 by then; the index bound stops
+// the loop at max_it in any case.  Also counts the body's kernel launches.
+__global__ void k_tol_loop_next(cudaGraphConditionalHandle h, const int* n_active, uint32_t* it,
+                                const double* omega_tab, double* omega, unsigned max_it,
+                                unsigned long long body_launches, unsigned long long* launches) {
+    const uint32_t i = *it + 1;
+    *it = i;
+    *launches += body_launches;
+    const bool more = *n_active > 0 && i < max_it;
+    if (more) *omega = omega_tab[i];
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+void launch_tol_loop_next(avbd_ctx* c, cudaGraphConditionalHandle h, unsigned max_it, unsigned body_launches,
+                          cudaStream_t st) {
+    k_tol_loop_next<<<1, 1, 0, st>>>(h, c->d_tol_count, c->d_tol_it, c->d_omega_tab, c->d_tol_omega, max_it,
+                                     body_launches + 1ull, c->d_counters + 5);
 }
 
 template <typename R>

@@ -221,6 +221,34 @@ def test_piece_launches_match_slab_launches(monkeypatch, precision):
     assert np.abs(xa - xb).max() / sc.bbox_diagonal() < 1e-7
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_iteration_loop_matches_host_loop(monkeypatch, precision):
+    """A run-to-tolerance step is one CUDA graph whose iteration loop is a
+    conditional while node (index and Chebyshev weight in device memory);
+    AVBD_GRAPH=0 runs the same launches from a host loop that reads the count
+    of scenes still iterating after every iteration.  The per-scene sums of
+    residuals are atomic, so the two agree to rounding: states, iteration
+    counts and launch counts (the graph adds one loop-control kernel per
+    iteration)."""
+    sc = scenes.batched_cubes(num_scenes=6, seed=5, n_min=3, n_max=7)
+    runs = {}
+    for graph in ("1", "0"):
+        monkeypatch.setenv("AVBD_GRAPH", graph)
+        e = Context()
+        sc.load(e, precision=precision, residual_tolerance=1e-4, max_iters=150)
+        e.finalize()
+        e.step(2)
+        e.step(4)  # the second call replays the recorded graph
+        st = e.stats()
+        runs[graph] = (e.positions(), st["iterations"], st["kernel_launches"], st["capped_scene_steps"])
+        e.close()
+    (xa, ia, la, ca), (xb, ib, lb, cb) = runs["1"], runs["0"]
+    assert ia > 6 * 6 and abs(ia - ib) <= 2, (ia, ib)
+    assert ca == cb
+    assert np.abs(xa - xb).max() / sc.bbox_diagonal() < 1e-7
+    assert lb < la < 1.2 * lb, (la, lb)
+
+
 def test_stats_and_no_fallback_on_c1(oracle_lib):
     sc = scenes.cube_fixed_bottom(8)
     e, _ = pair(sc, oracle_lib, "fp32")
