@@ -302,7 +302,8 @@ template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUN
 __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS>* __restrict__ inc, unsigned begin,
                                            unsigned count, unsigned gi, unsigned lane, const Consts<P>& c,
                                            unsigned long long* counters, double* out, const SceneTol& T,
-                                           const float4* __restrict__ aux, const uint32_t* __restrict__ list) {
+                                           const float4* __restrict__ aux, const uint32_t* __restrict__ list,
+                                           double* acc = nullptr) {
     bool active = gi < count;
     unsigned p = list ? (active ? list[gi] : 0u) : begin + (active ? gi : 0);
     uint8_t fl = active ? s.flags[p] : 0;
@@ -387,7 +388,8 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
             if (T.r2) {  // in-sweep residual: the block RHS just before this vertex's update
                 double q = (double)rhs.x * (double)rhs.x + (double)rhs.y * (double)rhs.y +
                            (double)rhs.z * (double)rhs.z;
-                atomicAdd(T.r2 + T.scene[p], q);
+                if (acc) *acc += q;  // one scene per block: summed over the block
+                else atomicAdd(T.r2 + T.scene[p], q);
             }
             V3<P> dx;
             P kappa = solve_sym3<P>(A, rhs, dx);
@@ -467,7 +469,10 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
     }
     if constexpr (MODE == MODE_RESIDUAL) {
         if (T.ex) {  // per-scene sums
-            if (active && lane == 0) atomicAdd(T.ex + T.scene[p], r2);
+            if (active && lane == 0) {
+                if (acc) *acc += r2;
+                else atomicAdd(T.ex + T.scene[p], r2);
+            }
             return;
         }
         // FP64 reduction: warp, then one atomic per warp
@@ -487,8 +492,11 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
 // (a piece of one scene's part of a color slab) and returns at once when the
 // scene is not iterating (solve) or not a residual candidate (residual):
 // with per-scene run-to-tolerance most scenes drop out of the later
-// iterations, and a block of them then costs one check.  Otherwise thread
-// groups map to vertices [begin, begin + count) (or to list).
+// iterations, and a block of them then costs one check.  The block's
+// residual terms (in-sweep or exact) are summed in registers and reduced
+// over the block: one atomic per piece instead of one per vertex on the
+// scene's sum.  Otherwise thread groups map to vertices [begin, begin +
+// count) (or to list).
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
 __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
@@ -500,9 +508,27 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
         const uint4 rg = ranges[blockIdx.x];
         const uint8_t* gate = MODE == MODE_SOLVE ? T.active : T.cand;
         if (gate && !gate[rg.z]) return;
+        double* sum = MODE == MODE_SOLVE ? T.r2 : (MODE == MODE_RESIDUAL ? T.ex : nullptr);
+        SceneTol TB = T;  // gated above, for the whole block
+        TB.active = nullptr;
+        TB.cand = nullptr;
+        double acc = 0.0;
         for (unsigned base = 0; base < rg.y; base += blockDim.x / LANES)
             tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, rg.x, rg.y, base + threadIdx.x / LANES, lane,
-                                                                  c, counters, out, T, aux, list);
+                                                                  c, counters, out, TB, aux, list,
+                                                                  sum ? &acc : nullptr);
+        if (sum) {
+            __shared__ double part[32];
+#pragma unroll
+            for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+            if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (unsigned w = 0; w < (blockDim.x >> 5); w++) t += part[w];
+                atomicAdd(sum + rg.z, t);
+            }
+        }
         return;
     }
     const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
