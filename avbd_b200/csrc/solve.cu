@@ -132,6 +132,8 @@ AVBD_D IncRec<float> load_rec<float>(const IncRec<float>* p) {
     r.d[8] = d.x; r.vlam = d.y; r.vmu = d.z; r.mol = d.w;
     return r;
 }
+AVBD_D void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 template <>
 AVBD_D IncRec<double> load_rec<double>(const IncRec<double>* p) {
     const double2* q = reinterpret_cast<const double2*>(p);
@@ -329,6 +331,8 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
             const unsigned kn = k + LANES;
             IncRec<RS> rn;
             if (kn < e) rn = load_rec<RS>(inc + kn);
+            // and the record three further on is fetched into L2
+            if (kn + 3 * LANES < e) prefetch_l2(inc + kn + 3 * LANES);
             accumulate_tet<P, RS, HT, DAMP>(s, r, xi, c.dt, B);
             if constexpr (MODE == MODE_FEATURES) {
 #pragma unroll
@@ -513,10 +517,21 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
         TB.active = nullptr;
         TB.cand = nullptr;
         double acc = 0.0;
-        for (unsigned base = 0; base < rg.y; base += blockDim.x / LANES)
+        for (unsigned base = 0; base < rg.y; base += blockDim.x / LANES) {
+            // the first records of this thread group's next vertex are fetched
+            // into L2 while this one is solved (its first loads are then not
+            // DRAM misses)
+            const unsigned gn = base + blockDim.x / LANES + threadIdx.x / LANES;
+            if (gn < rg.y) {
+                const unsigned bn = s.inc_begin[rg.x + gn], en = s.inc_begin[rg.x + gn + 1];
+#pragma unroll
+                for (unsigned j = 0; j < 4; j++)
+                    if (bn + lane + j * LANES < en) prefetch_l2(inc + bn + lane + j * LANES);
+            }
             tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, rg.x, rg.y, base + threadIdx.x / LANES, lane,
                                                                   c, counters, out, TB, aux, list,
                                                                   sum ? &acc : nullptr);
+        }
         if (sum) {
             __shared__ double part[32];
 #pragma unroll
