@@ -1015,10 +1015,10 @@ void enqueue_sweep(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_
 }
 
 template <typename R>
-void enqueue_chebyshev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+void enqueue_chebyshev(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st,
                        const SceneTol& T) {
-    launch_chebyshev_dual<R>(c, s, k, omega, st, T);
-    launch_chebyshev_rot<R>(c, s, k, omega, st, T);
+    launch_chebyshev_dual<R>(c, s, k, omega, it, st, T);
+    launch_chebyshev_rot<R>(c, s, k, omega, it, st, T);
     if (c->dyn) launch_contact_after_iter<R>(c, s, st, T);
 }
 
@@ -1041,9 +1041,9 @@ void enqueue_residual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double* 
 }
 
 template <typename R>
-void enqueue_iteration(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st) {
+void enqueue_iteration(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st) {
     enqueue_sweep<R>(c, s, k, st, SceneTol());
-    enqueue_chebyshev<R>(c, s, k, omega, st, SceneTol());
+    enqueue_chebyshev<R>(c, s, k, omega, it, st, SceneTol());
 }
 
 template <typename R>
@@ -1052,7 +1052,7 @@ int enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStr
     double omega = 1;
     for (unsigned i = 0; i < c->solver.solver_iters; i++) {
         omega = omega_at(i, c->solver.iter_acceleration, omega);
-        enqueue_iteration<R>(c, s, k, omega, st);
+        enqueue_iteration<R>(c, s, k, omega, i, st);
     }
     enqueue_velocity<R>(c, s, k, st);
     return AVBD_OK;
@@ -1152,6 +1152,7 @@ int build_tol_graph(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream
 
     SceneTol loopT = solveT;
     loopT.omega = c->d_tol_omega;
+    loopT.it = c->d_tol_it;
     const unsigned long long before = c->stats.kernel_launches;
     cudaGraph_t g = nullptr;
     CUDA_OR_FAIL(cudaGraphCreate(&g, 0));
@@ -1195,7 +1196,7 @@ int build_tol_graph(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream
     if (e != cudaSuccess) return abandon("graph capture: ", e);
     const unsigned long long body0 = c->stats.kernel_launches;
     enqueue_sweep<R>(c, s, k, st, loopT);
-    enqueue_chebyshev<R>(c, s, k, 1.0, st, loopT);
+    enqueue_chebyshev<R>(c, s, k, 1.0, 0, st, loopT);
     launch_tol_decide_a(c, tol, st);
     enqueue_residual<R>(c, s, k, nullptr, st, resT);
     launch_tol_decide_b(c, tol, max_it, st);
@@ -1268,7 +1269,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
             for (unsigned it = 0; it < max_it; it++) {
                 omega = omega_at(it, c->solver.iter_acceleration, omega);
                 enqueue_sweep<R>(c, s, k, st, solveT);
-                enqueue_chebyshev<R>(c, s, k, omega, st, solveT);
+                enqueue_chebyshev<R>(c, s, k, omega, it, st, solveT);
                 launch_tol_decide_a(c, tol, st);
                 enqueue_residual<R>(c, s, k, nullptr, st, resT);
                 launch_tol_decide_b(c, tol, max_it, st);
@@ -1586,8 +1587,8 @@ int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, doubl
             bytes += c->color_bytes[col];
             CUDA_OR_FAIL(cudaEventRecord(b, c->stream));
         }
-        if (use64(c)) enqueue_chebyshev<double>(c, c->d, k, omega, c->stream, SceneTol());
-        else enqueue_chebyshev<float>(c, c->f, k, omega, c->stream, SceneTol());
+        if (use64(c)) enqueue_chebyshev<double>(c, c->d, k, omega, it, c->stream, SceneTol());
+        else enqueue_chebyshev<float>(c, c->f, k, omega, it, c->stream, SceneTol());
     }
     CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
     double ms = 0;

@@ -65,6 +65,10 @@ template <typename R>
 struct DevState {
     using V4 = typename Vec4Of<R>::T;
     unsigned n = 0;
+    // xl, xll: the Chebyshev history, two buffers by iteration parity.
+    // Iteration k reads o_(k-2) from buffer k&1 (xl even, xll odd) and writes
+    // its accelerated iterate o_k there; both hold the step's start position
+    // before iteration 0.
     V4 *x = nullptr, *y = nullptr, *xp = nullptr, *xl = nullptr, *xll = nullptr, *v = nullptr, *vp = nullptr;
     uint8_t* flags = nullptr;
     IncRec<R>* inc = nullptr;
@@ -142,6 +146,7 @@ struct SceneTol {
     double* ex = nullptr;             // per-scene sum of exact block residuals^2
     const double* omega = nullptr;    // Chebyshev weight of this iteration in device memory
                                       // (device-driven iteration loop), else the launch argument
+    const uint32_t* it = nullptr;     // index of this iteration in device memory, likewise
 };
 
 // Scalar arguments of a step.
@@ -356,7 +361,7 @@ void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsign
                         cudaStream_t st, const SceneTol& T = SceneTol(), const uint32_t* list = nullptr,
                         const uint4* ranges = nullptr, unsigned nranges = 0);
 template <typename R>
-void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st,
                            const SceneTol& T = SceneTol());
 template <typename R>
 void launch_velocity(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);
@@ -370,7 +375,7 @@ template <typename R>
 void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
                       cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list = nullptr);
 template <typename R>
-void launch_chebyshev_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+void launch_chebyshev_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st,
                           const SceneTol& T = SceneTol());
 template <typename R>
 void launch_velocity_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st);

@@ -502,20 +502,21 @@ __global__ void __launch_bounds__(ROD_BLOCK) k_solve_rod(DevState<R> s, unsigned
 // Chebyshev acceleration of oriented particles (position and rotation) fused
 // with the dual updates of their rigid-body ground contact and joint.
 template <typename R>
-__global__ void __launch_bounds__(256) k_chebyshev_rot(DevState<R> s, R omega, SceneTol T) {
+__global__ void __launch_bounds__(256) k_chebyshev_rot(DevState<R> s, R omega, unsigned it, SceneTol T) {
     unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= s.n) return;
     uint8_t fl = s.flags[p];
     if (!(fl & VF_ORIENTED)) return;
     if (T.active && !T.active[T.scene[p]]) return;
     if (T.omega) omega = (R)*T.omega;
+    if (T.it) it = *T.it;
     unsigned slot = s.rot[p];
-    typename Vec4Of<R>::T x4 = s.x[p], l4 = s.xl[p], ll4 = s.xll[p];
+    typename Vec4Of<R>::T* h = (it & 1u) ? s.xll : s.xl;  // position history by parity
+    typename Vec4Of<R>::T x4 = s.x[p], ll4 = h[p];
     V3<R> xn = omega * (xyz(x4) - xyz(ll4)) + xyz(ll4);
     typename Vec4Of<R>::T o = make4<R>(xn, x4.w);
     s.x[p] = o;
-    s.xll[p] = l4;
-    s.xl[p] = o;
+    h[p] = o;
     Q4<R> q = q_of(s.q[slot]), qll = q_of(s.qll[slot]);
     Q4<R> qn = plus_s3_stored(qll, omega * minus_s3(q, qll));
     s.q[slot] = q_store(qn);
@@ -592,11 +593,11 @@ void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned
 }
 
 template <typename R>
-void launch_chebyshev_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
+void launch_chebyshev_rot(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st,
                           const SceneTol& T) {
     (void)k;
     if (s.no == 0) return;
-    k_chebyshev_rot<R><<<nblk(s.n, 256), 256, 0, st>>>(s, (R)omega, T);
+    k_chebyshev_rot<R><<<nblk(s.n, 256), 256, 0, st>>>(s, (R)omega, it, T);
     count_launch(c);
 }
 
@@ -618,7 +619,7 @@ void launch_store_rot(const DevState<R>& s, int which, double* dst, const uint32
     template void launch_begin_step_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);         \
     template void launch_solve_rod<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,          \
                                       cudaStream_t, const SceneTol&, int, double*, const uint32_t*);           \
-    template void launch_chebyshev_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t,    \
+    template void launch_chebyshev_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, unsigned, cudaStream_t,    \
                                           const SceneTol&);                                                     \
     template void launch_velocity_rot<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);            \
     template void launch_store_rot<R>(const DevState<R>&, int, double*, const uint32_t*, unsigned, cudaStream_t);

@@ -555,20 +555,22 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
 // update that follows it (CollisionConstraintEnergySolver::updateAfterIteration);
 // a ground energy reads only its own particle, so the fusion is exact.
 template <typename R>
-__global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega, SceneTol T) {
+__global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega, unsigned it, SceneTol T) {
     unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= s.n) return;
     uint8_t fl = s.flags[p];
     if (fl & VF_ORIENTED) return;
     if (T.active && !T.active[T.scene[p]]) return;
     if (T.omega) omega = (R)*T.omega;
-    typename Vec4Of<R>::T x4 = s.x[p], l4 = s.xl[p], ll4 = s.xll[p];
+    if (T.it) it = *T.it;
+    // o_k = omega (x - o_(k-2)) + o_(k-2); o_k replaces o_(k-2) in its buffer
+    typename Vec4Of<R>::T* h = (it & 1u) ? s.xll : s.xl;
+    typename Vec4Of<R>::T x4 = s.x[p], ll4 = h[p];
     V3<R> x = xyz(x4), ll = xyz(ll4);
     V3<R> xn = omega * (x - ll) + ll;
     typename Vec4Of<R>::T o = make4<R>(xn, x4.w);
     s.x[p] = o;
-    s.xll[p] = l4;
-    s.xl[p] = o;
+    h[p] = o;
     if (fl & VF_GROUND) {
         typename Vec4Of<R>::T k = s.gk[p], lam = s.glam[p], cp = s.gcp[p];
         uint8_t gf = s.gflag[p];
@@ -769,10 +771,10 @@ void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsign
 }
 
 template <typename R>
-void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, cudaStream_t st,
-                           const SceneTol& T) {
+void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it,
+                           cudaStream_t st, const SceneTol& T) {
     (void)k;
-    k_chebyshev_dual<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)omega, T);
+    k_chebyshev_dual<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)omega, it, T);
     count_launch(c);
 }
 
@@ -973,7 +975,7 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
     template void launch_tet_eprev<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                \
     template void launch_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,         \
                                         cudaStream_t, const SceneTol&, const uint32_t*, const uint4*, unsigned); \
-    template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, cudaStream_t,    \
+    template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, unsigned, cudaStream_t,    \
                                            const SceneTol&);                                                    \
     template void launch_velocity<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                 \
     template void launch_residual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double*, cudaStream_t,         \
