@@ -579,12 +579,15 @@ __global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega, 
         R ln = k.x * cc + lam.x;
         R lt = k.y * Ct + lam.y;
         R lb = k.z * Cb + lam.z;
+        // the penalties grow only in contact: elsewhere k is not stored back
+        bool k_grows = ln > R(0);
         if (ln > R(0)) k.x += R(AVBD_BETA) * fabs(cc);
         lam.x = ln > R(0) ? ln : R(0);
         R mag = sqrt(lt * lt + lb * lb);
         bool st = gf & GF_USE_STATIC;
         R mx = (st ? cp.z : cp.w) * lam.x;
         if (mag < mx) {
+            k_grows = true;
             k.y += R(AVBD_BETA) * fabs(Ct);
             k.z += R(AVBD_BETA) * fabs(Cb);
             lam.y = lt;
@@ -599,7 +602,7 @@ __global__ void __launch_bounds__(256) k_chebyshev_dual(DevState<R> s, R omega, 
             lam.z = lb / (mag + R(1e-8)) * mx;
             gf &= ~GF_UNCLAMPED;
         }
-        s.gk[p] = k;
+        if (k_grows) s.gk[p] = k;
         s.glam[p] = lam;
         s.gflag[p] = gf;
     }
