@@ -13,7 +13,9 @@ Cases (scene builders of avbd_b200.scenes, all seeded):
   cube_fixed_bottom4 -- NeoHookean cube, bottom fixed, fixed iterations, Chebyshev;
   batch3_tol         -- three cubes with ground contact run to R <= 1e-4 per scene;
   spheres_on_cube    -- triangle-sphere CCD, the triangle-rigid contact pool, recoloring;
-  rods_on_cube       -- Cosserat rods, triangle-rod contacts, 6-DOF solve.
+  rods_on_cube       -- Cosserat rods, triangle-rod contacts, 6-DOF solve;
+  rods_spheres       -- helical rods hanging from one-sided fixed joints, spheres,
+                        rigid-body ground contact.
 """
 import json
 import os
@@ -34,6 +36,8 @@ CASES = [
      {"residual_tolerance": 1e-4, "max_iters": 100}, [1, 6]),
     ("spheres_on_cube", lambda: scenes.spheres_on_cube(n=3, num_spheres=2, seed=2), {}, [1, 20]),
     ("rods_on_cube", lambda: scenes.rods_on_cube(n=3, num_rods=2, segments=6, seed=1), {}, [1, 20]),
+    ("rods_spheres", lambda: scenes.rods_and_spheres(num_rods=2, segments=40, num_spheres=2, seed=3, length=0.4),
+     {}, [1, 30]),
 ]
 
 

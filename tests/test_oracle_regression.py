@@ -25,7 +25,8 @@ def cases():
     return CASES
 
 
-@pytest.mark.parametrize("name", ["cube_fixed_bottom4", "batch3_tol", "spheres_on_cube", "rods_on_cube"])
+@pytest.mark.parametrize("name", ["cube_fixed_bottom4", "batch3_tol", "spheres_on_cube", "rods_on_cube",
+                                  "rods_spheres"])
 def test_oracle_reproduces_frozen_trajectory(oracle_lib, name):
     ref = golden("oracle_regression.json")[name]
     builder, kw = cases()[name]
