@@ -18,6 +18,7 @@ ERRORS = {
     5: "AVBD_ERR_NAN", 6: "AVBD_ERR_BARRIER_TIMEOUT", 7: "AVBD_ERR_CUDA", 8: "AVBD_ERR_STATE",
     9: "AVBD_ERR_UNSUPPORTED", 10: "AVBD_ERR_NO_DEVICE",
 }
+DEFAULT_WAIT_POLLS = 1 << 22
 PRECISION_FP32 = 0
 PRECISION_FP64 = 1
 PRECISION_MIXED = 2
@@ -96,6 +97,8 @@ SIGNATURES = {
     "avbd_get_rod_contact_pool": [_vp, C.c_uint, _up, _u8p, _dp, _up],
     "avbd_get_rod_contacts": [_vp, C.c_uint, _u64p, _up, _dp, _up],
     "avbd_debug_set_recolor_rounds": [_vp, C.c_uint],
+    "avbd_debug_set_pair_capacity": [_vp, C.c_uint],
+    "avbd_debug_set_wait_limit": [C.c_int, C.c_uint],
     "avbd_debug_block": [_vp, C.c_uint, _dp, _dp, C.POINTER(C.c_int)],
     "avbd_residual": [_vp, _dp],
     "avbd_profile_solve": [_vp, C.c_uint, _dp, _dp, _up],

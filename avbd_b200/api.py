@@ -318,6 +318,9 @@ class Context:
         return {"key": keys, "tri": idx[:, :3], "rod": idx[:, 3:5], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
                 "cp_local": vec[:, 6:9], "s": vec[:, 9]}
 
+    def set_pair_capacity(self, capacity):
+        check(self.L.avbd_debug_set_pair_capacity(self.h, int(capacity)))
+
     def set_recolor_rounds(self, rounds):
         check(self.L.avbd_debug_set_recolor_rounds(self.h, rounds))
 

@@ -82,6 +82,7 @@ static void free_device(avbd_ctx* c) {
     c->d_scene_cand = nullptr;
     c->d_scene_r2 = nullptr;
     c->d_scene_ex = nullptr;
+    c->d_scene_rin = nullptr;
     c->d_scene_mg2 = nullptr;
     c->d_scene_iters = nullptr;
     c->d_tol_count = nullptr;
@@ -900,7 +901,7 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
             }
         if ((rc = dalloc(c, &c->d_scene, n)) || (rc = dalloc(c, &c->d_scene_active, S)) ||
             (rc = dalloc(c, &c->d_scene_cand, S)) || (rc = dalloc(c, &c->d_scene_r2, S)) ||
-            (rc = dalloc(c, &c->d_scene_ex, S)) || (rc = dalloc(c, &c->d_scene_mg2, S)) ||
+            (rc = dalloc(c, &c->d_scene_ex, S)) || (rc = dalloc(c, &c->d_scene_rin, S)) || (rc = dalloc(c, &c->d_scene_mg2, S)) ||
             (rc = dalloc(c, &c->d_scene_iters, S)) || (rc = dalloc(c, &c->d_tol_count, 1)) ||
             (rc = dalloc(c, &c->d_tol_it, 1)) || (rc = dalloc(c, &c->d_tol_omega, 1)))
             return rc;
@@ -1326,6 +1327,9 @@ int device_error(avbd_ctx* c) {
     CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
     if (h == AVBD_ERR_NAN) return fail(h, "non-finite particle state");
     if (h == AVBD_ERR_UNSUPPORTED_PAIR) return fail(h, "Unsupported collision!");
+    if (h == AVBD_ERR_CAPACITY)
+        return fail(h, "a device buffer overflowed (candidate pairs, narrow-phase contacts or the traversal stack)");
+    if (h == AVBD_ERR_COLORS) return fail(h, "Ran out of colors (more than 256)");
     if (h) return fail(h, "device-side error");
     if (c->ws_mlp) return mlp_device_error(c->ws_mlp, c->stream);
     return AVBD_OK;
@@ -1378,7 +1382,7 @@ int avbd_get_stats(avbd_ctx* c, avbd_stats* out) {
         c->stats.warmstart_applied = h[4];
         loop_launches = h[5];
         if (c->solver.residual_tolerance > 0 && h[2]) {
-            // largest confirmed per-scene residual of the last step (order-preserving encoding)
+            // largest final per-scene residual of the last step (order-preserving encoding)
             unsigned long long u = h[2];
             u = (u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u;
             double r;

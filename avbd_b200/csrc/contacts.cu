@@ -609,11 +609,14 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     DynHost& D = *c->dyn;
     LbvhState& L = c->lbvh;
     // detections of the narrow phase and the pools' multipliers
-    uint32_t cnt = 0;
+    uint32_t cnt = 0, pairs = 0;
     DYN_CUDA(cudaMemcpyAsync(&cnt, L.contact_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaMemcpyAsync(&pairs, L.pair_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     for (int pl = 0; pl < 2; pl++)
         if (int r = download_pool<R>(s.cp[pl], D.pool[pl], st)) return r;
     DYN_CUDA(cudaStreamSynchronize(st));
+    if (pairs > L.pair_capacity)
+        return set_error(AVBD_ERR_CAPACITY, "broad-phase candidate pairs exceed the pair buffer's capacity");
     if (cnt > L.contact_capacity)
         return set_error(AVBD_ERR_CAPACITY, "narrow-phase contacts exceed the contact buffer's capacity");
     D.h_key.resize(cnt);
@@ -798,6 +801,13 @@ int avbd_get_contact_pool(avbd_ctx* c, unsigned capacity, unsigned* p4, uint8_t*
 int avbd_get_rod_contact_pool(avbd_ctx* c, unsigned capacity, unsigned* p5, uint8_t* active, double* data25,
                               unsigned* size) {
     return get_pool(c, POOL_TRI_ROD, capacity, p5, active, data25, size);
+}
+
+int avbd_debug_set_pair_capacity(avbd_ctx* c, unsigned capacity) {
+    if (!c) return set_error(AVBD_ERR_INVALID_ARG, "null context");
+    if (c->finalized) return set_error(AVBD_ERR_STATE, "the pair capacity is fixed at avbd_finalize");
+    c->debug_pair_capacity = capacity;
+    return AVBD_OK;
 }
 
 int avbd_debug_set_recolor_rounds(avbd_ctx* c, unsigned rounds) {

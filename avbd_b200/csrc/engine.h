@@ -216,6 +216,7 @@ struct avbd_ctx {
 
     // capacities (SimulationContext(particles, oriented, energies, prims, sdf))
     unsigned cap_particles, cap_oriented, cap_energies, cap_prims, cap_sdf;
+    unsigned debug_pair_capacity = 0;   // 0: max(1024, 64 primitives) candidate pairs
 
     // host staging in the reference's FP64 layout (external order)
     std::vector<double> x, v, vp, mass;
@@ -261,6 +262,7 @@ struct avbd_ctx {
     uint8_t* d_scene_cand = nullptr;
     double* d_scene_r2 = nullptr;
     double* d_scene_ex = nullptr;
+    double* d_scene_rin = nullptr;      // in-sweep residual of each scene's last iteration
     double* d_scene_mg2 = nullptr;
     uint32_t* d_scene_iters = nullptr;
     int* d_tol_count = nullptr;

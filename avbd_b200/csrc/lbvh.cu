@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(128) k_traverse(LbvhState L, const uint2* rang
         if (node < n) {
             unsigned slot = atomicAdd(L.pair_count, 1u);
             if (slot < L.pair_capacity) L.pairs[slot] = make_uint2(a, node);
+            else atomicExch(err, (int)AVBD_ERR_CAPACITY);  // a dropped pair would be a missed collision
             // narrow-phase dispatch (CollisionDetector.cpp:166-215): triangle-triangle and
             // rod-rod are no-ops; sphere-sphere and sphere-rod throw "Unsupported collision!"
             uint8_t tb = L.type[L.sorted[node]];
@@ -392,7 +393,7 @@ int lbvh_allocate(avbd_ctx* c, std::string& err) {
     L.n = n;
     const unsigned nn = 2 * n - 1;
     L.hist_blocks = nb(n, RB);
-    L.pair_capacity = std::max(1024u, 64u * n);
+    L.pair_capacity = c->debug_pair_capacity ? c->debug_pair_capacity : std::max(1024u, 64u * n);
     std::vector<uint8_t> type(n);
     std::vector<uint4> pidx(n);
     std::vector<double> radius(n);
@@ -565,7 +566,8 @@ extern "C" int avbd_get_candidate_pairs(avbd_ctx* c, unsigned capacity, unsigned
 // being recorded into a CUDA graph, a real-time loop with a fixed memory
 // budget, or an application whose device memory belongs to another
 // framework's allocator.  The arrays are sized for AVBD_NOALLOC_MAX_PRIMITIVES
-// primitives (about 4 MB) and stay resident on every GPU that loads the
+// primitives (about 6 MiB: two 2 MiB key buffers, a 1 MiB index buffer and a
+// 1 MiB digit histogram) and stay resident on every GPU that loads the
 // library until the process exits.
 
 namespace {
@@ -654,34 +656,49 @@ __global__ void __launch_bounds__(256) k_box_of_aabbs(const double* __restrict__
 extern "C" int avbd_lbvh_morton_sort_noalloc(const double* aabb6, unsigned n, uint64_t* morton,
                                              unsigned* sorted_order, void* stream) {
     if (n == 0) return AVBD_OK;
-    if (!aabb6 || !morton || !sorted_order) return AVBD_ERR_INVALID_ARG;
-    if (n > kNoAllocMax) return AVBD_ERR_CAPACITY;
+    if (!aabb6 || !morton || !sorted_order) return set_error(AVBD_ERR_INVALID_ARG, "null buffer");
+    if (n > kNoAllocMax)
+        return set_error(AVBD_ERR_CAPACITY, "more primitives than AVBD_NOALLOC_MAX_PRIMITIVES");
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return AVBD_ERR_NO_DEVICE;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(AVBD_ERR_NO_DEVICE, "no CUDA device");
     NoAllocScratch S;
-    if (int rc = noalloc_scratch(dev, S)) return rc;
+    if (int rc = noalloc_scratch(dev, S)) return set_error(rc, "cannot resolve the scratch arrays' addresses");
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned nblk = (n + RB - 1) / RB;
-    cudaMemsetAsync(S.box, 0xFF, 3 * sizeof(unsigned long long), st);
-    cudaMemsetAsync(S.box + 3, 0x00, 3 * sizeof(unsigned long long), st);
-    k_box_of_aabbs<<<(n + 255) / 256, 256, 0, st>>>(aabb6, n, S.box);
+    // Every call below reports its own status; an error some earlier work
+    // left pending is neither consumed nor mistaken for one of these.
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+        return e == cudaSuccess;
+    };
+    auto launch = [&](auto kernel, unsigned grid, unsigned block, auto... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.stream = st;
+        return ok(cudaLaunchKernelEx(&cfg, kernel, args...));
+    };
     LbvhState L;
     L.n = n;
     L.aabb = const_cast<double*>(aabb6);
     L.morton = morton;          // per-primitive codes (output)
     L.sorted = sorted_order;    // identity, sorted in place below
-    k_morton<<<(n + 255) / 256, 256, 0, st>>>(L, S.box);
-    cudaMemcpyAsync(S.keys_a, morton, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, st);
+    ok(cudaMemsetAsync(S.box, 0xFF, 3 * sizeof(unsigned long long), st)) &&
+        ok(cudaMemsetAsync(S.box + 3, 0x00, 3 * sizeof(unsigned long long), st)) &&
+        launch(k_box_of_aabbs, (n + 255) / 256, 256, (const double*)aabb6, n, S.box) &&
+        launch(k_morton, (n + 255) / 256, 256, L, (const unsigned long long*)S.box) &&
+        ok(cudaMemcpyAsync(S.keys_a, morton, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, st));
     uint64_t *ka = S.keys_a, *kb = S.keys_b;
     uint32_t *va = sorted_order, *vb = S.vals_b;
-    for (int shift = 0; shift < 64; shift += 8) {
-        k_radix_count<<<nblk, RB, 0, st>>>(ka, n, shift, S.hist, nblk);
-        k_radix_scan<<<1, 1024, 0, st>>>(S.hist, 256 * nblk);
-        k_radix_scatter<<<nblk, RB, 0, st>>>(ka, va, kb, vb, n, shift, S.hist, nblk);
+    for (int shift = 0; shift < 64 && e == cudaSuccess; shift += 8) {
+        launch(k_radix_count, nblk, RB, (const uint64_t*)ka, n, shift, S.hist, nblk) &&
+            launch(k_radix_scan, 1, 1024, S.hist, 256 * nblk) &&
+            launch(k_radix_scatter, nblk, RB, (const uint64_t*)ka, (const uint32_t*)va, kb, vb, n, shift,
+                   (const uint32_t*)S.hist, nblk);
         std::swap(ka, kb);
         std::swap(va, vb);
     }
     // eight passes: sorted keys are back in keys_a, the order in sorted_order
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? AVBD_OK : AVBD_ERR_CUDA;
+    return e == cudaSuccess ? AVBD_OK : set_error(AVBD_ERR_CUDA, cudaGetErrorString(e));
 }

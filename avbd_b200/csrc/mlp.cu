@@ -64,11 +64,26 @@ AVBD_D void load_kmaj(uint8_t* dst, const bf16* src, unsigned ld, unsigned R, un
     }
 }
 
+// Polls a barrier wait may take before it gives up (avbd_debug_set_wait_limit
+// lowers it so that tests can make the wait run out).
+__device__ uint32_t g_wait_polls = AVBD_DEFAULT_WAIT_POLLS;
+// Polls the drain after a timeout may take: the MMAs already issued must
+// land before the CTA frees the TMEM columns they write.
+constexpr uint32_t kDrainPolls = AVBD_DEFAULT_WAIT_POLLS;
+
 // all threads wait for the barrier phase; false (uniformly) if it timed out
 AVBD_D bool block_wait(uint64_t* bar, uint32_t& phase) {
-    bool got = tc::mbar_wait(bar, phase);
+    bool got = tc::mbar_wait(bar, phase, *(volatile uint32_t*)&g_wait_polls);
     phase ^= 1u;
     return __syncthreads_and(got ? 1 : 0) != 0;
+}
+
+// After a wait gave up (phase already flipped by block_wait): wait, bounded,
+// for the commit of the MMAs still in flight, so that no tensor-core write
+// reaches the TMEM columns after they are freed.
+AVBD_D void drain_after_timeout(uint64_t* bar, uint32_t phase) {
+    if (threadIdx.x == 0) tc::mbar_wait(bar, phase ^ 1u, kDrainPolls);
+    __syncthreads();
 }
 
 // one thread: D (+)= A B^T over `ksteps` K = 16 steps of two canonical operands
@@ -121,6 +136,7 @@ __global__ void __launch_bounds__(128) k_gemm(const bf16* __restrict__ A, unsign
         }
         ok = block_wait(&bar, phase);
     }
+    if (!ok) drain_after_timeout(&bar, phase);
     tc::fence_after();
     if (ok && ke > kb) {
         const unsigned r = warp * 32 + (tid & 31);
@@ -384,6 +400,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_apply(MlpW w, const bf16* __rest
         __syncthreads();
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy may land after the exit
+    if (!ok) drain_after_timeout(bar, phase);
     tc::fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -614,7 +631,12 @@ int mlp_device_error(const MlpDevice* m, cudaStream_t st) {
     if (cudaMemcpyAsync(&h, m->err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return set_error(AVBD_ERR_CUDA, "MLP error flag read failed");
-    return h ? set_error(h, "MLP kernel: a bounded wait on the tensor-core barrier gave up") : AVBD_OK;
+    if (!h) return AVBD_OK;
+    // the flag is cleared once reported, so the object stays usable
+    if (cudaMemsetAsync(m->err, 0, sizeof(int), st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+        return set_error(AVBD_ERR_CUDA, "MLP error flag reset failed");
+    return set_error(h, "MLP kernel: a bounded wait on the tensor-core barrier gave up; every result of that "
+                        "launch is invalid");
 }
 
 }  // namespace avbd
@@ -660,6 +682,16 @@ int avbd_gemm_bf16(const void* A, unsigned lda, const void* B, unsigned ldb, flo
     if (rc) return rc;
     if (e != cudaSuccess) return set_error(AVBD_ERR_CUDA, cudaGetErrorString(e));
     return h ? set_error(h, "GEMM: a bounded wait on the tensor-core barrier gave up") : AVBD_OK;
+}
+
+int avbd_debug_set_wait_limit(int device, unsigned polls) {
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess)
+        return set_error(AVBD_ERR_NO_DEVICE, "cudaSetDevice failed");
+    cudaError_t e = cudaMemcpyToSymbol(g_wait_polls, &polls, sizeof(polls));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaSetDevice(prev);
+    return e == cudaSuccess ? AVBD_OK : set_error(AVBD_ERR_CUDA, cudaGetErrorString(e));
 }
 
 int avbd_mlp_create(avbd_mlp** out, int device, const float* params) {

@@ -821,15 +821,20 @@ AVBD_D double scene_R(double r2, double mg2) { return mg2 > 0 ? sqrt(r2) / sqrt(
 
 // After a sweep: every active scene counts the iteration and becomes a
 // candidate when its in-sweep residual is at the tolerance.
+// The in-sweep residual is kept (rin) as the final residual of a scene that
+// then stops at the cap without becoming a candidate.
 __global__ void k_tol_decide_a(uint8_t* active, uint8_t* cand, double* r2, const double* m2, uint32_t* iters,
-                               unsigned S, double tol, double g2, unsigned long long* scene_iterations) {
+                               unsigned S, double tol, double g2, unsigned long long* scene_iterations,
+                               double* rin) {
     unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     cand[s] = 0;
     if (active[s]) {
         iters[s]++;
         atomicAdd(scene_iterations, 1ull);
-        cand[s] = scene_R(r2[s], m2[s] * g2) <= tol;
+        const double R = scene_R(r2[s], m2[s] * g2);
+        rin[s] = R;
+        cand[s] = R <= tol;
     }
     r2[s] = 0;
 }
@@ -840,25 +845,32 @@ AVBD_D unsigned long long ord_enc64(double d) {
 }
 
 // Candidates whose exact residual is at the tolerance stop; so does every
-// scene at the iteration cap.  Counts the scenes still iterating.
+// scene at the iteration cap.  Counts the scenes still iterating.  maxr[0]
+// receives the largest final residual of the step's scenes: the exact one
+// where it was evaluated in the stopping iteration, else the in-sweep one of
+// a capped scene; maxr[1] counts the capped scenes.
 __global__ void k_tol_decide_b(uint8_t* active, uint8_t* cand, double* ex, const double* m2, const uint32_t* iters,
                                unsigned S, double tol, double g2, unsigned max_it, int* n_active,
-                               unsigned long long* maxr) {
+                               unsigned long long* maxr, const double* rin) {
     unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S) return;
     if (active[s]) {
         bool done = false;
+        double R = rin[s];
         if (cand[s]) {
-            double R = scene_R(ex[s], m2[s] * g2);
-            atomicMax(maxr, ord_enc64(R));
+            R = scene_R(ex[s], m2[s] * g2);
             done = R <= tol;
         }
         if (!done && iters[s] >= max_it) {  // stopped at the cap, unconverged
             done = true;
             atomicAdd(maxr + 1, 1ull);
         }
-        if (done) active[s] = 0;
-        else atomicAdd(n_active, 1);
+        if (done) {
+            active[s] = 0;
+            atomicMax(maxr, ord_enc64(R));
+        } else {
+            atomicAdd(n_active, 1);
+        }
     }
     cand[s] = 0;
     ex[s] = 0;
@@ -876,7 +888,8 @@ void launch_tol_decide_a(avbd_ctx* c, double tol, cudaStream_t st) {
     unsigned S = c->num_scenes;
     k_tol_decide_a<<<nblocks(S, 256), 256, 0, st>>>(c->d_scene_active, c->d_scene_cand, c->d_scene_r2,
                                                     c->d_scene_mg2, c->d_scene_iters, S, tol,
-                                                    c->params.g_accel * c->params.g_accel, c->d_counters + 1);
+                                                    c->params.g_accel * c->params.g_accel, c->d_counters + 1,
+                                                    c->d_scene_rin);
     count_launch(c);
 }
 
@@ -886,7 +899,7 @@ void launch_tol_decide_b(avbd_ctx* c, double tol, unsigned max_it, cudaStream_t 
     k_tol_decide_b<<<nblocks(S, 256), 256, 0, st>>>(c->d_scene_active, c->d_scene_cand, c->d_scene_ex,
                                                     c->d_scene_mg2, c->d_scene_iters, S, tol,
                                                     c->params.g_accel * c->params.g_accel, max_it, c->d_tol_count,
-                                                    c->d_counters + 2);
+                                                    c->d_counters + 2, c->d_scene_rin);
     count_launch(c);
 }
 

@@ -100,7 +100,11 @@ typedef struct avbd_stats {
     unsigned long long iterations;        /* solver iterations executed       */
     unsigned long long fp64_fallbacks;    /* blocks solved in FP64            */
     unsigned long long candidate_pairs;   /* broad-phase pairs of last step   */
-    double   last_residual;               /* R after the last sweep (or -1)   */
+    double   last_residual;               /* run-to-tolerance steps: largest final
+                                             residual R over the last step's scenes
+                                             (exact where the stopping iteration
+                                             evaluated it, else a capped scene's
+                                             in-sweep R); 0 in fixed-iteration mode */
     unsigned num_colors;
     unsigned num_scenes;
     unsigned long long capped_scene_steps; /* run-to-tolerance scene-steps that
@@ -322,6 +326,14 @@ AVBD_API int avbd_get_rod_contact_pool(avbd_ctx* ctx, unsigned capacity, unsigne
  * (VBDSolver.hpp:82-87,108-119,474-509). */
 AVBD_API int avbd_debug_set_recolor_rounds(avbd_ctx* ctx, unsigned rounds);
 
+/* Test hook (before avbd_finalize): the capacity of the broad-phase
+ * candidate-pair buffer, max(1024, 64 x primitives) unless set (0 restores
+ * that).  The reference's pair list grows without bound
+ * (CollisionDetector.cpp:100-129); here a step whose traversal finds more
+ * pairs than the buffer holds fails with AVBD_ERR_CAPACITY instead of losing
+ * collisions.  A small capacity lets a test reach that path. */
+AVBD_API int avbd_debug_set_pair_capacity(avbd_ctx* ctx, unsigned capacity);
+
 /* Block gradient and Hessian of particle p at the current state: the
  * grad/hess accumulated by VBDSolver::_solveParticle<DOF>
  * (simulation/VBDSolver.hpp:293-447).  G is 3 or 6 doubles, H is 9 or 36
@@ -338,7 +350,7 @@ AVBD_API int avbd_residual(avbd_ctx* ctx, double* residual);
  * being recorded into a CUDA graph, a real-time loop on a fixed memory
  * budget, an application whose device memory belongs to another framework's
  * allocator).  Scratch lives in file-scope device arrays sized for
- * AVBD_NOALLOC_MAX_PRIMITIVES primitives (about 4 MB, resident on every GPU
+ * AVBD_NOALLOC_MAX_PRIMITIVES primitives (about 6 MiB, resident on every GPU
  * that loads the library until exit); larger n returns AVBD_ERR_CAPACITY.
  * aabb6 (n x {min xyz, max xyz} doubles), morton (n codes, one per primitive)
  * and sorted_order (n indices) are device pointers owned by the caller;
@@ -346,7 +358,9 @@ AVBD_API int avbd_residual(avbd_ctx* ctx, double* residual);
  * codes and sorted order of avbd_get_lbvh for the same boxes.  Every call
  * shares the scratch; calls that overlap on the GPU race.  The first call on
  * a device resolves the scratch addresses and should come before any stream
- * capture. */
+ * capture.  Each CUDA call it makes is checked on its own: a CUDA error left
+ * pending by earlier work is not consumed, and AVBD_ERR_CUDA means one of
+ * this call's own launches or copies failed. */
 #define AVBD_NOALLOC_MAX_PRIMITIVES 262144u
 AVBD_API int avbd_lbvh_morton_sort_noalloc(const double* aabb6, unsigned n, uint64_t* morton,
                                            unsigned* sorted_order, void* stream);
@@ -396,6 +410,17 @@ typedef struct avbd_mlp avbd_mlp;
 AVBD_API int avbd_mlp_create(avbd_mlp** out, int device, const float* params);
 AVBD_API int avbd_mlp_forward(avbd_mlp* m, const void* features, unsigned n, float* out, void* stream);
 AVBD_API int avbd_mlp_destroy(avbd_mlp* m);
+
+/* Debug hook with no counterpart in the reference: the number of polls a
+ * tensor-core barrier wait of the MLP and GEMM kernels may take on `device`
+ * before it gives up (AVBD_DEFAULT_WAIT_POLLS unless changed; 0 gives up at
+ * once).  A wait that gives up sets AVBD_ERR_BARRIER_TIMEOUT, which the
+ * launching call returns; every result of that launch is then invalid.  The
+ * kernel still waits, bounded, for the MMAs it issued before it frees its
+ * tensor memory, so the context stays usable.  Tests lower the limit to make
+ * the wait run out without any fault. */
+#define AVBD_DEFAULT_WAIT_POLLS (1u << 22)
+AVBD_API int avbd_debug_set_wait_limit(int device, unsigned polls);
 
 /* Training: mini-batches of `batch` rows (a multiple of 128) of device
  * features (BF16 [batch][32]) and targets (FP32 [batch][4]); loss = mean
