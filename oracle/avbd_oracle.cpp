@@ -15,16 +15,23 @@
 //   * swept AABBs, 63-bit Morton codes, stable LSD radix sort, Karras tree,
 //     refit and self traversal (collision/*).
 //
-// Parity status.  The reference cannot be compiled here (it needs Eigen3,
-// which is not installed), so no reference output exists to pin this file
-// against.  Parity is therefore UNPINNED against the reference binary; it is
-// pinned against what the reference's own tests hold: the finite-difference
-// checks of test/test_neohookean_accumulate.cpp, test_cosserat_accumulate.cpp
-// and test_one_sided_fixed_joint_accumulate.cpp (same inputs, same FD scheme,
+// Parity status: PINNED to the reference implementation itself.  The
+// reference's hot-path sources compile unmodified against the project's
+// Eigen-API shim (oracle/eigen_shim, oracle/Makefile -> oracle/_ref), and
+// tests/test_ref_pinning.py replays the reference's outputs
+// (tests/golden/reference_outputs.npz, written by
+// tests/golden/make_reference_golden.py) through this file: DSATUR colors,
+// Morton codes, sorted order, LBVH topology and bounds, candidate pairs and
+// contact-pool slots identical; positions within 1e-12 .. 1e-9 of the
+// bounding-box diagonal after 1-100 steps (the shim's LU and sums round
+// differently from Eigen's).  It is also pinned to what the reference's own
+// tests hold: the finite-difference checks of
+// test/test_neohookean_accumulate.cpp, test_cosserat_accumulate.cpp and
+// test_one_sided_fixed_joint_accumulate.cpp (same inputs, same FD scheme,
 // test/finite_difference.hpp), and the Karras-2012 radix-tree example of
-// test/test_lbvh.cpp:38-47 (topology derived by hand from the published
-// figure).  Build flags disable FMA contraction (-ffp-contract=off) so that the
-// FP64 Morton codes are reproducible operation by operation.
+// test/test_lbvh.cpp:38-47.  Build flags disable FMA contraction
+// (-ffp-contract=off) so that the FP64 Morton codes are reproducible
+// operation by operation.
 
 #include <algorithm>
 #include <cmath>

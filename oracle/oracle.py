@@ -2,9 +2,9 @@
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py, always as the checker.  The engine never loads
-this module.  Parity of the oracle against the reference binary is unpinned
-(the reference needs Eigen3, which is absent); see the header of
-avbd_oracle.cpp for what pins it.
+this module.  The oracle is pinned to the reference implementation itself
+(compiled from its own sources into oracle/_ref, see oracle/ref.py and
+tests/test_ref_pinning.py); the header of avbd_oracle.cpp lists the pins.
 
 The method names mirror the engine's Python facade (avbd_b200.Context), so a
 scene description can be loaded into either with the same calls.
