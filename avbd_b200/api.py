@@ -318,6 +318,13 @@ class Context:
         return {"key": keys, "tri": idx[:, :3], "rod": idx[:, 3:5], "normal": vec[:, 0:3], "barys": vec[:, 3:6],
                 "cp_local": vec[:, 6:9], "s": vec[:, 9]}
 
+    def scene_iterations(self):
+        """Iterations each scene ran in the last run-to-tolerance step."""
+        st = self.stats()
+        out = np.zeros(st["num_scenes"], dtype=np.uint32)
+        check(self.L.avbd_get_scene_iterations(self.h, _up(out)))
+        return out
+
     def set_pair_capacity(self, capacity):
         check(self.L.avbd_debug_set_pair_capacity(self.h, int(capacity)))
 

@@ -1748,6 +1748,16 @@ int avbd_warmstart_sample(avbd_ctx* c, void* features, float* targets, unsigned*
     return device_error(c);
 }
 
+int avbd_get_scene_iterations(avbd_ctx* c, unsigned* iterations) {
+    if (int r = check_ctx(c)) return r;
+    if (!iterations) return fail(AVBD_ERR_INVALID_ARG, "null output");
+    if (!c->finalized || !c->d_scene_iters) return fail(AVBD_ERR_STATE, "no run-to-tolerance step has run");
+    CUDA_OR_FAIL(cudaMemcpyAsync(iterations, c->d_scene_iters, sizeof(uint32_t) * c->num_scenes,
+                                 cudaMemcpyDeviceToHost, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return AVBD_OK;
+}
+
 int avbd_residual(avbd_ctx* c, double* residual) {
     if (int r = check_ctx(c)) return r;
     if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");

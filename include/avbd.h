@@ -344,6 +344,12 @@ AVBD_API int avbd_debug_block(avbd_ctx* ctx, unsigned p, double* G, double* H, i
  * sqrt(sum_v |m g|^2)), FP64 reduction on the device. */
 AVBD_API int avbd_residual(avbd_ctx* ctx, double* residual);
 
+/* Run-to-tolerance steps: the iterations each scene ran in the last step
+ * (num_scenes entries, scene order of avbd_begin_scene).  The reference has
+ * no tolerance mode; its counterpart is the fixed solver_iters of every
+ * step (simulation/VBDSolver.hpp:64). */
+AVBD_API int avbd_get_scene_iterations(avbd_ctx* ctx, unsigned* iterations);
+
 /* No counterpart in the reference.  Morton codes and the stable sorted order
  * of an LBVH build for caller-provided primitive boxes, allocating nothing:
  * for callers that must not allocate device memory while they run (a loop

@@ -2604,6 +2604,12 @@ void orc_element_accumulate(void* h, int type, unsigned slot, unsigned local, do
 double orc_residual(void* h) { return residual(*(Ctx*)h); }
 double orc_last_residual(void* h) { return ((Ctx*)h)->last_residual; }
 unsigned long long orc_iterations(void* h) { return ((Ctx*)h)->iterations; }
+// iterations each scene ran in the last run-to-tolerance step
+unsigned orc_scene_iterations(void* h, unsigned* out) {
+    Ctx& c = *(Ctx*)h;
+    for (size_t s = 0; s < c.scene_iters.size(); s++) out[s] = c.scene_iters[s];
+    return (unsigned)c.scene_iters.size();
+}
 
 // Math::Exp_s3 / Log_S3 / QuaternionFromXYZEulerAngles for test inputs
 void orc_exp_s3(const double* v, double* q) {

@@ -98,6 +98,7 @@ def lib():
             "orc_residual": (C.c_double, [vp]),
             "orc_last_residual": (C.c_double, [vp]),
             "orc_iterations": (C.c_ulonglong, [vp]),
+            "orc_scene_iterations": (C.c_uint, [vp, up]),
             "orc_exp_s3": (None, [dp, dp]),
             "orc_quat_from_xyz_euler": (None, [dp, dp]),
             "orc_plus_s3": (None, [dp, dp, dp]),
@@ -429,3 +430,9 @@ class Oracle:
     @property
     def iterations(self):
         return self.L.orc_iterations(self.h)
+
+    def scene_iterations(self):
+        """Iterations each scene ran in the last run-to-tolerance step."""
+        buf = np.zeros(1 << 16, dtype=np.uint32)
+        n = self.L.orc_scene_iterations(self.h, _p(buf, C.c_uint))
+        return buf[:n].copy()

@@ -78,6 +78,7 @@ def lib():
             "ref_add_spheres": (C.c_uint, [vp, C.c_uint, up, dp, up]),
             "ref_finalize": (C.c_int, [vp]),
             "ref_step": (C.c_int, [vp, C.c_uint]),
+            "ref_set_iterations": (C.c_int, [vp, C.c_uint]),
             "ref_time_steps": (C.c_double, [vp, C.c_uint]),
             "ref_num_particles": (C.c_uint, [vp]),
             "ref_get_positions": (None, [vp, dp]),
@@ -251,6 +252,10 @@ class RefSim:
     # ---- stepping and queries
     def step(self, n=1):
         self._check(self.L.ref_step(self.h, n))
+
+    def set_iterations(self, iters):
+        """The fixed iteration count of the following steps."""
+        self._check(self.L.ref_set_iterations(self.h, int(iters)))
 
     def time_steps(self, n) -> float:
         t = self.L.ref_time_steps(self.h, n)

@@ -284,6 +284,24 @@ int ref_finalize(void* h) {
     });
 }
 
+// The iteration count of the following steps.  VBDSolver takes it at
+// construction (simulation/VBDSolver.hpp:37-42), so the executor is built
+// again; its collision detector then starts without the previous step's
+// detections, which matters only to scenes with dynamic contacts.
+int ref_set_iterations(void* h, unsigned iters) {
+    Ref& r = *(Ref*)h;
+    if (!r.finalized) {
+        g_err = "finalize first";
+        return 1;
+    }
+    if (iters == r.iters) return 0;
+    REF_TRY({
+        r.iters = iters;
+        r.exec.reset();
+        r.exec = std::make_unique<Sim::SimulationExecutor>(r.ctx.get(), r.iters, r.rho, r.threads);
+    });
+}
+
 int ref_step(void* h, unsigned n) {
     Ref& r = *(Ref*)h;
     if (!r.finalized) {

@@ -1,0 +1,121 @@
+"""Parity at the benchmark configurations' own sizes, engine vs the FP64
+oracle (which tests/test_ref_pinning.py pins to the reference itself).
+
+* C4 -- the batch the headline times: scenes 0-7 of the seed-0 1024-cube
+  batch (n from 13 to 24 cells, E from 4e4 to 4e6; scene 7 is n = 20,
+  E = 2.1e6), run to R <= 1e-4 with at most 100 iterations, in the MIXED
+  precision the bench uses and in FP64: identical colors, every scene's
+  iteration count within 2 of the oracle's in every step, positions within
+  1e-6 (MIXED) / 1e-9 (FP64) of the bounding-box diagonal.
+* C2 -- the 32^3 cube (35,937 vertices, 196,608 tets, 12,288 surface
+  triangles, E 1e6, nu 0.49) dropped on the ground: the collision stage of
+  each of the first steps, fed the oracle's state, is identical bit for bit
+  (codes, order, tree, bounds, pairs; 12,288 primitives is above the
+  reference's 5,000-primitive parallel-refit threshold); positions of the
+  FP64 engine within 1e-9 and of the FP32 engine within the stated bound of
+  the oracle over 60 steps.
+* C3 -- 256 rods of 100 segments on one-sided fixed joints plus 64 spheres,
+  rigid-body ground contact, 20 iterations: identical colors, FP64 and MIXED
+  positions within 1e-9, quaternions within 1e-8, over 20 steps.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from avbd_b200 import Context, scenes
+
+pytestmark = pytest.mark.gpu
+
+THREADS = min(32, os.cpu_count() or 1)
+
+
+def _pair(oracle_lib, sc, precision, **kw):
+    e = Context()
+    sc.load(e, precision=precision, **kw)
+    e.finalize()
+    o = oracle_lib.Oracle(threads=THREADS)
+    sc.load(o, **kw)
+    o.finalize()
+    return e, o
+
+
+def quat_err(a, b):
+    s = np.sign(np.sum(a * b, axis=1, keepdims=True))
+    s[s == 0] = 1
+    return np.abs(a - s * b).max()
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 1e-6), ("fp64", 1e-9)])
+def test_c4_batch_sample_to_tolerance(oracle_lib, precision, tol):
+    sc = scenes.batched_cubes(num_scenes=1024, seed=0, scene_ids=range(8), iters=15)
+    assert max(sc.meta["cells"]) >= 20
+    e, o = _pair(oracle_lib, sc, precision, residual_tolerance=1e-4, max_iters=100)
+    ce, nce = e.coloring()
+    co, nco = o.coloring()
+    assert nce == nco and (ce == co).all()
+    diag = sc.bbox_diagonal()
+    for step in range(6):
+        e.step(1)
+        o.step(1)
+        ie, io = e.scene_iterations(), o.scene_iterations()
+        assert len(ie) == len(io) == 8
+        assert np.abs(ie.astype(int) - io.astype(int)).max() <= 2, (step, ie, io)
+        err = np.abs(e.positions() - o.positions()).max() / diag
+        assert err <= tol, f"step {step + 1}: {err:.2e} of the diagonal"
+    assert e.stats()["last_residual"] <= 1e-4 or e.stats()["capped_scene_steps"] > 0
+
+
+def test_c2_collision_stage_bit_exact_at_size(oracle_lib):
+    sc = scenes.cube_drop(n=32, surface=True)
+    assert sc.num_primitives == 12288
+    e, o = _pair(oracle_lib, sc, "fp64")
+    for step in range(4):
+        o.collision_stage()
+        e.set_positions(0, o.positions())
+        e.set_velocities(0, o.velocities())
+        e.collision_stage()
+        ge, go = e.lbvh(), o.lbvh(sc.num_primitives)
+        for k in ("morton", "sorted_order", "left", "right", "parent", "subtree_size"):
+            assert (ge[k] == go[k]).all(), (step, k)
+        assert ge["root"] == go["root"]
+        assert (ge["bounds"] == go["bounds"]).all(), step
+        assert np.array_equal(ge["pairs"], go["pairs"]), step
+        o.step(1)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-3)])
+def test_c2_trajectory_at_size(oracle_lib, precision, tol):
+    """FP32 bar: the cube lands at step ~18; after that, friction switches
+    between stick and slip on per-vertex thresholds, and FP32 rounding of
+    ~1e-7 m moves individual switches (the oracle fed FP32-rounded inputs
+    drifts the same way); 2e-3 of the diagonal bounds the 60-step drift."""
+    sc = scenes.cube_drop(n=32, surface=True)
+    e, o = _pair(oracle_lib, sc, precision)
+    diag = sc.bbox_diagonal()
+    worst = []
+    for step in range(1, 61):
+        e.step(1)
+        o.step(1)
+        if step in (1, 10, 20, 30, 45, 60):
+            err = np.abs(e.positions() - o.positions()).max() / diag
+            worst.append((step, err))
+            assert err <= tol, f"step {step}: {err:.2e} of the diagonal ({precision})"
+    print(precision, worst)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_c3_rods_at_size(oracle_lib, precision):
+    sc = scenes.rods_and_spheres(num_rods=256, segments=100, num_spheres=64, seed=0)
+    e, o = _pair(oracle_lib, sc, precision)
+    ce, nce = e.coloring()
+    co, nco = o.coloring()
+    assert nce == nco and (ce == co).all()
+    diag = sc.bbox_diagonal()
+    for step in range(1, 21):
+        e.step(1)
+        o.step(1)
+        if step in (1, 5, 10, 20):
+            err = np.abs(e.positions() - o.positions()).max() / diag
+            assert err <= 1e-9, f"step {step}: {err:.2e}"
+            assert quat_err(e.rotations(), o.rotations()) <= 1e-8, step
