@@ -103,6 +103,7 @@ SIGNATURES = {
     "avbd_residual": [_vp, _dp],
     "avbd_get_scene_iterations": [_vp, _up],
     "avbd_profile_solve": [_vp, C.c_uint, _dp, _dp, _up],
+    "avbd_profile_step": [_vp, _dp, _dp, _up, _up],
     "avbd_lbvh_morton_sort_noalloc": [_vp, C.c_uint, _vp, _vp, _vp],
     "avbd_gemm_bf16": [_vp, C.c_uint, _vp, C.c_uint, _vp, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, _vp],
     "avbd_mlp_create": [C.POINTER(_vp), C.c_int, _fp],

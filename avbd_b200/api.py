@@ -368,6 +368,14 @@ class Context:
         check(self.L.avbd_profile_solve(self.h, iterations, C.byref(ms), C.byref(b), C.byref(nl)))
         return ms.value, b.value, nl.value
 
+    def profile_step(self):
+        """One run-to-tolerance step with the timed step's launches: kernel
+        time (ms) and algorithmic bytes of its vertex-solve launches, the
+        launch count and the iterations (advances the state)."""
+        ms, b, nl, it = C.c_double(0), C.c_double(0), C.c_uint(0), C.c_uint(0)
+        check(self.L.avbd_profile_step(self.h, C.byref(ms), C.byref(b), C.byref(nl), C.byref(it)))
+        return ms.value, b.value, nl.value, it.value
+
     def stats(self):
         s = Stats()
         check(self.L.avbd_get_stats(self.h, C.byref(s)))

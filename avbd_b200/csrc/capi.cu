@@ -466,16 +466,24 @@ int upload_state(avbd_ctx* c, DevState<R>& s, const std::vector<unsigned>& inc_o
         begin[i + 1] = begin[i] + (solved ? inc_off[e + 1] - inc_off[e] : 0);
     }
     const size_t nrec = begin[n];
-    // algorithmic bytes of each color's solve launch
+    // algorithmic bytes of each color's solve launch, and of each scene's
+    // part of it (the pieces a run-to-tolerance sweep launches per scene)
     c->color_bytes.assign(c->num_colors, 0.0);
     {
         const double V4B = sizeof(V4), RECB = sizeof(IncRec<RS>);
         const double ground_b = c->ground.empty() ? 0.0 : 3 * V4B + 1;
+        std::vector<unsigned> sb = c->scene_begin;
+        if (sb.back() != n) sb.push_back(n);
+        const unsigned S = (unsigned)sb.size() - 1;
+        c->color_scene_bytes.assign((size_t)c->num_colors * S, 0.0);
         for (unsigned col = 0; col < c->num_colors; col++) {
             double b = 0;
             for (unsigned i = c->color_begin[col]; i < c->color_begin[col] + c->color_solve[col]; i++) {
-                b += 3 * V4B + 2 * sizeof(uint32_t) + 1 + RECB * (begin[i + 1] - begin[i]);
-                if (flags[i] & VF_GROUND) b += ground_b;
+                double bi = 3 * V4B + 2 * sizeof(uint32_t) + 1 + RECB * (begin[i + 1] - begin[i]);
+                if (flags[i] & VF_GROUND) bi += ground_b;
+                b += bi;
+                const unsigned sc = (unsigned)(std::upper_bound(sb.begin(), sb.end(), c->perm[i]) - sb.begin()) - 1;
+                c->color_scene_bytes[(size_t)col * S + sc] += bi;
             }
             c->color_bytes[col] = b;
         }
@@ -1559,6 +1567,103 @@ int avbd_debug_block(avbd_ctx* c, unsigned p, double* G, double* H, int* dof) {
     for (int i = 0; i < d * d; i++) H[i] = h[d + i];
     if (dof) *dof = d;
     return AVBD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One run-to-tolerance step with the launches the timed step uses (the
+// per-scene pieces of every color slab, converged scenes gated out), driven
+// from the host like the graph-less path, with CUDA events around every
+// color's sweep launch.  Bytes: the algorithmic bytes of the scenes still
+// iterating when each sweep starts.
+template <typename R>
+int profile_step_impl(avbd_ctx* c, DevState<R>& s, double* solve_ms, double* solve_bytes, unsigned* launches,
+                      unsigned* iterations) {
+    StepConsts k = consts(c);
+    cudaStream_t st = c->stream;
+    const unsigned max_it = c->solver.max_iters ? c->solver.max_iters : 1000;
+    const double tol = c->solver.residual_tolerance;
+    const unsigned S = c->num_scenes, nc = c->num_colors;
+    SceneTol solveT{c->d_scene, c->d_scene_active, nullptr, c->d_scene_r2, nullptr};
+    SceneTol resT{c->d_scene, nullptr, c->d_scene_cand, nullptr, c->d_scene_ex};
+    std::vector<uint8_t> act(S);
+    std::vector<cudaEvent_t> ev(2ull * nc);
+    for (auto& e : ev) CUDA_OR_FAIL(cudaEventCreate(&e));
+    double ms = 0, bytes = 0;
+    unsigned nl = 0, it = 0;
+    int rc = enqueue_begin<R>(c, s, k, st);
+    if (!rc) launch_tol_init(c, st);
+    double omega = 1;
+    for (; !rc && it < max_it; it++) {
+        omega = omega_at(it, c->solver.iter_acceleration, omega);
+        if (cudaMemcpyAsync(act.data(), c->d_scene_active, S, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = fail(AVBD_ERR_CUDA, "profile: scene flags");
+            break;
+        }
+        for (unsigned col = 0; col < nc; col++) {
+            cudaEventRecord(ev[2 * col], st);
+            if (c->color_solve[col]) {
+                const unsigned r0 = c->solve_range_off[col], r1 = c->solve_range_off[col + 1];
+                launch_solve_color<R>(c, s, k, 0, 0, st, solveT, nullptr, c->d_solve_ranges + r0, r1 - r0);
+                nl++;
+                for (unsigned sc = 0; sc < S; sc++)
+                    if (act[sc]) bytes += c->color_scene_bytes[(size_t)col * S + sc];
+            }
+            cudaEventRecord(ev[2 * col + 1], st);
+            if (c->color_orient[col])
+                launch_solve_rod<R>(c, s, k, c->color_begin[col] + c->color_solve[col], c->color_orient[col], st,
+                                    solveT, 0, nullptr);
+        }
+        enqueue_chebyshev<R>(c, s, k, omega, it, st, solveT);
+        launch_tol_decide_a(c, tol, st);
+        enqueue_residual<R>(c, s, k, nullptr, st, resT);
+        launch_tol_decide_b(c, tol, max_it, st);
+        int n_active = 0;
+        if (cudaMemcpyAsync(&n_active, c->d_tol_count, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = fail(AVBD_ERR_CUDA, "profile: iteration count");
+            break;
+        }
+        for (unsigned col = 0; col < nc; col++) {
+            float t = 0;
+            if (cudaEventElapsedTime(&t, ev[2 * col], ev[2 * col + 1]) == cudaSuccess) ms += t;
+        }
+        if (n_active == 0) {
+            it++;
+            break;
+        }
+    }
+    if (!rc) enqueue_velocity<R>(c, s, k, st);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    CUDA_OR_FAIL(cudaGetLastError());
+    CUDA_OR_FAIL(cudaStreamSynchronize(st));
+    if (solve_ms) *solve_ms = ms;
+    if (solve_bytes) *solve_bytes = bytes;
+    if (launches) *launches = nl;
+    if (iterations) *iterations = it;
+    return AVBD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int avbd_profile_step(avbd_ctx* c, double* solve_ms, double* solve_bytes, unsigned* launches,
+                      unsigned* iterations) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (c->solver.residual_tolerance <= 0 || !c->d_solve_ranges || c->dyn)
+        return fail(AVBD_ERR_STATE, "avbd_profile_step profiles run-to-tolerance steps of contexts without dynamic "
+                                    "contacts");
+    CUDA_OR_FAIL(cudaSetDevice(c->device));
+    int rc = use64(c) ? profile_step_impl<double>(c, c->d, solve_ms, solve_bytes, launches, iterations)
+                      : profile_step_impl<float>(c, c->f, solve_ms, solve_bytes, launches, iterations);
+    if (rc) return rc;
+    return device_error(c);
 }
 
 int avbd_profile_solve(avbd_ctx* c, unsigned iterations, double* solve_ms, double* solve_bytes,

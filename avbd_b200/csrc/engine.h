@@ -242,6 +242,7 @@ struct avbd_ctx {
     std::vector<unsigned> color_solve;  // vertices of the slab that run the 3-DOF solve
     std::vector<unsigned> color_orient; // oriented non-fixed vertices after them (6-DOF solve)
     std::vector<double> color_bytes;    // algorithmic bytes of each color's solve launch
+    std::vector<double> color_scene_bytes;  // [color][scene]: each scene's part of it
     unsigned max_color_solve = 0;
 
     avbd::DevState<float> f;

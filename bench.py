@@ -34,8 +34,12 @@ Prints one JSON line.  `value` is scene-steps/s over all ranks with the state
 resident in HBM; `e2e` repeats the measurement through the C-ABI with the
 state uploaded from pinned host memory and the positions read back every
 step; `roofline` reports the per-color vertex-solve kernel against the
-measured HBM bandwidth; `cpu_baseline` times the FP64 oracle port on the
-host cores on a sample of the same batch.
+measured HBM bandwidth on the launches a timed step uses; `cpu_baseline`
+times the reference's own CPU solver (compiled from its sources into
+oracle/_ref; the FP64 port where that library is absent) on the host cores,
+on a stratified sample of the same batch, each scene-step running the
+iterations the residual needs.  `--impl reference` prints that measurement
+over the same --steps / --warmup window as its own line.
 """
 from __future__ import annotations
 
@@ -66,7 +70,6 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--tol", type=float, default=1e-4)
     p.add_argument("--max-iters", type=int, default=100)
-    p.add_argument("--cpu-sample-scenes", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision", default=None, choices=["fp32", "mixed", "fp64"],
@@ -111,15 +114,6 @@ class Workload:
             self.unit = UNIT
             self.tol, self.max_iters = args.tol, args.max_iters
             self.method = "plain AVBD (no warm start)"
-
-    def sample(self, args, seed):
-        """The bounded sample the CPU baseline times, and its unit count."""
-        from avbd_b200 import scenes
-        if self.single:
-            return self.scene, 1, "the same scene"
-        S = args.cpu_sample_scenes
-        return (scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=range(S)), S,
-                f"{S} of {args.scenes} scenes of the same batch")
 
 
 def measured_bf16():
@@ -205,19 +199,121 @@ def traffic_for(workload: str):
         return None
 
 
-def cpu_sample(args, wl, seed, threads):
-    """FP64 oracle port on a bounded sample of the workload: units/s."""
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def stratified_sample(num_scenes, seed, size, pick_seed=20251):
+    """Scenes of the batch in 8 strata (cells per side 4-8 / 9-13 / 14-18 /
+    19-24 x E below / above 10^5.5); each stratum gets a share of the sample
+    proportional to its population (at least one scene), drawn with a fixed
+    generator.  Returns the scene ids and each one's weight (the stratum's
+    population over its sampled count), so that sum(weight * t) estimates a
+    per-scene total over the whole batch."""
+    import numpy as np
+    from avbd_b200.scenes import batched_cube_params
+    strata = {}
+    for s in range(num_scenes):
+        n, E, _, _ = batched_cube_params(seed, s)
+        strata.setdefault((min(3, (n - 4) // 5), int(np.log10(E) >= 5.5)), []).append(s)
+    keys = sorted(strata)
+    size = max(size, len(keys))
+    share = {k: max(1, int(round(size * len(strata[k]) / num_scenes))) for k in keys}
+    rng = np.random.default_rng(pick_seed)
+    ids, weights = [], []
+    for k in keys:
+        m = min(share[k], len(strata[k]))
+        for s in sorted(rng.choice(strata[k], size=m, replace=False).tolist()):
+            ids.append(int(s))
+            weights.append(len(strata[k]) / m)
+    return ids, weights
+
+
+def reference_batch(args, seed, warmup, steps, workers):
+    """The reference's own CPU solver (oracle/_ref, compiled from its sources)
+    on a stratified sample of the batch, each scene in its own
+    SimulationContext, `workers` scenes at a time on the host cores.
+
+    The reference has no residual: it runs a fixed iteration count.  Each
+    sampled scene's step therefore runs exactly the iterations that this
+    project's residual (evaluated by the FP64 port, which matches the
+    reference's trajectory to 1e-12) needs to reach the tolerance in that step,
+    at most max_iters -- the same count the GPU runs.  Steps 1..warmup run
+    untimed, steps warmup+1..warmup+steps are timed (wall clock per step).
+    Without oracle/_ref (no reference sources where it was built) the FP64
+    port itself is timed.  Returns the line's fields."""
+    import concurrent.futures as cf
+    import numpy as np
+    from avbd_b200 import scenes
+    from oracle import ref
     from oracle.oracle import Oracle
-    sc, S, what = wl.sample(args, seed)
-    o = Oracle(threads=threads)
-    sc.load(o, residual_tolerance=wl.tol, max_iters=wl.max_iters)
-    o.finalize()
-    o.step(1)  # warm-up (first contact step)
-    steps, t = 0, 0.0
-    while t < args.cpu_seconds and steps < 200:
-        t += o.time_steps(1)
-        steps += 1
-    return S * steps / t, what, steps, t
+    ids, weights = stratified_sample(args.scenes, seed, max(8, workers))
+    total = warmup + steps
+
+    def counts(s):  # iterations each step needs (untimed)
+        sc = scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=[s])
+        o = Oracle()
+        sc.load(o, residual_tolerance=args.tol, max_iters=args.max_iters)
+        o.finalize()
+        out = []
+        for _ in range(total):
+            o.step(1)
+            out.append(int(o.scene_iterations()[0]))
+        return out
+
+    use_ref = ref.available()
+
+    def timed(s, its):
+        sc = scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=[s])
+        if use_ref:
+            r = ref.RefSim(sc)
+            sc.load(r)
+            r.finalize()
+        else:
+            r = Oracle()
+            sc.load(r, residual_tolerance=args.tol, max_iters=args.max_iters)
+            r.finalize()
+        t = 0.0
+        for k, it in enumerate(its):
+            if use_ref:
+                r.set_iterations(it)
+            dt = r.time_steps(1)
+            if k >= warmup:
+                t += dt
+        verts = sc.num_particles
+        if use_ref:
+            r.close()
+        return t / steps, verts
+
+    t0 = time.time()
+    with cf.ThreadPoolExecutor(workers) as ex:
+        its = list(ex.map(counts, ids))
+        res = list(ex.map(timed, ids, its))
+    wall = time.time() - t0
+    w = np.asarray(weights)
+    t_scene = np.array([r[0] for r in res])            # s per step, one core
+    verts = np.array([r[1] for r in res], dtype=np.float64)
+    it_mean = np.array([np.mean(i[warmup:]) for i in its])
+    T1 = float((w * t_scene).sum())                   # one batch step on one core
+    value = args.scenes * workers / T1                 # scene-steps/s on `workers` cores
+    capped = np.array([np.mean([x >= args.max_iters for x in i[warmup:]]) for i in its])
+    return {
+        "value": value,
+        "iterations_per_scene_step": float((w * it_mean).sum() / w.sum()),
+        "vertex_iterations_per_s": float((w * verts * it_mean).sum() * workers / T1),
+        "capped_fraction": float((w * capped).sum() / w.sum()),
+        "kind": "reference" if use_ref else "port",
+        "cores": workers,
+        "sample": (f"{len(ids)} of {args.scenes} scenes of the same batch, stratified by size and stiffness "
+                   f"(weights = stratum population / sampled), steps {warmup + 1}-{total} of each "
+                   f"({steps} timed), each step running the iterations the residual needs (<= {args.max_iters}); "
+                   f"{'the reference compiled from its own sources' if use_ref else 'the FP64 port'}, "
+                   f"{workers} scenes at a time; {wall:.0f} s wall"),
+        "scene_ids": ids,
+    }
 
 
 def run_reference(args):
@@ -225,26 +321,46 @@ def run_reference(args):
     rank, world, _ = dist.env()
     if rank != 0:
         return
-    threads = min(os.cpu_count() or 1, 32)
-    from oracle.oracle import Oracle
+    workers = min(host_cores(), 32)
     wl = Workload(args, args.seed)
-    sc, S, what = wl.sample(args, args.seed)
-    o = Oracle(threads=threads)
-    sc.load(o, residual_tolerance=wl.tol, max_iters=wl.max_iters)
-    o.finalize()
-    for _ in range(args.warmup):
-        o.step(1)
-    t = o.time_steps(args.steps)
-    v = S * args.steps / t
-    sample = f"{what}, {args.steps} steps, FP64 oracle port, {threads} threads"
+    if wl.single:
+        v, kind, sample, it_ps = single_scene_reference(args, wl, args.warmup, args.steps, workers)
+        extra = {}
+    else:
+        rb = reference_batch(args, args.seed, args.warmup, args.steps, workers)
+        v, kind, sample = rb["value"], rb["kind"], rb["sample"]
+        extra = {k: rb[k] for k in ("iterations_per_scene_step", "vertex_iterations_per_s", "capped_fraction",
+                                    "scene_ids")}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": wl.unit, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wl.units / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wl.name, "units_timed": S,
-                       "residual_tolerance": wl.tol, "max_iters": wl.max_iters},
-            "cpu_baseline": {"value": v, "unit": wl.unit, "cores": threads, "kind": "port", "sample": sample},
+            "config": {"workload": wl.name, "residual_tolerance": wl.tol, "max_iters": wl.max_iters, **extra},
+            "cpu_baseline": {"value": v, "unit": wl.unit, "cores": workers, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def single_scene_reference(args, wl, warmup, steps, threads):
+    """The reference (or, without oracle/_ref, the FP64 port) on the
+    single-scene workloads, with its own worker threads: steps/s."""
+    from oracle import ref
+    from oracle.oracle import Oracle
+    sc = wl.scene
+    if ref.available():
+        r = ref.RefSim(sc, threads=threads)
+        kind = "reference"
+    else:
+        r = Oracle(threads=threads)
+        kind = "port"
+    sc.load(r)
+    r.finalize()
+    r.step(max(1, warmup))
+    n, t = 0, 0.0
+    while n < steps and (t < args.cpu_seconds or n == 0):
+        t += r.time_steps(1)
+        n += 1
+    what = "the reference compiled from its own sources" if kind == "reference" else "the FP64 port"
+    return n / t, kind, f"the same scene, {n} steps after {max(1, warmup)} untimed, {what}, {threads} threads", None
 
 
 def make_context(wl, args, local, stream):
@@ -256,14 +372,18 @@ def make_context(wl, args, local, stream):
     return e
 
 
-def time_steps(e, stream, steps, flush=None):
+def time_steps(e, stream, steps, flush=None, scene_verts=None):
     """Device time (ms) of `steps` steps on the engine's stream, with the
     counters they moved.  With `flush` (a tensor larger than L2) every step
-    is preceded by a write of it and timed alone."""
+    is preceded by a write of it and timed alone.  With `scene_verts` (the
+    vertex count of every scene of a run-to-tolerance batch) each step's
+    per-scene iteration counts are read after it (outside its events) and
+    summed into vertex-iterations."""
     import numpy as np
     import torch
     st0 = e.stats()
     evs = []
+    vert_it = 0.0
     for _ in range(steps):
         if flush is not None:
             with torch.cuda.stream(stream):
@@ -273,12 +393,15 @@ def time_steps(e, stream, steps, flush=None):
         e.step(1)
         b.record(stream)
         evs.append((a, b))
+        if scene_verts is not None:
+            vert_it += float((e.scene_iterations().astype(np.float64) * scene_verts).sum())
     stream.synchronize()
     per = [a.elapsed_time(b) for a, b in evs]
     ms = sum(per)
     st1 = e.stats()
     d = {k: st1[k] - st0[k] for k in ("kernel_launches", "iterations", "capped_scene_steps", "warmstart_applied")}
     d["p50_ms"], d["p99_ms"] = float(np.percentile(per, 50)), float(np.percentile(per, 99))
+    d["vertex_iterations"] = vert_it
     return ms, d
 
 
@@ -375,8 +498,9 @@ def run_engine(args):
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
-    ms_plain, c_plain = time_steps(ep, stream, args.steps, flush)
-    ms_learn, c_learn = time_steps(el, stream, args.steps, flush) if el is not None else (None, None)
+    verts = None if wl.single else np.array([(c + 1) ** 3 for c in sc.meta["cells"]], dtype=np.float64)
+    ms_plain, c_plain = time_steps(ep, stream, args.steps, flush, verts)
+    ms_learn, c_learn = time_steps(el, stream, args.steps, flush, verts) if el is not None else (None, None)
     dist.barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -391,8 +515,14 @@ def run_engine(args):
     clk_e2e = clocks_e2e.stop()
     dist.barrier()
 
-    # ---- rooflines: the per-color vertex solve, and the MLP on the tensor cores
-    solve_ms, solve_bytes, solve_launches = ep.profile_solve(2)
+    # ---- rooflines: the per-color vertex solve on the launches the timed step
+    # uses (run-to-tolerance: per-scene pieces, converged scenes gated out;
+    # fixed iterations: whole color slabs), and the MLP on the tensor cores
+    if wl.tol > 0:
+        solve_ms, solve_bytes, solve_launches, prof_iters = ep.profile_step()
+    else:
+        solve_ms, solve_bytes, solve_launches = ep.profile_solve(2)
+        prof_iters = 2
     ep.synchronize()
     peak, peak_kind = measured_peaks()
     roof_mlp = mlp_roofline(el, n, local, measured_bf16()) if el is not None else None
@@ -412,24 +542,37 @@ def run_engine(args):
                   else "k_solve_tet (per-color vertex block solve)")
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic_for(workload), "kernel": kernel,
-                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "peak_source": peak_kind}
+                "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "peak_source": peak_kind,
+                "launch_shape": ("one run-to-tolerance step as timed: per-scene pieces of every color slab, "
+                                 f"converged scenes gated out ({solve_launches} launches, {prof_iters} iterations)"
+                                 if wl.tol > 0 else f"whole color slabs ({solve_launches} launches, "
+                                 f"{prof_iters} iterations)")}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            threads = min(os.cpu_count() or 1, 32)
-            v_cpu, what, steps, t = cpu_sample(args, wl, seed, threads)
-            cpu = {"value": v_cpu, "unit": wl.unit, "cores": threads, "kind": "port",
-                   "sample": f"{what}, {steps} steps in {t:.1f} s, FP64 oracle port"}
+            workers = min(host_cores(), 32)
+            if wl.single:
+                v_cpu, kind, what, _ = single_scene_reference(args, wl, args.warmup, 3, workers)
+                cpu = {"value": v_cpu, "unit": wl.unit, "cores": workers, "kind": kind, "sample": what}
+            else:
+                rb = reference_batch(args, seed, args.warmup, min(args.steps, 3), workers)
+                cpu = {"value": rb["value"], "unit": wl.unit, "cores": workers, "kind": rb["kind"],
+                       "sample": rb["sample"], "iterations_per_scene_step": rb["iterations_per_scene_step"],
+                       "vertex_iterations_per_s": rb["vertex_iterations_per_s"]}
         su = args.steps * wl.units
-        arms = {"plain": {"value": value_plain, "ms_per_step": ms_plain_max / args.steps,
-                          "step_latency_ms": {"p50": c_plain["p50_ms"], "p99": c_plain["p99_ms"]},
-                          "iterations_per_scene_step": c_plain["iterations"] / su,
-                          "capped_fraction": c_plain["capped_scene_steps"] / su if wl.tol > 0 else None}}
+        def arm(val, ms_arm, c):
+            a = {"value": val, "ms_per_step": ms_arm / args.steps,
+                 "step_latency_ms": {"p50": c["p50_ms"], "p99": c["p99_ms"]},
+                 "iterations_per_scene_step": c["iterations"] / su}
+            if wl.tol > 0:
+                a["capped_fraction"] = c["capped_scene_steps"] / su
+                a["converged_scene_steps_per_s"] = val * (1 - c["capped_scene_steps"] / su)
+                a["vertex_iterations_per_s"] = c["vertex_iterations"] * world / (ms_arm / 1e3)
+            return a
+
+        arms = {"plain": arm(value_plain, ms_plain_max, c_plain)}
         if el is not None:
-            arms["learned"] = {"value": value, "ms_per_step": ms_max / args.steps,
-                               "step_latency_ms": {"p50": c_learn["p50_ms"], "p99": c_learn["p99_ms"]},
-                               "iterations_per_scene_step": c_learn["iterations"] / su,
-                               "capped_fraction": c_learn["capped_scene_steps"] / su,
-                               "corrections_applied_fraction": c_learn["warmstart_applied"] / (args.steps * n)}
+            arms["learned"] = arm(value, ms_max, c_learn)
+            arms["learned"]["corrections_applied_fraction"] = c_learn["warmstart_applied"] / (args.steps * n)
         method = (wl.method if el is None else
                   "learned warm start (MLP 27-128-128-128-3, BF16 tcgen05) + plain AVBD iterations")
         line = {

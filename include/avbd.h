@@ -381,6 +381,17 @@ AVBD_API int avbd_lbvh_morton_sort_noalloc(const double* aabb6, unsigned n, uint
 AVBD_API int avbd_profile_solve(avbd_ctx* ctx, unsigned iterations, double* solve_ms, double* solve_bytes,
                                 unsigned* launches);
 
+/* Measurement entry point (no counterpart in the reference): advances one
+ * run-to-tolerance step with exactly the launches a timed step uses (the
+ * per-scene pieces of each color slab, scenes that have converged gated
+ * out), driven from the host, with CUDA events around every color's
+ * vertex-solve launch.  Returns their summed time, the algorithmic bytes of
+ * the scenes still iterating when each launch started (per solved vertex as
+ * for avbd_profile_solve), the launches and the iterations the step ran.
+ * Contexts with dynamic contacts are refused (AVBD_ERR_STATE). */
+AVBD_API int avbd_profile_step(avbd_ctx* ctx, double* solve_ms, double* solve_bytes, unsigned* launches,
+                               unsigned* iterations);
+
 /* ------------------------------------------------ learned warm start
  * No counterpart in the reference (it has no learned component).  A
  * per-vertex MLP 27 -> 128 -> 128 -> 128 -> 3 with SiLU, BF16 weights and

@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -38,12 +39,29 @@ struct NullBuf : std::streambuf {
     std::streamsize xsputn(const char*, std::streamsize n) override { return n; }
 };
 
+// std::cout is one object per process: contexts stepping on several threads
+// share one muted period (the first to enter swaps the buffer, the last to
+// leave restores it).
 struct MuteCout {
-    NullBuf nb;
-    std::streambuf* old;
-    MuteCout() : old(std::cout.rdbuf(&nb)) {}
-    ~MuteCout() { std::cout.rdbuf(old); }
+    static std::mutex& mu() {
+        static std::mutex m;
+        return m;
+    }
+    static NullBuf nb;
+    static int depth;
+    static std::streambuf* old;
+    MuteCout() {
+        std::lock_guard<std::mutex> g(mu());
+        if (depth++ == 0) old = std::cout.rdbuf(&nb);
+    }
+    ~MuteCout() {
+        std::lock_guard<std::mutex> g(mu());
+        if (--depth == 0) std::cout.rdbuf(old);
+    }
 };
+NullBuf MuteCout::nb;
+int MuteCout::depth = 0;
+std::streambuf* MuteCout::old = nullptr;
 
 struct Ref {
     std::unique_ptr<Sim::SimulationContext> ctx;
