@@ -1076,9 +1076,11 @@ StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_acc
 template <typename R>
 int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     const char* env = getenv("AVBD_LANES");
-    if (env) {
+    const char* env_stage = getenv("AVBD_STAGE");
+    if (env) {  // a fixed launch shape: lanes, and (AVBD_STAGE=1) staged neighbour positions
         int l = atoi(env);
         if (l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32) c->lanes = l;
+        c->stage = env_stage && atoi(env_stage) != 0 && c->lanes <= 8;
         return AVBD_OK;
     }
     unsigned long long solved = 0;
@@ -1096,9 +1098,16 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     CUDA_OR_FAIL(cudaEventCreate(&b));
     const unsigned long long launches0 = c->stats.kernel_launches;
     int best = 8;
+    bool best_stage = false;
     float best_ms = 1e30f;
-    for (int l : {1, 2, 4, 8, 16}) {
+    // launch shapes: threads per vertex, and whether the neighbour positions
+    // are staged through shared memory (1-8 threads per vertex)
+    const int shapes[][2] = {{1, 0}, {1, 1}, {2, 0}, {2, 1}, {4, 0}, {4, 1}, {8, 0}, {8, 1}, {16, 0}};
+    for (const auto& sh : shapes) {
+        const int l = sh[0];
+        if (env_stage && (atoi(env_stage) != 0) != (sh[1] != 0)) continue;
         c->lanes = l;
+        c->stage = sh[1] != 0;
         for (int rep = 0; rep < 2; rep++) {  // rep 0 warms up, rep 1 is timed
             if (rep == 1) CUDA_OR_FAIL(cudaEventRecord(a, st));
             for (unsigned col = 0; col < c->num_colors; col++) {
@@ -1115,9 +1124,13 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
         CUDA_OR_FAIL(cudaEventSynchronize(b));
         float ms = 0;
         CUDA_OR_FAIL(cudaEventElapsedTime(&ms, a, b));
+        if (getenv("AVBD_TRACE"))
+            fprintf(stderr, "[avbd] autotune: %d threads per vertex%s: %.3f ms per sweep\n", l,
+                    c->stage ? ", staged neighbours" : "", ms);
         if (ms < best_ms) {
             best_ms = ms;
             best = l;
+            best_stage = c->stage;
         }
         CUDA_OR_FAIL(cudaMemcpyAsync(s.x, snap, sizeof(V4) * s.n, cudaMemcpyDeviceToDevice, st));
     }
@@ -1127,8 +1140,11 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     cudaEventDestroy(b);
     cudaFree(snap);
     c->lanes = best;
+    c->stage = best_stage;
     c->stats.kernel_launches = launches0;
-    if (getenv("AVBD_TRACE")) fprintf(stderr, "[avbd] autotune: %d threads per vertex (%.3f ms per sweep)\n", best, best_ms);
+    if (getenv("AVBD_TRACE"))
+        fprintf(stderr, "[avbd] autotune: %d threads per vertex%s (%.3f ms per sweep)\n", best,
+                best_stage ? ", staged neighbours" : "", best_ms);
     return AVBD_OK;
 }
 

@@ -290,6 +290,7 @@ struct avbd_ctx {
     bool graph_tol = false;
     bool use_graph = true;
     int lanes = 8;                      // threads per vertex in the tet solve
+    bool stage = false;                 // tet solve stages neighbour positions in shared memory
     int block = 256;
 
     // learned warm start (mlp.cu): 0 off, 1 record features/targets, 2 apply

@@ -72,6 +72,9 @@ def parse():
     p.add_argument("--max-iters", type=int, default=100)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--split", default="strong", choices=["strong", "weak"],
+                   help="multi-GPU batch_cubes: one batch split across the ranks by tets (strong), or one "
+                        "batch per rank with a rank-specific seed (weak)")
     p.add_argument("--precision", default=None, choices=["fp32", "mixed", "fp64"],
                    help="default: mixed for batch_cubes, fp32 for rods_spheres and contacts")
     p.add_argument("--workload", default="batch_cubes", choices=["batch_cubes", "rods_spheres", "contacts"])
@@ -87,8 +90,8 @@ def parse():
 class Workload:
     """The scene set one rank advances, and how its steps are counted."""
 
-    def __init__(self, args, seed):
-        from avbd_b200 import scenes
+    def __init__(self, args, seed, rank=0, world=1):
+        from avbd_b200 import dist, scenes
         self.rods = args.workload == "rods_spheres"
         self.contacts = args.workload == "contacts"
         self.single = self.rods or self.contacts   # one scene, fixed iterations, working set within L2
@@ -108,9 +111,12 @@ class Workload:
             self.method = ("plain AVBD with triangle-rod contacts (narrow phase, contact pool, "
                            "incremental recoloring), 20 fixed iterations per step")
         else:
-            self.scene = scenes.batched_cubes(num_scenes=args.scenes, seed=seed)
+            # strong scaling: this rank's tet-balanced part of one batch;
+            # weak scaling: a whole batch of this rank's own seed
+            ids = dist.batch_partition(args.scenes, seed, world)[rank] if args.split == "strong" else None
+            self.scene = scenes.batched_cubes(num_scenes=args.scenes, seed=seed, scene_ids=ids)
             self.name = f"batch{args.scenes}_cubes"
-            self.units = args.scenes
+            self.units = len(ids) if ids is not None else args.scenes
             self.unit = UNIT
             self.tol, self.max_iters = args.tol, args.max_iters
             self.method = "plain AVBD (no warm start)"
@@ -464,11 +470,11 @@ def run_engine(args):
     rank, world, local = dist.env()
     torch.cuda.set_device(local)
     dist.init("nccl")
-    seed = dist.shard_seed(args.seed, rank)
+    seed = dist.shard_seed(args.seed, rank) if args.split == "weak" else args.seed
     dev = torch.device("cuda", local)
 
     t0 = time.time()
-    wl = Workload(args, seed)
+    wl = Workload(args, seed, rank, world)
     sc = wl.scene
     n = sc.num_particles
     stream = torch.cuda.Stream(device=local)
@@ -518,8 +524,10 @@ def run_engine(args):
     # ---- rooflines: the per-color vertex solve on the launches the timed step
     # uses (run-to-tolerance: per-scene pieces, converged scenes gated out;
     # fixed iterations: whole color slabs), and the MLP on the tensor cores
+    sum_sweep_bytes = 0.0
     if wl.tol > 0:
         solve_ms, solve_bytes, solve_launches, prof_iters = ep.profile_step()
+        sum_sweep_bytes = ep.profile_solve(1)[1]   # one whole-slab sweep: every scene's data
     else:
         solve_ms, solve_bytes, solve_launches = ep.profile_solve(2)
         prof_iters = 2
@@ -529,9 +537,10 @@ def run_engine(args):
 
     red = dist.reduce([ms, ms_e2e, ms_plain], "max", device=dev)
     ms_max, ms_e2e_max, ms_plain_max = red
-    value = wl.units * world * args.steps / (ms_max / 1e3)
-    value_e2e = wl.units * world * args.steps / (ms_e2e_max / 1e3)
-    value_plain = wl.units * world * args.steps / (ms_plain_max / 1e3)
+    units_all = dist.reduce([float(wl.units)], "sum", device=dev)[0]   # scenes all ranks advance
+    value = units_all * args.steps / (ms_max / 1e3)
+    value_e2e = units_all * args.steps / (ms_e2e_max / 1e3)
+    value_plain = units_all * args.steps / (ms_plain_max / 1e3)
 
     if rank == 0:
         per_launch_ms = solve_ms / max(1, solve_launches)
@@ -577,15 +586,20 @@ def run_engine(args):
                   "learned warm start (MLP 27-128-128-128-3, BF16 tcgen05) + plain AVBD iterations")
         line = {
             "metric": METRIC, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong" if (args.split == "strong" and not wl.single) else "weak",
             "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
             "config": {"workload": workload, "scenes_per_gpu": wl.units, "vertices_per_gpu": n,
                        "tets_per_gpu": sc.num_tets, "residual_tolerance": wl.tol, "max_iters": wl.max_iters,
                        "method": method, "arms": arms, "precision": args.precision,
-                       "l2": (f"L2 flushed (256 MB write) before every timed step; {solve_bytes / 2 / 1e6:.1f} MB "
-                              "of solve data per iteration" if wl.single else
-                              f"inputs larger than L2: {solve_bytes / 2 / 1e9:.2f} GB of solve data per iteration"),
-                       "parallelism": f"dp{world} (independent scenes per GPU)", "setup_s": round(setup_s, 1)},
+                       "l2": (f"L2 flushed (256 MB write) before every timed step; "
+                              f"{solve_bytes / prof_iters / 1e6:.1f} MB of solve data per iteration" if wl.single else
+                              f"inputs larger than L2: {sum_sweep_bytes / 1e9:.2f} GB of solve data in a sweep of "
+                              "every scene"),
+                       "parallelism": (f"dp{world}: one batch split across the GPUs, balanced by tets"
+                                       if args.split == "strong" and not wl.single else
+                                       f"dp{world}: independent scenes per GPU"),
+                       "setup_s": round(setup_s, 1)},
             "clocks": clk, "gpu_launches": cnt["kernel_launches"],
             "e2e": {"value": value_e2e, "unit": wl.unit, "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
                     "iterations_per_scene_step": it_e2e / su, "clocks": clk_e2e},

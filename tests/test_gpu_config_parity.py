@@ -12,8 +12,9 @@ oracle (which tests/test_ref_pinning.py pins to the reference itself).
   each of the first steps, fed the oracle's state, is identical bit for bit
   (codes, order, tree, bounds, pairs; 12,288 primitives is above the
   reference's 5,000-primitive parallel-refit threshold); positions of the
-  FP64 engine within 1e-9 and of the FP32 engine within the stated bound of
-  the oracle over 60 steps.
+  FP64 engine within 1e-9 of the oracle over 60 steps, of the FP32 engine
+  within 1e-5 before touchdown and within 3x the oracle's own sensitivity to
+  an FP32 rounding of its inputs after it.
 * C3 -- 256 rods of 100 segments on one-sided fixed joints plus 64 spheres,
   rigid-body ground contact, 20 iterations: identical colors, FP64 and MIXED
   positions within 1e-9, quaternions within 1e-8, over 20 steps.
@@ -84,24 +85,46 @@ def test_c2_collision_stage_bit_exact_at_size(oracle_lib):
         o.step(1)
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-3)])
-def test_c2_trajectory_at_size(oracle_lib, precision, tol):
-    """FP32 bar: the cube lands at step ~18; after that, friction switches
-    between stick and slip on per-vertex thresholds, and FP32 rounding of
-    ~1e-7 m moves individual switches (the oracle fed FP32-rounded inputs
-    drifts the same way); 2e-3 of the diagonal bounds the 60-step drift."""
+def test_c2_trajectory_at_size_fp64(oracle_lib):
     sc = scenes.cube_drop(n=32, surface=True)
-    e, o = _pair(oracle_lib, sc, precision)
+    e, o = _pair(oracle_lib, sc, "fp64")
     diag = sc.bbox_diagonal()
-    worst = []
     for step in range(1, 61):
         e.step(1)
         o.step(1)
         if step in (1, 10, 20, 30, 45, 60):
             err = np.abs(e.positions() - o.positions()).max() / diag
-            worst.append((step, err))
-            assert err <= tol, f"step {step}: {err:.2e} of the diagonal ({precision})"
-    print(precision, worst)
+            assert err <= 1e-9, f"step {step}: {err:.2e} of the diagonal"
+
+
+def test_c2_trajectory_at_size_fp32(oracle_lib):
+    """FP32 engine vs the FP64 oracle on the 32^3 drop: before touchdown
+    (step ~18) within 1e-5 of the diagonal; after it, friction switches
+    between stick and slip on per-vertex thresholds, so an FP32 rounding of
+    the inputs alone moves the trajectory.  That sensitivity is measured with
+    a second oracle started from the initial positions rounded to FP32; the
+    engine must stay within 3x of it (+1e-5) at every checkpoint."""
+    sc = scenes.cube_drop(n=32, surface=True)
+    e, o = _pair(oracle_lib, sc, "fp32")
+    o32 = oracle_lib.Oracle(threads=THREADS)
+    sc.load(o32)
+    o32.finalize()
+    o32.set_positions_raw(0, o32.positions().astype(np.float32).astype(np.float64))
+    diag = sc.bbox_diagonal()
+    seen = []
+    for step in range(1, 61):
+        e.step(1)
+        o.step(1)
+        o32.step(1)
+        if step in (1, 5, 10, 15, 20, 30, 45, 60):
+            X = o.positions()
+            err = np.abs(e.positions() - X).max() / diag
+            sens = np.abs(o32.positions() - X).max() / diag
+            seen.append((step, round(err, 8), round(sens, 8)))
+            if step <= 15:
+                assert err <= 1e-5, f"step {step}: {err:.2e} before touchdown"
+            assert err <= 3 * sens + 1e-5, f"step {step}: {err:.2e} vs the oracle's own FP32 sensitivity {sens:.2e}"
+    print("C2 FP32 (step, error, oracle sensitivity):", seen)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
