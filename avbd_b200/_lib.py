@@ -116,6 +116,7 @@ SIGNATURES = {
     "avbd_mlp_trainer_destroy": [_vp],
     "avbd_set_warmstart": [_vp, C.c_int, _fp],
     "avbd_warmstart_sample": [_vp, _vp, _vp, _up],
+    "avbd_set_initial_guess": [_vp, _dp],
     "avbd_last_error_string": [],
     "avbd_version": [],
 }

@@ -368,6 +368,15 @@ class Context:
         check(self.L.avbd_profile_solve(self.h, iterations, C.byref(ms), C.byref(b), C.byref(nl)))
         return ms.value, b.value, nl.value
 
+    def set_initial_guess(self, positions):
+        """The next step's initial guess for every solved positional particle
+        (particles x 3), used once in place of the inertial initialisation."""
+        if positions is None:
+            check(self.L.avbd_set_initial_guess(self.h, None))
+            return
+        x = _d(positions, (-1, 3))
+        check(self.L.avbd_set_initial_guess(self.h, _dp(x)))
+
     def profile_step(self):
         """One run-to-tolerance step with the timed step's launches: kernel
         time (ms) and algorithmic bytes of its vertex-solve launches, the

@@ -98,6 +98,8 @@ static void free_device(avbd_ctx* c) {
     c->d_ws_feat = c->d_ws_x0 = nullptr;
     c->d_ws_target = nullptr;
     c->ws_mode = 0;
+    c->d_ws_guess = nullptr;
+    c->ws_guess_pending = false;
     c->ws_recorded = false;
     c->finalized = false;
     c->graph_dirty = true;
@@ -988,6 +990,11 @@ int enqueue_begin(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t
     if (c->damping) launch_tet_eprev<R>(c, s, k, st);
     launch_begin_step<R>(c, s, k, st);
     launch_begin_step_rot<R>(c, s, k, st);
+    if (c->ws_guess_pending) {  // the caller's initial guess replaces the inertial one, once
+        launch_load_positions<R>(s, c->d_ws_guess, c->d_inv, 0, (unsigned)c->mass.size(), 4, st);
+        count_launch(c);
+        c->ws_guess_pending = false;
+    }
     if (c->ws_mode) {
         // learned warm start: features at the inertial guess x0, then either
         // x0 += s MLP(features) or (recording) a copy of x0 for the targets
@@ -1076,11 +1083,9 @@ StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_acc
 template <typename R>
 int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     const char* env = getenv("AVBD_LANES");
-    const char* env_stage = getenv("AVBD_STAGE");
-    if (env) {  // a fixed launch shape: lanes, and (AVBD_STAGE=1) staged neighbour positions
+    if (env) {
         int l = atoi(env);
         if (l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32) c->lanes = l;
-        c->stage = env_stage && atoi(env_stage) != 0 && c->lanes <= 8;
         return AVBD_OK;
     }
     unsigned long long solved = 0;
@@ -1098,16 +1103,9 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     CUDA_OR_FAIL(cudaEventCreate(&b));
     const unsigned long long launches0 = c->stats.kernel_launches;
     int best = 8;
-    bool best_stage = false;
     float best_ms = 1e30f;
-    // launch shapes: threads per vertex, and whether the neighbour positions
-    // are staged through shared memory (1-8 threads per vertex)
-    const int shapes[][2] = {{1, 0}, {1, 1}, {2, 0}, {2, 1}, {4, 0}, {4, 1}, {8, 0}, {8, 1}, {16, 0}};
-    for (const auto& sh : shapes) {
-        const int l = sh[0];
-        if (env_stage && (atoi(env_stage) != 0) != (sh[1] != 0)) continue;
+    for (int l : {1, 2, 4, 8, 16}) {
         c->lanes = l;
-        c->stage = sh[1] != 0;
         for (int rep = 0; rep < 2; rep++) {  // rep 0 warms up, rep 1 is timed
             if (rep == 1) CUDA_OR_FAIL(cudaEventRecord(a, st));
             for (unsigned col = 0; col < c->num_colors; col++) {
@@ -1124,13 +1122,10 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
         CUDA_OR_FAIL(cudaEventSynchronize(b));
         float ms = 0;
         CUDA_OR_FAIL(cudaEventElapsedTime(&ms, a, b));
-        if (getenv("AVBD_TRACE"))
-            fprintf(stderr, "[avbd] autotune: %d threads per vertex%s: %.3f ms per sweep\n", l,
-                    c->stage ? ", staged neighbours" : "", ms);
+        if (getenv("AVBD_TRACE")) fprintf(stderr, "[avbd] autotune: %d threads per vertex: %.3f ms per sweep\n", l, ms);
         if (ms < best_ms) {
             best_ms = ms;
             best = l;
-            best_stage = c->stage;
         }
         CUDA_OR_FAIL(cudaMemcpyAsync(s.x, snap, sizeof(V4) * s.n, cudaMemcpyDeviceToDevice, st));
     }
@@ -1140,11 +1135,8 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     cudaEventDestroy(b);
     cudaFree(snap);
     c->lanes = best;
-    c->stage = best_stage;
     c->stats.kernel_launches = launches0;
-    if (getenv("AVBD_TRACE"))
-        fprintf(stderr, "[avbd] autotune: %d threads per vertex%s (%.3f ms per sweep)\n", best,
-                best_stage ? ", staged neighbours" : "", best_ms);
+    if (getenv("AVBD_TRACE")) fprintf(stderr, "[avbd] autotune: %d threads per vertex (%.3f ms per sweep)\n", best, best_ms);
     return AVBD_OK;
 }
 
@@ -1256,8 +1248,8 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
     StepConsts k = consts(c);
     cudaStream_t st = c->stream;
     // a step with dynamic contacts runs host work between its launches: no graph
-    const bool capturable =
-        c->use_graph && !c->dyn && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+    const bool capturable = c->use_graph && !c->dyn && !c->ws_guess_pending && st != nullptr &&
+                            st != cudaStreamLegacy && st != cudaStreamPerThread;
     const bool tol_mode = c->solver.residual_tolerance > 0;
     if (c->graph && (c->graph_dirty || c->graph_tol != tol_mode || !capturable)) {
         cudaGraphExecDestroy(c->graph);
@@ -1851,6 +1843,22 @@ int avbd_set_warmstart(avbd_ctx* c, int mode, const float* params) {
     c->ws_recorded = false;
     c->graph_dirty = true;
     CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    return AVBD_OK;
+}
+
+int avbd_set_initial_guess(avbd_ctx* c, const double* positions) {
+    if (int r = check_ctx(c)) return r;
+    if (!c->finalized) return fail(AVBD_ERR_STATE, "finalize first");
+    if (!positions) {
+        c->ws_guess_pending = false;
+        return AVBD_OK;
+    }
+    const size_t n = c->mass.size();
+    if (!c->d_ws_guess)
+        if (int rc = dalloc(c, &c->d_ws_guess, 3 * n)) return rc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(c->d_ws_guess, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+    c->ws_guess_pending = true;
     return AVBD_OK;
 }
 

@@ -290,7 +290,6 @@ struct avbd_ctx {
     bool graph_tol = false;
     bool use_graph = true;
     int lanes = 8;                      // threads per vertex in the tet solve
-    bool stage = false;                 // tet solve stages neighbour positions in shared memory
     int block = 256;
 
     // learned warm start (mlp.cu): 0 off, 1 record features/targets, 2 apply
@@ -302,6 +301,8 @@ struct avbd_ctx {
     const float* ws_prev_arg = nullptr; // previous-correction rows for the features launch in flight
     float ws_kappa = 0.5f;              // relative error assumed by the acceptance test
     bool ws_recorded = false;
+    double* d_ws_guess = nullptr;       // caller's initial guess of the next step (external order, FP64)
+    bool ws_guess_pending = false;
 
     // dynamic triangle-rigid contacts: pool, recoloring and per-color lists,
     // managed on the host every step (contacts.cu); null without sphere primitives

@@ -150,64 +150,6 @@ AVBD_D IncRec<double> load_rec<double>(const IncRec<double>* p) {
     return r;
 }
 
-// ------------------------------------------- staged neighbour positions
-// The staged form of the record loop splits a record into its index word
-// (the three other vertices and the tet) and its data (the three other rows
-// of D = [Q; -1^T Q], V lambda, V mu, mu/lambda).  Index words are loaded two
-// records ahead, so the three neighbour positions of the next record can be
-// copied into a per-thread shared-memory slot (cp.async) while the current
-// record is evaluated; no registers are held for them in flight.
-template <typename RS>
-struct RecDat {
-    RS d[9];
-    RS vlam, vmu, mol;
-};
-
-template <typename RS>
-AVBD_D uint4 ld_idx(const IncRec<RS>* p) {
-    return __ldcs(reinterpret_cast<const uint4*>(p));
-}
-template <typename RS>
-AVBD_D RecDat<RS> ld_dat(const IncRec<RS>* p);
-template <>
-AVBD_D RecDat<float> ld_dat<float>(const IncRec<float>* p) {
-    const float4* q = reinterpret_cast<const float4*>(p);
-    float4 b = __ldcs(q + 1), c = __ldcs(q + 2), d = __ldcs(q + 3);
-    RecDat<float> r;
-    r.d[0] = b.x; r.d[1] = b.y; r.d[2] = b.z; r.d[3] = b.w;
-    r.d[4] = c.x; r.d[5] = c.y; r.d[6] = c.z; r.d[7] = c.w;
-    r.d[8] = d.x; r.vlam = d.y; r.vmu = d.z; r.mol = d.w;
-    return r;
-}
-template <>
-AVBD_D RecDat<double> ld_dat<double>(const IncRec<double>* p) {
-    const double2* q = reinterpret_cast<const double2*>(p);
-    RecDat<double> r;
-    double2 v;
-    v = __ldcs(q + 1); r.d[0] = v.x; r.d[1] = v.y;
-    v = __ldcs(q + 2); r.d[2] = v.x; r.d[3] = v.y;
-    v = __ldcs(q + 3); r.d[4] = v.x; r.d[5] = v.y;
-    v = __ldcs(q + 4); r.d[6] = v.x; r.d[7] = v.y;
-    v = __ldcs(q + 5); r.d[8] = v.x; r.vlam = v.y;
-    v = __ldcs(q + 6); r.vmu = v.x; r.mol = v.y;
-    return r;
-}
-
-AVBD_D uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-AVBD_D void cp_async16(void* smem, const void* gmem) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
-}
-AVBD_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-AVBD_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// copies one vertex vector (16 B FP32, 32 B FP64) into shared memory
-AVBD_D void stage_vec(float4* dst, const float4* src) { cp_async16(dst, src); }
-AVBD_D void stage_vec(double4a* dst, const double4a* src) {
-    cp_async16(dst, src);
-    cp_async16(reinterpret_cast<char*>(dst) + 16, reinterpret_cast<const char*>(src) + 16);
-}
-
 // Accumulated block: gradient in the state precision P, Hessian in HT.  The
 // Hessian only shapes the Newton step, never the converged state, so the
 // mixed mode keeps it in FP32 while the gradient (which the residual
@@ -221,8 +163,8 @@ struct Block3 {
 // One NeoHookean incidence: NeoHookeanEnergySolver::accumulate with the tet
 // restated relative to the solved vertex (see IncRec).  P is the precision of
 // positions and gradient, RS the stored record scalar, HT the Hessian type.
-// The terms from the three edge vectors e_j = x_(o_j) - x_i; `r` is an
-// IncRec or a RecDat (same data members), `tet` indexes the damping state.
+// The terms from the three edge vectors e_j = x_(o_j) - x_i; `tet` indexes
+// the damping state.
 template <typename P, typename RS, typename HT, bool DAMP, typename RD>
 AVBD_D void accumulate_tet_e(const DevState<P>& s, const RD& r, unsigned tet, V3<P> e1, V3<P> e2, V3<P> e3, P dt,
                              Block3<P, HT>& B) {
@@ -366,14 +308,12 @@ struct SolveMinBlocks {
 // DYN: the instantiation for vertices with dynamic contact energies or a
 // color changed by the recoloring, launched over per-color lists; the slab
 // launches (DYN false) skip those vertices and carry no dynamic code.
-template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN,
-          bool STAGE = false>
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
 __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS>* __restrict__ inc, unsigned begin,
                                            unsigned count, unsigned gi, unsigned lane, const Consts<P>& c,
                                            unsigned long long* counters, double* out, const SceneTol& T,
                                            const float4* __restrict__ aux, const uint32_t* __restrict__ list,
                                            double* acc = nullptr) {
-    static_assert(!STAGE || ((MODE == MODE_SOLVE || MODE == MODE_RESIDUAL) && !DYN), "staged loop: slab solves only");
     bool active = gi < count;
     unsigned p = list ? (active ? list[gi] : 0u) : begin + (active ? gi : 0);
     uint8_t fl = active ? s.flags[p] : 0;
@@ -388,58 +328,7 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
     V3<P> xi = mk3<P>(0, 0, 0);
     // MODE_FEATURES: sum of the other vertices' velocities and of mu/lambda over the incident tets
     float fv0 = 0.f, fv1 = 0.f, fv2 = 0.f, fmol = 0.f, fcnt = 0.f;
-    if (STAGE && active) {
-        // staged record loop (see RecDat): the neighbour positions of the
-        // next record are copied into this thread's shared-memory slots
-        // while the current record is evaluated; slot j of thread t is
-        // ring[j * blockDim.x + t] (two stages of three vertex vectors)
-        using V4 = typename Vec4Of<P>::T;
-        extern __shared__ __align__(32) unsigned char stage_mem[];
-        V4* ring = reinterpret_cast<V4*>(stage_mem) + threadIdx.x;
-        const unsigned W = blockDim.x;
-        xi = xyz(s.x[p]);
-        const unsigned b = s.inc_begin[p], e = s.inc_begin[p + 1];
-        unsigned k = b + lane;
-        uint4 id_cur = make_uint4(0, 0, 0, 0), id_nxt = id_cur;
-        RecDat<RS> dat_cur, dat_nxt;
-        if (k < e) {
-            id_cur = ld_idx(inc + k);
-            dat_cur = ld_dat(inc + k);
-            stage_vec(ring, s.x + id_cur.x);
-            stage_vec(ring + W, s.x + id_cur.y);
-            stage_vec(ring + 2 * W, s.x + id_cur.z);
-        }
-        cp_async_commit();
-        if (k + LANES < e) {
-            id_nxt = ld_idx(inc + k + LANES);
-            dat_nxt = ld_dat(inc + k + LANES);
-        }
-        unsigned stg = 0;
-        while (k < e) {
-            const unsigned kn = k + LANES, k2 = kn + LANES;
-            uint4 id_n2 = make_uint4(0, 0, 0, 0);
-            if (k2 < e) id_n2 = ld_idx(inc + k2);
-            if (kn < e) {
-                V4* dst = ring + 3 * (stg ^ 1u) * W;
-                stage_vec(dst, s.x + id_nxt.x);
-                stage_vec(dst + W, s.x + id_nxt.y);
-                stage_vec(dst + 2 * W, s.x + id_nxt.z);
-            }
-            cp_async_commit();
-            if (k2 + 2 * LANES < e) prefetch_l2(inc + k2 + 2 * LANES);
-            cp_async_wait<1>();  // this record's neighbours have landed
-            const V4* src = ring + 3 * stg * W;
-            accumulate_tet_e<P, RS, HT, DAMP>(s, dat_cur, id_cur.w, xyz(src[0]) - xi, xyz(src[W]) - xi,
-                                              xyz(src[2 * W]) - xi, c.dt, B);
-            id_cur = id_nxt;
-            dat_cur = dat_nxt;
-            id_nxt = id_n2;
-            if (k2 < e) dat_nxt = ld_dat(inc + k2);
-            stg ^= 1u;
-            k = kn;
-        }
-        cp_async_wait<0>();  // no copy may land after the loop
-    } else if (active) {
+    if (active) {
         xi = xyz(s.x[p]);
         unsigned b = s.inc_begin[p], e = s.inc_begin[p + 1];
         // software pipeline: the next record streams in while this one is processed
@@ -620,8 +509,7 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
 // over the block: one atomic per piece instead of one per vertex on the
 // scene's sum.  Otherwise thread groups map to vertices [begin, begin +
 // count) (or to list).
-template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN,
-          bool STAGE = false>
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
 __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
                                                    unsigned long long* counters, double* out, SceneTol T,
@@ -648,9 +536,9 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
                 for (unsigned j = 0; j < 4; j++)
                     if (bn + lane + j * LANES < en) prefetch_l2(inc + bn + lane + j * LANES);
             }
-            tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN, STAGE>(s, inc, rg.x, rg.y,
-                                                                         base + threadIdx.x / LANES, lane, c, counters,
-                                                                         out, TB, aux, list, sum ? &acc : nullptr);
+            tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, rg.x, rg.y, base + threadIdx.x / LANES, lane,
+                                                                  c, counters, out, TB, aux, list,
+                                                                  sum ? &acc : nullptr);
         }
         if (sum) {
             __shared__ double part[32];
@@ -667,8 +555,8 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
         return;
     }
     const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
-    tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN, STAGE>(s, inc, begin, count, tid / LANES, lane, c, counters,
-                                                                 out, T, aux, list);
+    tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, begin, count, tid / LANES, lane, c, counters, out, T,
+                                                          aux, list);
 }
 
 // Chebyshev acceleration of every particle fused with the ground-contact dual
@@ -762,6 +650,13 @@ __global__ void k_load(DevState<R> s, const double* src, const uint32_t* inv_map
         return;
     }
     typename Vec4Of<R>::T o = make4<R>(v, R(0));
+    if (mode == 4) {  // a caller's initial guess of the step: solved positional vertices only
+        if (s.flags[p] & (VF_FIXED | VF_ORIENTED)) return;
+        s.x[p] = o;
+        s.xl[p] = o;
+        s.xll[p] = o;
+        return;
+    }
     s.x[p] = o;
     if (mode == 1) {
         typename Vec4Of<R>::T y4 = s.y[p];
@@ -810,18 +705,6 @@ static void solve_dispatch(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, c
     auto kc = mkc<P>(k);
     auto* ctr = c->d_counters;
     const float4* aux = reinterpret_cast<const float4*>(c->ws_prev_arg);
-    if constexpr ((MODE == MODE_SOLVE || MODE == MODE_RESIDUAL) && !DYN && LANES <= 8) {
-        if (c->stage && !damp) {  // neighbour positions staged through shared memory
-            const size_t smem = 6 * 256 * sizeof(typename Vec4Of<P>::T);
-            // above the default 48 KB together with the kernel's static shared memory
-            auto kf = ground ? k_solve_tet<P, RS, HT, LANES, false, true, MODE, false, true>
-                             : k_solve_tet<P, RS, HT, LANES, false, false, MODE, false, true>;
-            cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            kf<<<blocks, 256, smem, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list, ranges);
-            count_launch(c);
-            return;
-        }
-    }
     if (damp && ground)
         k_solve_tet<P, RS, HT, LANES, true, true, MODE, DYN><<<blocks, 256, 0, st>>>(s, inc, begin, count, kc, ctr, out, T, aux, list, ranges);
     else if (damp)

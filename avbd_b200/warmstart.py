@@ -273,3 +273,55 @@ def evaluate(params, Fv, Tv, device: int = 0):
 def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
     with np.load(path) as d:
         return np.ascontiguousarray(d["params"], dtype=np.float32)
+
+
+def guess_bound(scene, steps: int, warmup: int = 3, precision: str = "mixed", tol: float = 1e-4,
+                max_iters: int = 100, device: int = 0):
+    """What any displacement warm start can save, measured: every step runs
+    twice from the same start state -- once with the inertial initial guess
+    (plain AVBD), once with the step's own converged positions as the guess
+    (avbd_set_initial_guess), i.e. a perfect predictor of the converged
+    displacement.  Both then iterate to the same residual tolerance.
+    Returns per-step arrays of per-scene iterations (plain, perfect guess)."""
+    from .api import Context
+    a, b = Context(device=device), Context(device=device)
+    for e in (a, b):
+        scene.load(e, residual_tolerance=tol, max_iters=max_iters, precision=precision)
+        e.finalize()
+        e.step(warmup)
+    plain, perfect = [], []
+    for _ in range(steps):
+        x0, v0 = a.positions(), a.velocities()
+        a.step(1)
+        plain.append(a.scene_iterations())
+        b.set_state(x0, v0)
+        b.set_initial_guess(a.positions())
+        b.step(1)
+        perfect.append(b.scene_iterations())
+    a.close()
+    b.close()
+    return np.array(plain), np.array(perfect)
+
+
+if __name__ == "__main__":
+    # python -m avbd_b200.warmstart [scenes] [steps] [warmup]: the perfect-guess
+    # bound on the benchmark batch (seed 0, MIXED, R <= 1e-4, <= 100 iterations)
+    import json
+    import sys
+
+    from . import scenes as _scenes
+    S = int(sys.argv[1]) if len(sys.argv) > 1 else 1024
+    K = int(sys.argv[2]) if len(sys.argv) > 2 else 10
+    W = int(sys.argv[3]) if len(sys.argv) > 3 else 3
+    sc = _scenes.batched_cubes(num_scenes=S, seed=0)
+    plain, perfect = guess_bound(sc, K, W)
+    verts = np.array([(c + 1) ** 3 for c in sc.meta["cells"]], dtype=np.float64)
+    capped_p, capped_g = (plain >= 100).mean(), (perfect >= 100).mean()
+    print(json.dumps({
+        "scenes": S, "steps": K, "warmup": W,
+        "iterations_per_scene_step": {"plain": float(plain.mean()), "perfect_guess": float(perfect.mean())},
+        "vertex_weighted_iterations": {"plain": float((plain * verts).sum() / (verts.sum() * K)),
+                                       "perfect_guess": float((perfect * verts).sum() / (verts.sum() * K))},
+        "capped_fraction": {"plain": float(capped_p), "perfect_guess": float(capped_g)},
+        "reduction": float(plain.mean() / max(perfect.mean(), 1e-9)),
+    }))

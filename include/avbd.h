@@ -488,6 +488,16 @@ AVBD_API int avbd_set_warmstart(avbd_ctx* ctx, int mode, const float* params);
  *   25    incident tet count / 24 */
 AVBD_API int avbd_warmstart_sample(avbd_ctx* ctx, void* features, float* targets, unsigned* rows);
 
+/* No counterpart in the reference: the initial guess x0 of the next step's
+ * iterations for every solved positional particle, supplied by the caller
+ * (positions: particles x 3 doubles, the order of avbd_particles_add),
+ * replacing the adaptive inertial initialisation (VBDSolver.hpp:208-248)
+ * once; the inertial prediction y itself is unchanged.  For an external
+ * predictor, and for bounding what any displacement warm start can save:
+ * given the step's converged positions, the iterations still needed are a
+ * floor for every predictor of them.  NULL cancels a pending guess. */
+AVBD_API int avbd_set_initial_guess(avbd_ctx* ctx, const double* positions);
+
 AVBD_API const char* avbd_last_error_string(void);
 AVBD_API const char* avbd_version(void);
 

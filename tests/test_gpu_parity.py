@@ -221,36 +221,6 @@ def test_piece_launches_match_slab_launches(monkeypatch, precision):
     assert np.abs(xa - xb).max() / sc.bbox_diagonal() < 1e-7
 
 
-@pytest.mark.parametrize("lanes", ["1", "2", "4", "8"])
-@pytest.mark.parametrize("precision", ["fp32", "fp64", "mixed"])
-def test_staged_neighbours_match_direct_gathers(monkeypatch, precision, lanes):
-    """The solve's staged record loop (neighbour positions copied into
-    shared memory one record ahead, AVBD_STAGE=1) evaluates the same terms
-    in the same order as the direct loop: identical states and iteration
-    counts in fixed-iteration steps (whole slabs); in run-to-tolerance steps
-    (per-scene pieces, with the residual pass) the same up to the order of
-    the residual pass's atomic per-scene sums, which can move a stop
-    decision by an iteration."""
-    sc = scenes.batched_cubes(num_scenes=5, seed=11, n_min=3, n_max=9)
-    for tol, iters in ((1e-4, 150), (0.0, 0)):
-        runs = {}
-        for stage in ("1", "0"):
-            monkeypatch.setenv("AVBD_LANES", lanes)
-            monkeypatch.setenv("AVBD_STAGE", stage)
-            e = Context()
-            sc.load(e, precision=precision, residual_tolerance=tol, max_iters=iters)
-            e.finalize()
-            e.step(4)
-            runs[stage] = (e.positions(), e.stats()["iterations"])
-            e.close()
-        if tol == 0.0:
-            assert runs["1"][1] == runs["0"][1]
-            assert np.array_equal(runs["1"][0], runs["0"][0]), (precision, lanes)
-        else:
-            assert abs(int(runs["1"][1]) - int(runs["0"][1])) <= 5
-            assert np.abs(runs["1"][0] - runs["0"][0]).max() / sc.bbox_diagonal() < 1e-7, (precision, lanes)
-
-
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_device_iteration_loop_matches_host_loop(monkeypatch, precision):
     """A run-to-tolerance step is one CUDA graph whose iteration loop is a
