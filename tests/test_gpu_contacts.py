@@ -94,21 +94,35 @@ def test_contact_blocks_and_residual_match_oracle(oracle_lib):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp32"])
-def test_contacts_lower_precision_land_spheres(oracle_lib, precision):
-    """Mixed and FP32 runs form contacts and keep the spheres on the cube
-    (their detections may differ from FP64's near the margin)."""
+def test_contacts_lower_precision_track_oracle(oracle_lib, precision):
+    """MIXED and FP32 runs against the FP64 oracle over 60 steps.  A
+    detection within rounding of the collision margin, or a friction
+    stick/slip switch, moves with any rounding of the state, so the bar is
+    the oracle's own sensitivity: a second oracle started from the positions
+    rounded to FP32.  The engine stays within 3x that drift (+1e-5 of the
+    diagonal) at every checkpoint, forms contacts, and its live-contact count
+    stays within 2 of the oracle's."""
     sc, e, o = pair(oracle_lib, precision)
+    o32 = oracle_lib.Oracle()
+    sc.load(o32)
+    o32.finalize()
+    o32.set_positions_raw(0, o32.positions().astype(np.float32).astype(np.float64))
+    diag = sc.bbox_diagonal()
     live = 0
+    seen = []
     for _ in range(6):
         e.step(10)
+        o.step(10)
+        o32.step(10)
+        X = o.positions()
+        err = np.abs(e.positions() - X).max() / diag
+        sens = np.abs(o32.positions() - X).max() / diag
+        seen.append((round(err, 7), round(sens, 7)))
+        assert err <= 3 * sens + 1e-5, (precision, seen)
         live = max(live, e.dynamic_info()["live"])
-    x = e.positions()
-    assert np.isfinite(x).all()
+        assert abs(e.dynamic_info()["live"] - o.dynamic_info()["live"]) <= 2
     assert live > 0
-    top = x[:N_CUBE, 1].max()
-    radii = np.array([a[1][0] for m, a, _ in sc.calls if m == "add_spheres"])
-    low = x[N_CUBE:, 1] - radii
-    assert np.all(low > top - 0.08) and np.all(low < top + 0.02), (low, top)
+    print(precision, "error vs oracle sensitivity per 10 steps:", seen)
 
 
 def test_contacts_run_to_tolerance(oracle_lib):

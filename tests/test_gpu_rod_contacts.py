@@ -121,12 +121,27 @@ def test_rod_contact_blocks_match_oracle(oracle_lib):
 
 @pytest.mark.parametrize("precision", ["mixed", "fp32"])
 def test_rod_contacts_lower_precision(oracle_lib, precision):
+    """MIXED and FP32 rod contacts against the FP64 oracle over 60 steps,
+    held to 3x the oracle's own drift when its positions are rounded to FP32
+    (+1e-5 of the diagonal), with the live-contact count within 2."""
     sc, e, o = pair(oracle_lib, precision)
+    o32 = oracle_lib.Oracle()
+    sc.load(o32)
+    o32.finalize()
+    o32.set_positions_raw(0, o32.positions().astype(np.float32).astype(np.float64))
+    diag = sc.bbox_diagonal()
     live = 0
+    seen = []
     for _ in range(6):
         e.step(10)
+        o.step(10)
+        o32.step(10)
+        X = o.positions()
+        err = np.abs(e.positions() - X).max() / diag
+        sens = np.abs(o32.positions() - X).max() / diag
+        seen.append((round(err, 7), round(sens, 7)))
+        assert err <= 3 * sens + 1e-5, (precision, seen)
         live = max(live, e.dynamic_info()["rod_live"])
-    x = e.positions()
-    top = x[:N_CUBE, 1].max()
-    assert np.isfinite(x).all() and live > 0
-    assert np.all(x[N_CUBE:, 1] > top - 0.02) and np.all(x[N_CUBE:, 1] < top + 0.1)
+        assert abs(e.dynamic_info()["rod_live"] - o.dynamic_info()["rod_live"]) <= 2
+    assert live > 0
+    print(precision, "error vs oracle sensitivity per 10 steps:", seen)
