@@ -384,9 +384,61 @@ enum { RMODE_SOLVE = 0, RMODE_RESIDUAL = 1, RMODE_DEBUG = 2 };
 // serves the static slabs; the lists of vertices with contacts use 8, since a
 // rod node may carry many contacts, each a chain of rotation and Jacobian
 // functions.
+// FP32 solve of a symmetric positive definite 6x6 block: Jacobi scaling
+// (A_s = S A S, S = diag(A)^-1/2) and an LDL^T factorisation of A_s.  A rod
+// node's block mixes translational stiffness (EA/L ~ 1e5 N/m) with
+// rotational terms (EI/L ~ 1 N m) and has a 2-norm condition number ~2e5;
+// scaled, ~2 (at most ~10 on the C3 scene).  Returns the pivot ratio
+// max(d)/min(d) of the scaled factorisation as the condition estimate
+// (infinite when a pivot is not positive); the caller re-solves in FP64
+// above its threshold.
+AVBD_D float ldlt6_scaled(const float (&A)[6][6], const float (&b)[6], float (&x)[6]) {
+    float sc[6], L[6][6], d[6], y[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) sc[i] = A[i][i] > 0.f ? rsqrtf(A[i][i]) : 0.f;
+    float dmin = 3.402823e38f, dmax = 0.f;
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+        float dj = A[j][j] * sc[j] * sc[j];
+#pragma unroll
+        for (int k = 0; k < j; k++) dj -= L[j][k] * L[j][k] * d[k];
+        d[j] = dj;
+        dmin = fminf(dmin, dj);
+        dmax = fmaxf(dmax, dj);
+        const float inv = 1.f / dj;
+#pragma unroll
+        for (int i = j + 1; i < 6; i++) {
+            float v = A[i][j] * sc[i] * sc[j];
+#pragma unroll
+            for (int k = 0; k < j; k++) v -= L[i][k] * L[j][k] * d[k];
+            L[i][j] = v * inv;
+        }
+    }
+    if (!(dmin > 0.f)) return 3.402823e38f;
+#pragma unroll
+    for (int i = 0; i < 6; i++) {  // L y = S b
+        float v = b[i] * sc[i];
+#pragma unroll
+        for (int k = 0; k < i; k++) v -= L[i][k] * y[k];
+        y[i] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < 6; i++) y[i] /= d[i];
+#pragma unroll
+    for (int i = 5; i >= 0; i--) {  // L^T z = y, x = S z
+        float v = y[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; k++) v -= L[k][i] * y[k];
+        y[i] = v;
+        x[i] = v * sc[i];
+    }
+    return dmax / dmin;
+}
+
 template <typename R, int MODE, int LANES>
 __global__ void __launch_bounds__(ROD_BLOCK) k_solve_rod(DevState<R> s, unsigned begin, unsigned count, R dt, double g,
-                                                   double* out, SceneTol T, const uint32_t* __restrict__ list) {
+                                                   double* out, SceneTol T, const uint32_t* __restrict__ list,
+                                                   double kappa_max, unsigned long long* counters) {
     const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned gi = tid / LANES, lane = tid % LANES;
     if (LANES == 1 && gi >= count) return;
@@ -475,18 +527,46 @@ __global__ void __launch_bounds__(ROD_BLOCK) k_solve_rod(DevState<R> s, unsigned
         for (int i = 0; i < 6; i++) r2 += rhs[i] * rhs[i];
         atomicAdd(T.r2 + T.scene[p], r2);
     }
-    double A[6][6];
-    for (int i = 0; i < 6; i++)
-        for (int j = 0; j < 6; j++) A[i][j] = (double)B.h[i][j];
-    double mh = (double)m * (double)idt2;
-    A[0][0] += mh;
-    A[1][1] += mh;
-    A[2][2] += mh;
-    A[3][3] += (double)I.x * (double)idt2;
-    A[4][4] += (double)I.y * (double)idt2;
-    A[5][5] += (double)I.z * (double)idt2;
     double dx[6];
-    lu_solve_d<6>(A, rhs, dx);
+    bool solved = false;
+    if constexpr (sizeof(R) == 4) {
+        // FP32 mode: scaled FP32 LDL^T, FP64 only above the condition threshold
+        float Af[6][6], bf[6], xf[6];
+#pragma unroll
+        for (int i = 0; i < 6; i++) {
+#pragma unroll
+            for (int j = 0; j < 6; j++) Af[i][j] = (float)B.h[i][j];
+            bf[i] = (float)rhs[i];
+        }
+        const float mhf = m * idt2;
+        Af[0][0] += mhf;
+        Af[1][1] += mhf;
+        Af[2][2] += mhf;
+        Af[3][3] += I.x * idt2;
+        Af[4][4] += I.y * idt2;
+        Af[5][5] += I.z * idt2;
+        const float kap = ldlt6_scaled(Af, bf, xf);
+        if (kap <= (float)kappa_max) {
+#pragma unroll
+            for (int i = 0; i < 6; i++) dx[i] = (double)xf[i];
+            solved = true;
+        } else if (counters) {
+            atomicAdd(counters, 1ull);
+        }
+    }
+    if (!solved) {
+        double A[6][6];
+        for (int i = 0; i < 6; i++)
+            for (int j = 0; j < 6; j++) A[i][j] = (double)B.h[i][j];
+        double mh = (double)m * (double)idt2;
+        A[0][0] += mh;
+        A[1][1] += mh;
+        A[2][2] += mh;
+        A[3][3] += (double)I.x * (double)idt2;
+        A[4][4] += (double)I.y * (double)idt2;
+        A[5][5] += (double)I.z * (double)idt2;
+        lu_solve_d<6>(A, rhs, dx);
+    }
     V3<R> xn = x + mk3<R>((R)dx[0], (R)dx[1], (R)dx[2]);
     if (s.conflicted && s.conflicted[p]) {
         // intra-color conflict: the position is buffered and committed after the
@@ -581,14 +661,16 @@ void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned
                       cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list) {
     if (count == 0) return;
     // nodes with contacts (lists; the debug pass) take 8 lanes, the static slabs one
+    const double km = k.kappa_max;
+    unsigned long long* ctr = c->d_counters;  // [0]: blocks solved in FP64
     if (mode == RMODE_RESIDUAL)
-        k_solve_rod<R, RMODE_RESIDUAL, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_RESIDUAL, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
     else if (mode == RMODE_DEBUG)
-        k_solve_rod<R, RMODE_DEBUG, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_DEBUG, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
     else if (list)
-        k_solve_rod<R, RMODE_SOLVE, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_SOLVE, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
     else
-        k_solve_rod<R, RMODE_SOLVE, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list);
+        k_solve_rod<R, RMODE_SOLVE, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
     count_launch(c);
 }
 
