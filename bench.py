@@ -194,13 +194,15 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def traffic_for(workload: str):
-    """Per-launch DRAM bytes of the solve kernel from the committed ncu summary."""
+def traffic_for(workload: str, bytes_per_launch: float):
+    """Per-launch DRAM bytes of the solve kernel: the DRAM/algorithmic ratio of
+    the committed ncu capture times the algorithmic bytes per launch."""
     path = os.path.join(ROOT, "profiles", "solve_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get(workload)
+        ratio = d[workload]["dram_over_algorithmic"]
+        return ratio * bytes_per_launch
     except Exception:
         return None
 
@@ -550,7 +552,7 @@ def run_engine(args):
         kernel = ("k_solve_rod (per-color 6-DOF vertex block solve)" if wl.rods
                   else "k_solve_tet (per-color vertex block solve)")
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic_for(workload), "kernel": kernel,
+                "traffic": traffic_for(workload, per_launch_bytes), "kernel": kernel,
                 "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "peak_source": peak_kind,
                 "launch_shape": ("one run-to-tolerance step as timed: per-scene pieces of every color slab, "
                                  f"converged scenes gated out ({solve_launches} launches, {prof_iters} iterations)"
