@@ -317,7 +317,12 @@ if __name__ == "__main__":
     plain, perfect = guess_bound(sc, K, W)
     verts = np.array([(c + 1) ** 3 for c in sc.meta["cells"]], dtype=np.float64)
     capped_p, capped_g = (plain >= 100).mean(), (perfect >= 100).mean()
+    conv = plain < 100  # scene-steps whose plain end state met the tolerance: the guess is their solution
     print(json.dumps({
+        "converged_scene_steps": {"fraction": float(conv.mean()), "plain": float(plain[conv].mean()),
+                                  "perfect_guess": float(perfect[conv].mean())},
+        "capped_scene_steps": {"plain": float(plain[~conv].mean()) if (~conv).any() else None,
+                               "perfect_guess": float(perfect[~conv].mean()) if (~conv).any() else None},
         "scenes": S, "steps": K, "warmup": W,
         "iterations_per_scene_step": {"plain": float(plain.mean()), "perfect_guess": float(perfect.mean())},
         "vertex_weighted_iterations": {"plain": float((plain * verts).sum() / (verts.sum() * K)),

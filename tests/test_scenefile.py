@@ -88,11 +88,16 @@ def test_msh_rejects_binary_and_bad_tags(tmp_path):
         meshio.read_msh(str(p))
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/resource/cube2.msh"), reason="reference meshes absent")
+def _reference_mesh():
+    from oracle.ref import REFERENCE_ROOT  # AVBD_REFERENCE_ROOT
+    return os.path.join(REFERENCE_ROOT, "resource", "cube2.msh")
+
+
+@pytest.mark.skipif(not os.path.exists(_reference_mesh()), reason="reference meshes absent")
 def test_reference_cube2_matches_golden_element():
     import json
     g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "neohookean_element0.json")))
-    v, t, f = meshio.read_msh("/root/reference/resource/cube2.msh")
+    v, t, f = meshio.read_msh(_reference_mesh())
     assert (v.shape, t.shape, f.shape) == ((27, 3), (40, 4), (48, 3))
     assert (t[0] + 1).tolist() == g["element_node_tags"]
     assert np.allclose(v[t[0]], g["vertices"])
