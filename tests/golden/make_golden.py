@@ -1,6 +1,7 @@
 """Generates the committed golden fixtures of tests/golden/ from the reference's
-own test inputs.  Run in a checkout that has the reference mounted at
-/root/reference; the GPU box and the tests only read the JSON it writes.
+own test inputs.  Reads the reference checkout named by AVBD_REFERENCE_ROOT
+(default /root/reference); the GPU box and the tests only read the JSON it
+writes.
 
 neohookean_element0.json -- the element used by test/test_neohookean_accumulate.cpp:
   tet 0 of resource/cube2.msh (gmsh MSH 4.1 ASCII, read directly because gmsh
@@ -10,7 +11,7 @@ neohookean_element0.json -- the element used by test/test_neohookean_accumulate.
 import json
 import os
 
-REF = "/root/reference"
+REF = os.environ.get("AVBD_REFERENCE_ROOT", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

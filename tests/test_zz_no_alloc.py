@@ -87,6 +87,35 @@ def test_noalloc_matches_context_path_twice():
         assert (order == ref["sorted_order"]).all(), f"call {call}: sorted order differs"
 
 
+def test_noalloc_at_the_primitive_limit():
+    """AVBD_NOALLOC_MAX_PRIMITIVES (262,144) random boxes, twice: the
+    single-block scan then runs over all 256 x 1,024 digit-histogram entries.
+    Codes are checked against a NumPy restatement of the Morton arithmetic
+    (LBVHBuilder.cpp:98-127; every step is one IEEE operation, so numpy
+    reproduces it) and the order against a stable sort of the codes."""
+    n = 262144
+    rng = np.random.default_rng(2026)
+    for call in range(2):
+        lo = rng.uniform(-3.0, 3.0, size=(n, 3))
+        boxes = np.ascontiguousarray(np.concatenate([lo, lo + rng.uniform(0, 0.05, size=(n, 3))], axis=1))
+        morton, order = _noalloc(boxes)
+        smin, smax = boxes[:, :3].min(0), boxes[:, 3:].max(0)
+        ext = np.maximum(smax - smin, 1e-6)
+        c = (boxes[:, :3] + boxes[:, 3:]) * 0.5
+        q = np.clip((c - smin) / ext * 2097152.0, 0.0, 2097151.0).astype(np.uint64)
+
+        def expand(v):
+            v = v & np.uint64(0x1FFFFF)
+            for sh, m in ((32, 0x1F00000000FFFF), (16, 0x1F0000FF0000FF), (8, 0x100F00F00F00F00F),
+                          (4, 0x10C30C30C30C30C3), (2, 0x1249249249249249)):
+                v = (v | (v << np.uint64(sh))) & np.uint64(m)
+            return v
+
+        codes = expand(q[:, 0]) | (expand(q[:, 1]) << np.uint64(1)) | (expand(q[:, 2]) << np.uint64(2))
+        assert (morton == codes).all(), f"call {call}: Morton codes differ"
+        assert (order == np.argsort(codes, kind="stable")).all(), f"call {call}: sorted order differs"
+
+
 def test_noalloc_rejects_oversized_input():
     import torch
     L = _lib.load()
