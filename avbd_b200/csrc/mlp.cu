@@ -425,19 +425,21 @@ __global__ void k_bias_act(float* Z, const float* bias, unsigned B, unsigned N, 
     if (HT) HT[(size_t)c * B + r] = hb;
 }
 
-// loss = mean over rows and the 3 outputs of (y - t)^2; dY = dloss/dy in
-// BF16 ([B][16] and [16][B]); db4 += column sums
+// loss = mean over rows and the 3 outputs of w (y - t)^2, w the row's
+// weight (target column 3); dY = dloss/dy in BF16 ([B][16] and [16][B]);
+// db4 += column sums
 __global__ void k_loss(const float* Y, const float* T, unsigned B, bf16* dY, bf16* dYT, float* loss, float* db4) {
     unsigned r = blockIdx.x * blockDim.x + threadIdx.x;
     float l = 0, g[AVBD_MLP_OUT] = {0, 0, 0};
     if (r < B) {
+        const float w = T[(size_t)r * 4 + 3];
 #pragma unroll
         for (int j = 0; j < (int)OUT; j++) {
             float d = 0;
             if (j < AVBD_MLP_OUT) {
                 float e = Y[(size_t)r * OUT + j] - T[(size_t)r * 4 + j];
-                l += e * e;
-                d = 2.0f * e / (float)(B * AVBD_MLP_OUT);
+                l += w * e * e;
+                d = 2.0f * w * e / (float)(B * AVBD_MLP_OUT);
                 g[j] = d;
             }
             bf16 db = __float2bfloat16_rn(d);

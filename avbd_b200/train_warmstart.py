@@ -1,7 +1,8 @@
 """Trains the learned warm start on trajectories of the plain GPU solver.
 
     python -m avbd_b200.train_warmstart [--scenes 256] [--steps 100]
-        [--samples 2000000] [--epochs 20] [--out avbd_b200/data/warmstart_mlp.npz]
+        [--samples 2000000] [--epochs 20] [--weighted]
+        [--out avbd_b200/data/warmstart_mlp.npz]
 
 Training data: batched uneven NeoHookean cubes (n ~ U{4..24} cells per side,
 E log-uniform 1e4..1e7, nu ~ U(0.3, 0.49), random rotation, ground contact)
@@ -35,17 +36,32 @@ def make_context(sc, device, tol, max_iters):
 
 
 def iterations_per_step(sc, params, steps, device, tol, max_iters):
-    """Scene-iterations per scene-step over `steps` steps, plain and learned."""
+    """Scene-iterations per scene-step over `steps` steps: plain, learned with
+    the acceptance test (kappa 0.5, the engine's default) and learned
+    applied to every vertex the residual gate admits (kappa 0)."""
     out = {}
-    for name, p in (("plain", None), ("learned", params)):
+    for name, p, kappa in (("plain", None, None), ("learned", params, "0.5"), ("learned_ungated", params, "0")):
         e = make_context(sc, device, tol, max_iters)
         if p is not None:
+            os.environ["AVBD_WS_KAPPA"] = kappa
             e.set_warmstart(2, p)
+            del os.environ["AVBD_WS_KAPPA"]
         e.step(steps)
         st = e.stats()
         out[name] = st["iterations"] / (steps * sc.num_scenes)
         e.close()
     return out
+
+
+def residual_weights(F):
+    """Row weights of the residual-weighted loss: a position error e (in
+    units of g h^2) changes the block residual (in units of m g) by about
+    (I + H h^2 / m) e, so rows are weighted by (1 + mean_a H_aa h^2 / m)^2
+    (features 18-20 hold log(1 + H_aa h^2 / m)), normalised to mean 1."""
+    import torch
+    lam = torch.expm1(F[:, 18:21].float()).mean(1)
+    w = (1.0 + lam) ** 2
+    return w / w.mean()
 
 
 def main(argv=None):
@@ -62,6 +78,8 @@ def main(argv=None):
     ap.add_argument("--max-iters", type=int, default=100)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--weighted", action="store_true",
+                    help="residual-weighted loss: rows weighted by (1 + H h^2/m)^2 (see residual_weights)")
     a = ap.parse_args(argv)
 
     import torch
@@ -80,6 +98,9 @@ def main(argv=None):
     e.close()
     t_data = time.time() - t0
     print(f"data: {F.shape[0]} training rows, {Fv.shape[0]} validation rows in {t_data:.1f} s", flush=True)
+    if a.weighted:
+        T[:, 3] = residual_weights(F)
+        Tv[:, 3] = residual_weights(Fv)
 
     t1 = time.time()
     params, rep = warmstart.train(F, T, Fv, Tv, epochs=a.epochs, batch=a.batch, lr=a.lr, device=a.device)
@@ -96,7 +117,10 @@ def main(argv=None):
               "batch": a.batch, "lr": a.lr, "loss_per_epoch": rep["loss"],
               "rms_inertial_guess": rep["rms_inertial_guess"], "rms_mlp_guess": rep["rms_mlp_guess"],
               "rms_ratio": rep["rms_ratio"], "iterations_per_scene_step": its, "data_s": round(t_data, 1),
-              "train_s": round(t_train, 1), "residual_tolerance": a.tol, "max_iters": a.max_iters}
+              "train_s": round(t_train, 1), "residual_tolerance": a.tol, "max_iters": a.max_iters,
+              "loss": "residual-weighted" if a.weighted else "unweighted",
+              "rms_weighted_mlp_guess": rep.get("rms_weighted_mlp_guess"),
+              "rms_weighted_inertial_guess": rep.get("rms_weighted_inertial_guess")}
     os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
     np.savez(out, params=params, mean=rep["mean"], std=rep["std"], out_std=rep["out_std"],
              report=json.dumps(report))

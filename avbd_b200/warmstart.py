@@ -266,8 +266,14 @@ def evaluate(params, Fv, Tv, device: int = 0):
     t = Tv[:, :OUT]
     rms_plain = float(torch.sqrt((t ** 2).sum(1).mean()))
     rms_mlp = float(torch.sqrt(((t - pred) ** 2).sum(1).mean()))
+    # the same distances weighted by (1 + mean_a H_aa h^2 / m)^2: a proxy for
+    # the residual each guess leaves (features 18-20 hold log(1 + H_aa h^2/m))
+    w = (1.0 + torch.expm1(Fv[:, 18:21].float()).mean(1)) ** 2
+    wr_plain = float(torch.sqrt((w * (t ** 2).sum(1)).mean()))
+    wr_mlp = float(torch.sqrt((w * ((t - pred) ** 2).sum(1)).mean()))
     return {"val_rows": int(Fv.shape[0]), "rms_inertial_guess": rms_plain, "rms_mlp_guess": rms_mlp,
-            "rms_ratio": rms_mlp / max(rms_plain, 1e-30)}
+            "rms_ratio": rms_mlp / max(rms_plain, 1e-30), "rms_weighted_inertial_guess": wr_plain,
+            "rms_weighted_mlp_guess": wr_mlp}
 
 
 def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:

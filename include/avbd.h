@@ -440,8 +440,9 @@ AVBD_API int avbd_mlp_destroy(avbd_mlp* m);
 AVBD_API int avbd_debug_set_wait_limit(int device, unsigned polls);
 
 /* Training: mini-batches of `batch` rows (a multiple of 128) of device
- * features (BF16 [batch][32]) and targets (FP32 [batch][4]); loss = mean
- * squared error over the 3 outputs; Adam (beta1 0.9, beta2 0.999, eps 1e-8)
+ * features (BF16 [batch][32]) and targets (FP32 [batch][4]: 3 outputs and
+ * the row's loss weight w); loss = mean over rows and outputs of
+ * w (y - t)^2; Adam (beta1 0.9, beta2 0.999, eps 1e-8)
  * on FP32 master weights.  avbd_mlp_trainer_grad evaluates the loss and the
  * gradient (host FP32 [AVBD_MLP_NPARAMS]) without updating. */
 typedef struct avbd_mlp_trainer avbd_mlp_trainer;

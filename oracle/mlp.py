@@ -61,14 +61,15 @@ def forward(p, X, bf16=False):
 
 
 def loss_and_grad(p, X, T, bf16=False):
-    """Mean squared error over rows and the 3 outputs, and its gradient
-    (flat, padding entries zero)."""
+    """Mean over rows and the 3 outputs of w (y - t)^2, w = T[:, 3] the row's
+    weight, and its gradient (flat, padding entries zero)."""
     y, c = forward(p, X, bf16)
     n = X.shape[0]
+    w = np.asarray(T[:, 3], dtype=np.float64)[:, None]
     e = np.zeros_like(y)
     e[:, :OUT] = y[:, :OUT] - T[:, :OUT]
-    loss = float((e[:, :OUT] ** 2).sum() / (n * OUT))
-    dy = 2.0 * e / (n * OUT)
+    loss = float((w * e[:, :OUT] ** 2).sum() / (n * OUT))
+    dy = 2.0 * w * e / (n * OUT)
     g = np.zeros(NPARAMS)
     W = c["W"]
     view(g, "W4")[:] = dy.T @ c["H3"]

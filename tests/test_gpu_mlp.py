@@ -69,6 +69,7 @@ def test_trainer_gradient_matches_fp64_reference():
     X = np.zeros((B, 32), dtype=np.float32)
     X[:, :27] = rng.normal(size=(B, 27))
     T = rng.normal(size=(B, 4)).astype(np.float32)
+    T[:, 3] = rng.uniform(0.5, 2.0, size=B)  # row weights of the loss
     tr = warmstart.Trainer(B, p)
     loss, g = tr.grad(bf(X), torch.tensor(T, device="cuda"))
     tr.close()
@@ -90,7 +91,7 @@ def test_trainer_fits_a_smooth_map():
     X = np.zeros((N, 32), dtype=np.float32)
     X[:, :27] = rng.normal(size=(N, 27))
     Amat = rng.normal(size=(27, 3)) / 5
-    T = np.zeros((N, 4), dtype=np.float32)
+    T = np.ones((N, 4), dtype=np.float32)
     T[:, :3] = np.tanh(X[:, :27]) @ Amat
     Xd, Td = bf(X), torch.tensor(T, device="cuda")
     tr = warmstart.Trainer(2048, warmstart.init_params(0))

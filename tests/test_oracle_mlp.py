@@ -19,6 +19,7 @@ def test_gradient_matches_central_differences():
     X = np.zeros((7, mlp.IN_PAD))
     X[:, :mlp.IN] = rng.normal(size=(7, mlp.IN))
     T = rng.normal(size=(7, 4))
+    T[:, 3] = rng.uniform(0.5, 2.0, size=7)  # row weights
     loss, g = mlp.loss_and_grad(p, X, T)
     idx = np.concatenate([rng.choice(np.arange(off, off + int(np.prod(sh))), 12, replace=False)
                           for off, sh in mlp.LAYOUT.values()])
