@@ -145,6 +145,8 @@ int avbd_create(avbd_ctx** out, int device, unsigned particles_capacity, unsigne
     }
     c->stream = c->own_stream;
     if (const char* g = getenv("AVBD_GRAPH")) c->use_graph = atoi(g) != 0;  // 0: no CUDA graphs
+    // condition threshold above which a block is re-solved in FP64 (0: always)
+    if (const char* km = getenv("AVBD_KAPPA_MAX")) c->kappa_max = atof(km);
     *out = c;
     return AVBD_OK;
 }
