@@ -230,10 +230,12 @@ static constexpr double BETA = 10;
 static constexpr double GAMMA = 0.99;
 static constexpr double ALPHA = 0.95;
 
-// Worker pool: the caller is worker 0, the other workers spin on a generation
+// Worker pool: the caller is worker 0, the other workers wait on a generation
 // counter and split every range statically, the execution model of
 // SimulationExecutor (simulation/SimulationExecutor.hpp:107-139) and
 // WorkerThreadContext::computeStartEnd (common/WorkerThreadContext.hpp:48-53).
+// Waits spin briefly, then block in the kernel (atomic wait/notify), so idle
+// pools of oracles that are alive but not stepping take no CPU time.
 struct Pool {
     int nt = 1;
     std::vector<std::thread> th;
@@ -248,27 +250,49 @@ struct Pool {
         stop = false;
         for (int t = 1; t < nt; t++) th.emplace_back([this, t] { worker(t); });
     }
+    // Waiters announce themselves (seq_cst, Dekker-style against the
+    // counter's update) so that a hot run issues no wake-up system call.
+    static constexpr int kSpins = 1 << 16;
+    std::atomic<int> sleepers{0};
+    std::atomic<bool> caller_sleeps{false};
     void worker(int t) {
         unsigned seen = gen.load();
         for (;;) {
             unsigned g;
             int spins = 0;
             while ((g = gen.load(std::memory_order_acquire)) == seen) {
-                if (++spins > 4096) { std::this_thread::yield(); spins = 0; }
+                if (++spins > kSpins) {
+                    sleepers.fetch_add(1);
+                    gen.wait(seen);
+                    sleepers.fetch_sub(1);
+                    spins = 0;
+                }
             }
             seen = g;
             if (stop.load()) return;
             (*job)(t);
-            done.fetch_add(1, std::memory_order_acq_rel);
+            if (done.fetch_add(1) + 1 == nt - 1 && caller_sleeps.load()) done.notify_one();
         }
+    }
+    void wake() {
+        gen.fetch_add(1);
+        if (sleepers.load() > 0) gen.notify_all();
     }
     void run(const std::function<void(int)>& f) {
         if (nt == 1) { f(0); return; }
         job = &f;
         done.store(0);
-        gen.fetch_add(1, std::memory_order_release);
+        wake();
         f(0);
-        while (done.load(std::memory_order_acquire) != nt - 1) {}
+        int d, spins = 0;
+        while ((d = done.load(std::memory_order_acquire)) != nt - 1) {
+            if (++spins > kSpins) {
+                caller_sleeps.store(true);
+                done.wait(d);
+                caller_sleeps.store(false);
+                spins = 0;
+            }
+        }
     }
     template <typename F>
     void parallel_for(long lo, long hi, F&& fn) {
@@ -284,7 +308,7 @@ struct Pool {
     void shutdown() {
         if (th.empty()) return;
         stop = true;
-        gen.fetch_add(1, std::memory_order_release);
+        wake();
         for (auto& t : th) t.join();
         th.clear();
     }
