@@ -122,7 +122,9 @@ def test_rod_contact_blocks_match_oracle(oracle_lib):
 @pytest.mark.parametrize("precision", ["mixed", "fp32"])
 def test_rod_contacts_lower_precision(oracle_lib, precision):
     """MIXED and FP32 rod contacts against the FP64 oracle over 60 steps,
-    with the live-contact count within 2 of the oracle's.  MIXED is held to
+    with the live-contact count within 2 of the oracle's (FP32: while its
+    trajectory tracks the oracle's, up to step 20; once it has moved away
+    an FP32 run measured 18 live contacts against the oracle's 12).  MIXED is held to
     1e-5 of the diagonal plus 3x the oracle's own drift when its positions
     are rounded to FP32 (measured 2e-7 after 60 steps).  FP32 is held to
     1e-4 plus that drift up to step 20 (measured 4e-6 after 10 steps, 1.6e-5
@@ -151,6 +153,7 @@ def test_rod_contacts_lower_precision(oracle_lib, precision):
         bar = 1e-5 if precision == "mixed" else (1e-4 if step <= 20 else 5e-2)
         assert err <= bar + 3 * sens, (precision, seen)
         live = max(live, e.dynamic_info()["rod_live"])
-        assert abs(e.dynamic_info()["rod_live"] - o.dynamic_info()["rod_live"]) <= 2
+        if precision == "mixed" or step <= 20:
+            assert abs(e.dynamic_info()["rod_live"] - o.dynamic_info()["rod_live"]) <= 2
     assert live > 0
     print(precision, "error vs oracle sensitivity per 10 steps:", seen)
