@@ -147,6 +147,11 @@ int avbd_create(avbd_ctx** out, int device, unsigned particles_capacity, unsigne
     if (const char* g = getenv("AVBD_GRAPH")) c->use_graph = atoi(g) != 0;  // 0: no CUDA graphs
     // condition threshold above which a block is re-solved in FP64 (0: always)
     if (const char* km = getenv("AVBD_KAPPA_MAX")) c->kappa_max = atof(km);
+    // the sweeps of run-to-tolerance steps as one persistent cooperative launch
+    // per iteration (default; 0 launches each color separately)
+    if (const char* ps = getenv("AVBD_PERSISTENT")) c->persistent = atoi(ps) != 0;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess) c->num_sms = (unsigned)sms;
     *out = c;
     return AVBD_OK;
 }
@@ -950,6 +955,12 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
             if ((rc = dalloc(c, &c->d_solve_ranges, pieces.size()))) return rc;
             CUDA_OR_FAIL(cudaMemcpyAsync(c->d_solve_ranges, pieces.data(), sizeof(uint4) * pieces.size(),
                                          cudaMemcpyHostToDevice, c->stream));
+            if (c->persistent) {
+                if ((rc = dalloc(c, &c->d_solve_range_off, nc + 1)) || (rc = dalloc(c, &c->d_sweep_sync, 3)))
+                    return rc;
+                CUDA_OR_FAIL(cudaMemcpyAsync(c->d_solve_range_off, c->solve_range_off.data(),
+                                             sizeof(uint32_t) * (nc + 1), cudaMemcpyHostToDevice, c->stream));
+            }
         }
         CUDA_OR_FAIL(cudaMemcpyAsync(c->d_scene_mg2, mg2.data(), sizeof(double) * S, cudaMemcpyHostToDevice, c->stream));
         CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
@@ -1020,6 +1031,8 @@ void enqueue_sweep(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_
         for (unsigned col = 0; col < nc; col++) dyn_solve_color<R>(c, s, k, col, st, T);
         return;
     }
+    // the persistent sweep covers tet-only contexts (no 6-DOF slabs between the colors)
+    if (T.active && c->persistent && s.no == 0 && launch_sweep_persistent<R>(c, s, k, st, T)) return;
     for (unsigned col = 0; col < c->num_colors; col++) {
         if (c->color_solve[col] && T.active && c->d_solve_ranges) {  // run-to-tolerance: per-scene pieces
             const unsigned r0 = c->solve_range_off[col], r1 = c->solve_range_off[col + 1];
@@ -1250,7 +1263,7 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
     StepConsts k = consts(c);
     cudaStream_t st = c->stream;
     // a step with dynamic contacts runs host work between its launches: no graph
-    const bool capturable = c->use_graph && !c->dyn && !c->ws_guess_pending && st != nullptr &&
+    bool capturable = c->use_graph && !c->dyn && !c->ws_guess_pending && st != nullptr &&
                             st != cudaStreamLegacy && st != cudaStreamPerThread;
     const bool tol_mode = c->solver.residual_tolerance > 0;
     if (c->graph && (c->graph_dirty || c->graph_tol != tol_mode || !capturable)) {
@@ -1271,9 +1284,21 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         const double tol = c->solver.residual_tolerance;
         SceneTol solveT{c->d_scene, c->d_scene_active, nullptr, c->d_scene_r2, nullptr};
         SceneTol resT{c->d_scene, nullptr, c->d_scene_cand, nullptr, c->d_scene_ex};
+        int gr = AVBD_OK;
+        if (capturable && !c->graph) {
+            gr = build_tol_graph<R>(c, s, k, st, max_it, tol, solveT, resT);
+            if (gr != AVBD_OK && c->persistent) {
+                // a graph that cannot hold the cooperative launch: the
+                // host-driven loop runs the same kernels from now on
+                cudaGetLastError();
+                c->use_graph = false;
+                capturable = false;
+                trace("persistent sweep: step graph not built, host-driven iteration loop");
+            } else if (gr != AVBD_OK) {
+                return gr;
+            }
+        }
         if (capturable) {
-            if (!c->graph)
-                if (int r = build_tol_graph<R>(c, s, k, st, max_it, tol, solveT, resT)) return r;
             for (unsigned t = 0; t < n_steps; t++) {
                 CUDA_OR_FAIL(cudaGraphLaunch(c->graph, st));
                 c->stats.kernel_launches += c->launches_per_step;
@@ -1348,6 +1373,13 @@ int device_error(avbd_ctx* c) {
     if (h == AVBD_ERR_CAPACITY)
         return fail(h, "a device buffer overflowed (candidate pairs, narrow-phase contacts or the traversal stack)");
     if (h == AVBD_ERR_COLORS) return fail(h, "Ran out of colors (more than 256)");
+    if (h == AVBD_ERR_BARRIER_TIMEOUT) {
+        // the launch gave up as a whole (every block left the kernel); the
+        // step's results are invalid, the context stays usable
+        CUDA_OR_FAIL(cudaMemsetAsync(c->d_error, 0, sizeof(int), c->stream));
+        CUDA_OR_FAIL(cudaStreamSynchronize(c->stream));
+        return fail(h, "a grid-barrier wait of the persistent sweep gave up");
+    }
     if (h) return fail(h, "device-side error");
     if (c->ws_mlp) return mlp_device_error(c->ws_mlp, c->stream);
     return AVBD_OK;
@@ -1613,20 +1645,31 @@ int profile_step_impl(avbd_ctx* c, DevState<R>& s, double* solve_ms, double* sol
             rc = fail(AVBD_ERR_CUDA, "profile: scene flags");
             break;
         }
+        // the persistent sweep: one launch (and its 12-byte sync reset) timed
+        // for all colors
+        bool persist = false;
+        if (c->persistent && s.no == 0) {
+            cudaEventRecord(ev[0], st);
+            persist = launch_sweep_persistent<R>(c, s, k, st, solveT);
+            cudaEventRecord(ev[1], st);
+        }
         for (unsigned col = 0; col < nc; col++) {
-            cudaEventRecord(ev[2 * col], st);
+            if (!persist) cudaEventRecord(ev[2 * col], st);
             if (c->color_solve[col]) {
-                const unsigned r0 = c->solve_range_off[col], r1 = c->solve_range_off[col + 1];
-                launch_solve_color<R>(c, s, k, 0, 0, st, solveT, nullptr, c->d_solve_ranges + r0, r1 - r0);
-                nl++;
+                if (!persist) {
+                    const unsigned r0 = c->solve_range_off[col], r1 = c->solve_range_off[col + 1];
+                    launch_solve_color<R>(c, s, k, 0, 0, st, solveT, nullptr, c->d_solve_ranges + r0, r1 - r0);
+                    nl++;
+                }
                 for (unsigned sc = 0; sc < S; sc++)
                     if (act[sc]) bytes += c->color_scene_bytes[(size_t)col * S + sc];
             }
-            cudaEventRecord(ev[2 * col + 1], st);
+            if (!persist) cudaEventRecord(ev[2 * col + 1], st);
             if (c->color_orient[col])
                 launch_solve_rod<R>(c, s, k, c->color_begin[col] + c->color_solve[col], c->color_orient[col], st,
                                     solveT, 0, nullptr);
         }
+        if (persist) nl++;
         enqueue_chebyshev<R>(c, s, k, omega, it, st, solveT);
         launch_tol_decide_a(c, tol, st);
         enqueue_residual<R>(c, s, k, nullptr, st, resT);
@@ -1637,7 +1680,7 @@ int profile_step_impl(avbd_ctx* c, DevState<R>& s, double* solve_ms, double* sol
             rc = fail(AVBD_ERR_CUDA, "profile: iteration count");
             break;
         }
-        for (unsigned col = 0; col < nc; col++) {
+        for (unsigned col = 0; col < (persist ? 1u : nc); col++) {
             float t = 0;
             if (cudaEventElapsedTime(&t, ev[2 * col], ev[2 * col + 1]) == cudaSuccess) ms += t;
         }

@@ -280,7 +280,14 @@ struct avbd_ctx {
     // run-to-tolerance steps launch one block per piece
     uint4* d_solve_ranges = nullptr;
     std::vector<unsigned> solve_range_off;
+    uint32_t* d_solve_range_off = nullptr;  // device copy of solve_range_off
     unsigned solve_chunk = 512;
+    // persistent sweep (default; AVBD_PERSISTENT=0 turns it off): all colors
+    // of an iteration in one cooperative launch with grid barriers;
+    // [ticket, arrivals, generation]
+    bool persistent = true;
+    uint32_t* d_sweep_sync = nullptr;
+    unsigned num_sms = 0;
     unsigned long long host_iterations = 0;  // scene-iterations of fixed-iteration steps
 
     // CUDA graph of one full step: fixed iterations, or (graph_tol) the
@@ -365,6 +372,12 @@ template <typename R>
 void launch_solve_color(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
                         cudaStream_t st, const SceneTol& T = SceneTol(), const uint32_t* list = nullptr,
                         const uint4* ranges = nullptr, unsigned nranges = 0);
+// the whole sweep of a run-to-tolerance iteration as one cooperative launch
+// (persistent contexts); false when the context does not qualify
+template <typename R>
+bool launch_sweep_persistent(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, const SceneTol& T);
+// poll limit of the persistent sweep's grid barriers (avbd_debug_set_wait_limit)
+int solve_set_wait_limit(unsigned polls);
 template <typename R>
 void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st,
                            const SceneTol& T = SceneTol());

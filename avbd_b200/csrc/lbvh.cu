@@ -203,25 +203,47 @@ __global__ void __launch_bounds__(RB) k_radix_count(const uint64_t* __restrict__
 }
 
 // Exclusive scan of the digit-major histogram (digit d of block b at d*nblk+b).
+// One block of 32 warps; warp w owns a contiguous segment and walks it 32
+// entries at a time with coalesced loads (the walk's loads do not depend on
+// the running carry, so they are in flight together): segment totals, a scan
+// of the 32 totals, then the segment's exclusive scan from its offset.
+// Integer sums, so the result does not depend on the split.
 __global__ void __launch_bounds__(1024) k_radix_scan(uint32_t* hist, unsigned total) {
-    __shared__ uint32_t part[1024];
-    unsigned per = (total + 1023) / 1024;
-    unsigned b = threadIdx.x * per, e = min(b + per, total);
+    __shared__ uint32_t wsum[32];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned seg = (total + 31u) / 32u;
+    const unsigned b = min(warp * seg, total), e = min(b + seg, total);
     uint32_t s = 0;
-    for (unsigned k = b; k < e; k++) s += hist[k];
-    part[threadIdx.x] = s;
+#pragma unroll 4
+    for (unsigned k = b + lane; k < e; k += 32u) s += hist[k];
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+    if (lane == 0) wsum[warp] = s;
     __syncthreads();
-    for (unsigned off = 1; off < 1024; off <<= 1) {
-        uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+    if (warp == 0) {
+        const uint32_t t = wsum[lane];
+        uint32_t incl = t;
+#pragma unroll
+        for (int m = 1; m < 32; m <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, m);
+            if (lane >= (unsigned)m) incl += u;
+        }
+        wsum[lane] = incl - t;
     }
-    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0;
-    for (unsigned k = b; k < e; k++) {
-        uint32_t v = hist[k];
-        hist[k] = run;
-        run += v;
+    __syncthreads();
+    uint32_t carry = wsum[warp];
+#pragma unroll 4
+    for (unsigned k0 = b; k0 < e; k0 += 32u) {
+        const unsigned k = k0 + lane;
+        const uint32_t v = k < e ? hist[k] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int m = 1; m < 32; m <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, m);
+            if (lane >= (unsigned)m) incl += u;
+        }
+        if (k < e) hist[k] = carry + incl - v;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
     }
 }
 
@@ -305,6 +327,12 @@ __global__ void __launch_bounds__(256) k_karras(LbvhState L, const uint64_t* key
     range[i] = make_uint2((unsigned)min(i, j), (unsigned)max(i, j));
 }
 
+AVBD_D unsigned atomic_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Bottom-up refit with one visit counter per internal node: the second child
 // to arrive computes the union (LBVHBuilder::assembleBVH).  min/max are exact,
 // so the result does not depend on arrival order.
@@ -319,9 +347,10 @@ __global__ void __launch_bounds__(256) k_refit(LbvhState L) {
     L.right[l] = INVALID;
     unsigned node = L.parent[l];
     while (node != INVALID) {
-        __threadfence();
-        if (atomicAdd(&L.visited[node], 1u) == 0) break;
-        __threadfence();
+        // the first child to arrive stops; the second combines both.  The
+        // count is an acquire-release RMW at device scope: the first arrival
+        // releases its subtree's writes, the second acquires them
+        if (atomic_add_acq_rel(&L.visited[node], 1u) == 0) break;
         unsigned a = L.left[node], c = L.right[node];
 #pragma unroll
         for (int k = 0; k < 3; k++) {

@@ -691,8 +691,10 @@ int avbd_debug_set_wait_limit(int device, unsigned polls) {
     if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess)
         return set_error(AVBD_ERR_NO_DEVICE, "cudaSetDevice failed");
     cudaError_t e = cudaMemcpyToSymbol(g_wait_polls, &polls, sizeof(polls));
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int rc = e == cudaSuccess ? solve_set_wait_limit(polls) : AVBD_OK;
+    if (e == cudaSuccess && rc == AVBD_OK) e = cudaDeviceSynchronize();
     cudaSetDevice(prev);
+    if (rc != AVBD_OK) return rc;
     return e == cudaSuccess ? AVBD_OK : set_error(AVBD_ERR_CUDA, cudaGetErrorString(e));
 }
 

@@ -660,7 +660,9 @@ template <typename R>
 void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned begin, unsigned count,
                       cudaStream_t st, const SceneTol& T, int mode, double* out, const uint32_t* list) {
     if (count == 0) return;
-    // nodes with contacts (lists; the debug pass) take 8 lanes, the static slabs one
+    // nodes with contacts (lists; the debug pass) take 8 lanes, the static
+    // slabs two (a node's rod elements split over a lane pair: 1,289 against
+    // 1,225 steps/s with one lane and 893 with eight on 256 rods x 100)
     const double km = k.kappa_max;
     unsigned long long* ctr = c->d_counters;  // [0]: blocks solved in FP64
     if (mode == RMODE_RESIDUAL)
@@ -670,7 +672,7 @@ void launch_solve_rod(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned
     else if (list)
         k_solve_rod<R, RMODE_SOLVE, 8><<<nblk(8 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
     else
-        k_solve_rod<R, RMODE_SOLVE, 1><<<nblk(count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
+        k_solve_rod<R, RMODE_SOLVE, 2><<<nblk(2 * count, ROD_BLOCK), ROD_BLOCK, 0, st>>>(s, begin, count, (R)k.dt, k.g, out, T, list, km, ctr);
     count_launch(c);
 }
 

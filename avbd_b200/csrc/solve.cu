@@ -235,11 +235,20 @@ AVBD_D void accumulate_tet_e(const DevState<P>& s, const RD& r, unsigned tet, V3
     }
 }
 
-template <typename P, typename RS, typename HT, bool DAMP>
+// COH: neighbour positions by coherent loads (the persistent sweep, whose own
+// launch writes them); otherwise through the read-only path.
+template <typename P, typename RS, typename HT, bool DAMP, bool COH = false>
 AVBD_D void accumulate_tet(const DevState<P>& s, const IncRec<RS>& r, V3<P> xi, P dt, Block3<P, HT>& B) {
-    V3<P> e1 = xyz(ld_ro(s.x + r.o[0])) - xi;
-    V3<P> e2 = xyz(ld_ro(s.x + r.o[1])) - xi;
-    V3<P> e3 = xyz(ld_ro(s.x + r.o[2])) - xi;
+    V3<P> e1, e2, e3;
+    if constexpr (COH) {
+        e1 = xyz(s.x[r.o[0]]) - xi;
+        e2 = xyz(s.x[r.o[1]]) - xi;
+        e3 = xyz(s.x[r.o[2]]) - xi;
+    } else {
+        e1 = xyz(ld_ro(s.x + r.o[0])) - xi;
+        e2 = xyz(ld_ro(s.x + r.o[1])) - xi;
+        e3 = xyz(ld_ro(s.x + r.o[2])) - xi;
+    }
     accumulate_tet_e<P, RS, HT, DAMP>(s, r, r.tet, e1, e2, e3, dt, B);
 }
 
@@ -309,7 +318,7 @@ struct SolveMinBlocks {
 // DYN: the instantiation for vertices with dynamic contact energies or a
 // color changed by the recoloring, launched over per-color lists; the slab
 // launches (DYN false) skip those vertices and carry no dynamic code.
-template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN, bool COH = false>
 __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS>* __restrict__ inc, unsigned begin,
                                            unsigned count, unsigned gi, unsigned lane, const Consts<P>& c,
                                            unsigned long long* counters, double* out, const SceneTol& T,
@@ -342,7 +351,7 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
             if (kn < e) prefetch_l1(inc + kn);
             IncRec<RS> r = load_rec<RS>(inc + k);
             if (kn + 3 * LANES < e) prefetch_l2(inc + kn + 3 * LANES);
-            accumulate_tet<P, RS, HT, DAMP>(s, r, xi, c.dt, B);
+            accumulate_tet<P, RS, HT, DAMP, COH>(s, r, xi, c.dt, B);
             if constexpr (MODE == MODE_FEATURES) {
 #pragma unroll
                 for (int j = 0; j < 3; j++) {
@@ -509,54 +518,136 @@ __device__ __forceinline__ void tet_vertex(const DevState<P>& s, const IncRec<RS
 // over the block: one atomic per piece instead of one per vertex on the
 // scene's sum.  Otherwise thread groups map to vertices [begin, begin +
 // count) (or to list).
+// One piece (at most 512 consecutive solved vertices of one scene in one
+// color slab) solved by one block; its residual terms are summed over the
+// block.  rg = (first vertex, count, scene).
+template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN, bool COH>
+__device__ __forceinline__ void solve_piece(const DevState<P>& s, const IncRec<RS>* __restrict__ inc, const uint4 rg,
+                                            const Consts<P>& c, unsigned long long* counters, double* out,
+                                            const SceneTol& T, const float4* __restrict__ aux,
+                                            const uint32_t* __restrict__ list) {
+    const unsigned lane = threadIdx.x % LANES;
+    const uint8_t* gate = MODE == MODE_SOLVE ? T.active : T.cand;
+    if (gate && !gate[rg.z]) return;
+    double* sum = MODE == MODE_SOLVE ? T.r2 : (MODE == MODE_RESIDUAL ? T.ex : nullptr);
+    SceneTol TB = T;  // gated above, for the whole block
+    TB.active = nullptr;
+    TB.cand = nullptr;
+    double acc = 0.0;
+    for (unsigned base = 0; base < rg.y; base += blockDim.x / LANES) {
+        // the first records of this thread group's next vertex are fetched
+        // into L2 while this one is solved (its first loads are then not
+        // DRAM misses)
+        const unsigned gn = base + blockDim.x / LANES + threadIdx.x / LANES;
+        if (gn < rg.y) {
+            const unsigned bn = s.inc_begin[rg.x + gn], en = s.inc_begin[rg.x + gn + 1];
+#pragma unroll
+            for (unsigned j = 0; j < 4; j++)
+                if (bn + lane + j * LANES < en) prefetch_l2(inc + bn + lane + j * LANES);
+        }
+        tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN, COH>(s, inc, rg.x, rg.y, base + threadIdx.x / LANES,
+                                                                   lane, c, counters, out, TB, aux, list,
+                                                                   sum ? &acc : nullptr);
+    }
+    if (sum) {
+        __shared__ double part[32];
+#pragma unroll
+        for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+        if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (unsigned w = 0; w < (blockDim.x >> 5); w++) t += part[w];
+            atomicAdd(sum + rg.z, t);
+        }
+    }
+}
+
 template <typename P, typename RS, typename HT, int LANES, bool DAMP, bool GROUND, int MODE, bool DYN>
 __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet(DevState<P> s, const IncRec<RS>* __restrict__ inc,
                                                    unsigned begin, unsigned count, Consts<P> c,
                                                    unsigned long long* counters, double* out, SceneTol T,
                                                    const float4* __restrict__ aux, const uint32_t* __restrict__ list,
                                                    const uint4* __restrict__ ranges) {
-    const unsigned lane = threadIdx.x % LANES;
     if (ranges) {
-        const uint4 rg = ranges[blockIdx.x];
-        const uint8_t* gate = MODE == MODE_SOLVE ? T.active : T.cand;
-        if (gate && !gate[rg.z]) return;
-        double* sum = MODE == MODE_SOLVE ? T.r2 : (MODE == MODE_RESIDUAL ? T.ex : nullptr);
-        SceneTol TB = T;  // gated above, for the whole block
-        TB.active = nullptr;
-        TB.cand = nullptr;
-        double acc = 0.0;
-        for (unsigned base = 0; base < rg.y; base += blockDim.x / LANES) {
-            // the first records of this thread group's next vertex are fetched
-            // into L2 while this one is solved (its first loads are then not
-            // DRAM misses)
-            const unsigned gn = base + blockDim.x / LANES + threadIdx.x / LANES;
-            if (gn < rg.y) {
-                const unsigned bn = s.inc_begin[rg.x + gn], en = s.inc_begin[rg.x + gn + 1];
-#pragma unroll
-                for (unsigned j = 0; j < 4; j++)
-                    if (bn + lane + j * LANES < en) prefetch_l2(inc + bn + lane + j * LANES);
-            }
-            tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, rg.x, rg.y, base + threadIdx.x / LANES, lane,
-                                                                  c, counters, out, TB, aux, list,
-                                                                  sum ? &acc : nullptr);
-        }
-        if (sum) {
-            __shared__ double part[32];
-#pragma unroll
-            for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
-            if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double t = 0.0;
-                for (unsigned w = 0; w < (blockDim.x >> 5); w++) t += part[w];
-                atomicAdd(sum + rg.z, t);
-            }
-        }
+        solve_piece<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN, false>(s, inc, ranges[blockIdx.x], c, counters, out, T,
+                                                                      aux, list);
         return;
     }
     const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
-    tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, begin, count, tid / LANES, lane, c, counters, out, T,
-                                                          aux, list);
+    tet_vertex<P, RS, HT, LANES, DAMP, GROUND, MODE, DYN>(s, inc, begin, count, tid / LANES, tid % LANES, c, counters,
+                                                          out, T, aux, list);
+}
+
+// Polls a grid-barrier wait of the persistent sweep may take before it gives
+// up (avbd_debug_set_wait_limit lowers it so that tests can make it run out).
+__device__ uint32_t g_sweep_wait_polls = AVBD_DEFAULT_WAIT_POLLS;
+
+// Barrier over every block of a cooperative launch.  sync[0] counts the
+// arrivals, sync[1] is the generation: thread 0 of the last block to arrive
+// resets the count and advances the generation, the others poll it at most
+// g_sweep_wait_polls times and then set AVBD_ERR_BARRIER_TIMEOUT.  A block
+// returns false when that error (or any other device error) is set, so that
+// every block leaves the kernel; the polls are bounded, so none waits forever.
+AVBD_D bool grid_barrier(unsigned* sync, int* err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned limit = *(volatile uint32_t*)&g_sweep_wait_polls;
+        const unsigned gen = *(volatile unsigned*)(sync + 1);
+        int good = 1;
+        __threadfence();
+        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
+            atomicExch(sync, 0u);
+            __threadfence();
+            atomicAdd(sync + 1, 1u);
+        } else {
+            unsigned polls = 0;
+            while (*(volatile unsigned*)(sync + 1) == gen) {
+                if (polls++ >= limit || *(volatile int*)err != 0) {
+                    good = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (!good) atomicCAS(err, 0, (int)AVBD_ERR_BARRIER_TIMEOUT);
+        ok = good && *(volatile int*)err == 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The whole sweep of a run-to-tolerance iteration in one cooperative launch:
+// for each color in turn the blocks draw its pieces from a shared ticket
+// counter (dynamic, so uneven pieces balance), then meet at a grid barrier
+// before the next color reads the positions this one wrote.  In color k each
+// block draws exactly one ticket past the color's pieces, so color k's tickets
+// start at sum over earlier colors of (pieces + blocks).  sync: [ticket,
+// arrivals, generation], zeroed before each launch.
+template <typename P, typename RS, typename HT, int LANES, bool GROUND>
+__global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value)
+    k_sweep_persistent(DevState<P> s, const IncRec<RS>* __restrict__ inc, Consts<P> c, unsigned long long* counters,
+                       SceneTol T, const uint4* __restrict__ ranges, const unsigned* __restrict__ color_off,
+                       unsigned ncolors, unsigned* sync) {
+    __shared__ unsigned ticket;
+    unsigned base = 0;
+    for (unsigned col = 0; col < ncolors; col++) {
+        const unsigned r0 = color_off[col], np = color_off[col + 1] - r0;
+        for (;;) {
+            __syncthreads();  // every thread has read the previous ticket
+            if (threadIdx.x == 0) ticket = atomicAdd(sync, 1u) - base;
+            __syncthreads();
+            const unsigned t = ticket;
+            if (t >= np) break;
+            solve_piece<P, RS, HT, LANES, false, GROUND, MODE_SOLVE, false, true>(s, inc, ranges[r0 + t], c,
+                                                                                  counters, nullptr, T, nullptr,
+                                                                                  nullptr);
+        }
+        base += np + gridDim.x;
+        if (col + 1 < ncolors && !grid_barrier(sync + 1, s.err)) return;
+    }
 }
 
 // Chebyshev acceleration of every particle fused with the ground-contact dual
@@ -779,6 +870,59 @@ static void solve_lanes(avbd_ctx* c, DevState<double>& s, const StepConsts& k, u
         solve_lanes_t<double, float, float, MODE>(c, s, s.inc32, k, begin, count, st, out, T, list, ranges, nranges);
     else
         solve_lanes_t<double, double, double, MODE>(c, s, s.inc, k, begin, count, st, out, T, list, ranges, nranges);
+}
+
+// The persistent sweep (default; AVBD_PERSISTENT=0 at context creation turns
+// it off): one cooperative launch per iteration instead of one per color.  Taken for the run-to-tolerance
+// sweeps of contexts whose solve runs 2 threads per vertex with no damping,
+// no oriented particles and no dynamic contacts (the caller checks the last
+// two); returns false, having launched nothing, otherwise.
+template <typename P, typename RS, typename HT>
+static bool sweep_persistent_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* inc, const StepConsts& k,
+                               cudaStream_t st, const SceneTol& T) {
+    if (!c->persistent || c->lanes != 2 || c->damping || !c->d_solve_ranges || !c->d_solve_range_off ||
+        !c->d_sweep_sync || c->num_sms == 0)
+        return false;
+    const bool ground = !c->ground.empty();
+    auto kern = ground ? k_sweep_persistent<P, RS, HT, 2, true> : k_sweep_persistent<P, RS, HT, 2, false>;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1)
+        return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)per_sm * c->num_sms);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaMemsetAsync(c->d_sweep_sync, 0, 3 * sizeof(unsigned), st);
+    // a failed launch is left in the runtime's last error, which the step checks
+    cudaLaunchKernelEx(&cfg, kern, s, inc, mkc<P>(k), c->d_counters, T, (const uint4*)c->d_solve_ranges,
+                       (const unsigned*)c->d_solve_range_off, c->num_colors, c->d_sweep_sync);
+    count_launch(c);
+    return true;
+}
+static bool sweep_persistent(avbd_ctx* c, DevState<float>& s, const StepConsts& k, cudaStream_t st,
+                             const SceneTol& T) {
+    return sweep_persistent_t<float, float, float>(c, s, s.inc, k, st, T);
+}
+static bool sweep_persistent(avbd_ctx* c, DevState<double>& s, const StepConsts& k, cudaStream_t st,
+                             const SceneTol& T) {
+    if (c->solver.precision == AVBD_PRECISION_MIXED)
+        return sweep_persistent_t<double, float, float>(c, s, s.inc32, k, st, T);
+    return sweep_persistent_t<double, double, double>(c, s, s.inc, k, st, T);
+}
+
+template <typename R>
+bool launch_sweep_persistent(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, const SceneTol& T) {
+    return sweep_persistent(c, s, k, st, T);
+}
+
+int solve_set_wait_limit(unsigned polls) {
+    cudaError_t e = cudaMemcpyToSymbol(g_sweep_wait_polls, &polls, sizeof(polls));
+    return e == cudaSuccess ? AVBD_OK : set_error(AVBD_ERR_CUDA, cudaGetErrorString(e));
 }
 
 template <typename R>
@@ -1006,6 +1150,8 @@ void launch_store_vec(const DevState<R>& s, int which, double* dst, const uint32
     template void launch_tet_eprev<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                \
     template void launch_solve_color<R>(avbd_ctx*, DevState<R>&, const StepConsts&, unsigned, unsigned,         \
                                         cudaStream_t, const SceneTol&, const uint32_t*, const uint4*, unsigned); \
+    template bool launch_sweep_persistent<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t,           \
+                                             const SceneTol&);                                                  \
     template void launch_chebyshev_dual<R>(avbd_ctx*, DevState<R>&, const StepConsts&, double, unsigned, cudaStream_t,    \
                                            const SceneTol&);                                                    \
     template void launch_velocity<R>(avbd_ctx*, DevState<R>&, const StepConsts&, cudaStream_t);                 \

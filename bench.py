@@ -549,12 +549,20 @@ def run_engine(args):
         per_launch_bytes = solve_bytes / max(1, solve_launches)
         achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
         workload = wl.name
+        # one solve launch per iteration: the persistent sweep (every color of
+        # the iteration in one cooperative launch)
+        persistent = wl.tol > 0 and not wl.rods and solve_launches == prof_iters
         kernel = ("k_solve_rod (per-color 6-DOF vertex block solve)" if wl.rods
-                  else "k_solve_tet (per-color vertex block solve)")
+                  else "k_sweep_persistent (vertex block solve, every color of an iteration in one launch)"
+                  if persistent else "k_solve_tet (per-color vertex block solve)")
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic_for(workload, per_launch_bytes), "kernel": kernel,
                 "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms, "peak_source": peak_kind,
-                "launch_shape": ("one run-to-tolerance step as timed: per-scene pieces of every color slab, "
+                "launch_shape": ("one run-to-tolerance step as timed: one persistent sweep per iteration, "
+                                 "blocks drawing the per-scene pieces of each color slab in turn, converged "
+                                 f"scenes gated out ({solve_launches} launches, {prof_iters} iterations)"
+                                 if persistent else
+                                 "one run-to-tolerance step as timed: per-scene pieces of every color slab, "
                                  f"converged scenes gated out ({solve_launches} launches, {prof_iters} iterations)"
                                  if wl.tol > 0 else f"whole color slabs ({solve_launches} launches, "
                                  f"{prof_iters} iterations)")}

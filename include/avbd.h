@@ -429,13 +429,19 @@ AVBD_API int avbd_mlp_forward(avbd_mlp* m, const void* features, unsigned n, flo
 AVBD_API int avbd_mlp_destroy(avbd_mlp* m);
 
 /* Debug hook with no counterpart in the reference: the number of polls a
- * tensor-core barrier wait of the MLP and GEMM kernels may take on `device`
- * before it gives up (AVBD_DEFAULT_WAIT_POLLS unless changed; 0 gives up at
- * once).  A wait that gives up sets AVBD_ERR_BARRIER_TIMEOUT, which the
- * launching call returns; every result of that launch is then invalid.  The
- * kernel still waits, bounded, for the MMAs it issued before it frees its
- * tensor memory, so the context stays usable.  Tests lower the limit to make
- * the wait run out without any fault. */
+ * bounded wait may take on `device` before it gives up
+ * (AVBD_DEFAULT_WAIT_POLLS unless changed; 0 gives up at once): the
+ * tensor-core barrier waits of the MLP and GEMM kernels, and the grid-barrier
+ * waits of the persistent sweep (unless AVBD_PERSISTENT=0 is in the
+ * environment when a context is created, each run-to-tolerance sweep of a
+ * tetrahedral context runs as one cooperative launch whose blocks meet at a
+ * grid barrier between colors).  A wait that gives up
+ * sets AVBD_ERR_BARRIER_TIMEOUT, which the launching call (avbd_step for the
+ * sweep) returns; every result of that launch is then invalid.  The MLP
+ * kernels still wait, bounded, for the MMAs they issued before they free
+ * their tensor memory, and every block of the sweep leaves the kernel, so the
+ * context stays usable.  Tests lower the limit to make the wait run out
+ * without any fault. */
 #define AVBD_DEFAULT_WAIT_POLLS (1u << 22)
 AVBD_API int avbd_debug_set_wait_limit(int device, unsigned polls);
 
