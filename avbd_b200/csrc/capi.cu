@@ -936,7 +936,10 @@ extern "C" int avbd_finalize(avbd_ctx* c) {
             }
         }
         // pieces of at most solve_chunk vertices for the sweeps (AVBD_SOLVE_CHUNK
-        // overrides; 0 launches whole slabs)
+        // overrides; 0 launches whole slabs): 256 for the persistent sweep,
+        // whose blocks draw pieces by ticket (a finer grain shortens each
+        // color's tail at its grid barrier), 512 for one block per piece
+        c->solve_chunk = c->persistent ? 256 : 512;
         if (const char* env = getenv("AVBD_SOLVE_CHUNK")) c->solve_chunk = (unsigned)atoi(env);
         c->solve_range_off.assign(nc + 1, 0);
         std::vector<uint4> pieces;
