@@ -131,9 +131,11 @@ def test_contacts_run_to_tolerance(oracle_lib):
     """Per-scene run-to-tolerance with contacts: iteration counts and states
     follow the oracle."""
     sc, e, o = pair(oracle_lib, "fp64", tol=1e-3, max_iters=200)
-    for _ in range(20):
+    for step in range(20):
+        i0e, i0o = e.stats()["iterations"], o.iterations
         e.step(1)
         o.step(1)
-    st = e.stats()
-    assert abs(st["iterations"] - o.iterations) <= 2 * 20, (st["iterations"], o.iterations)
+        # each step's iterations within 2 of the oracle's
+        de, do = e.stats()["iterations"] - i0e, o.iterations - i0o
+        assert abs(de - do) <= 2, (step, de, do)
     assert np.abs(e.positions() - o.positions()).max() / sc.bbox_diagonal() < 1e-6
