@@ -17,7 +17,9 @@ oracle (which tests/test_ref_pinning.py pins to the reference itself).
   FP32 rounding of its inputs (measured 7.1e-3 after 60 steps).
 * C3 -- 256 rods of 100 segments on one-sided fixed joints plus 64 spheres,
   rigid-body ground contact, 20 iterations: identical colors, FP64 and MIXED
-  positions within 1e-9, quaternions within 1e-8, over 20 steps.
+  positions within 1e-9, quaternions within 1e-8, over 20 steps; FP32 (the
+  rods workload's precision) within 1e-4 plus 3x the oracle's own FP32
+  sensitivity (measured 6.6e-5 after 20 steps), quaternions within 3e-3.
 """
 import os
 
@@ -144,3 +146,36 @@ def test_c3_rods_at_size(oracle_lib, precision):
             err = np.abs(e.positions() - o.positions()).max() / diag
             assert err <= 1e-9, f"step {step}: {err:.2e}"
             assert quat_err(e.rotations(), o.rotations()) <= 1e-8, step
+
+
+def test_c3_rods_at_size_fp32(oracle_lib):
+    """C3 in FP32 (the rods workload's precision: FP32 state, scaled FP32
+    LDL^T 6x6 solves with the FP64 re-solve above the condition threshold)
+    against the FP64 oracle over 20 steps, next to a second oracle started
+    from the initial state rounded to FP32.  Measured, as a fraction of the
+    bbox diagonal: 3.1e-7 after 1 step, 3.3e-6 after 5, 1.4e-5 after 10,
+    6.6e-5 after 20 (the oracle's own sensitivity 3e-8 .. 1.3e-6);
+    quaternions 2.5e-5 .. 1.6e-3.  Bars: 1e-4 plus 3x that sensitivity, and
+    3e-3 for the quaternions."""
+    sc = scenes.rods_and_spheres(num_rods=256, segments=100, num_spheres=64, seed=0)
+    e, o = _pair(oracle_lib, sc, "fp32")
+    o32 = oracle_lib.Oracle(threads=THREADS)
+    sc.load(o32)
+    o32.finalize()
+    o32.set_positions_raw(0, o32.positions().astype(np.float32).astype(np.float64))
+    diag = sc.bbox_diagonal()
+    seen = []
+    for step in range(1, 21):
+        e.step(1)
+        o.step(1)
+        o32.step(1)
+        if step in (1, 5, 10, 20):
+            X = o.positions()
+            err = np.abs(e.positions() - X).max() / diag
+            sens = np.abs(o32.positions() - X).max() / diag
+            qerr = quat_err(e.rotations(), o.rotations())
+            seen.append((step, float(f"{err:.3g}"), float(f"{sens:.3g}"), float(f"{qerr:.3g}")))
+    print("C3 FP32 (step, position error, oracle sensitivity, quaternion error):", seen)
+    for step, err, sens, qerr in seen:
+        assert err <= 1e-4 + 3 * sens, (step, err, sens)
+        assert qerr <= 3e-3, (step, qerr)
