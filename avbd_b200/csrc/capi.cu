@@ -64,6 +64,10 @@ static void free_device(avbd_ctx* c) {
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
     }
+    if (c->dyn_graph) {
+        cudaGraphExecDestroy(c->dyn_graph);
+        c->dyn_graph = nullptr;
+    }
     for (void* p : c->allocations) cudaFree(p);
     c->allocations.clear();
     dyn_destroy(c);
@@ -1092,6 +1096,61 @@ int enqueue_step_fixed(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStr
     return AVBD_OK;
 }
 
+int ensure_omega_table(avbd_ctx* c, unsigned n, cudaStream_t st);
+
+// A fixed-iteration step with dynamic contacts: the step start runs the
+// host contact management (so the step as a whole cannot be one graph), then
+// one iteration -- the sweep over the step's colors and contact lists,
+// Chebyshev with the contact dual updates, the index advance -- is recorded
+// as a graph whose iteration index and Chebyshev weight live in device
+// memory, and replayed solver_iters times: the same kernels with the same
+// arguments as the host loop's, a few microseconds of host time per
+// iteration instead of one launch call per kernel.  The executable graph is
+// updated in place while the launch sequence keeps its shape.
+template <typename R>
+int step_fixed_dyn_graph(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st) {
+    if (int r = enqueue_begin<R>(c, s, k, st)) return r;
+    const unsigned n = c->solver.solver_iters;
+    if (n > 0) {
+        if (int r = ensure_omega_table(c, n, st)) return r;
+        SceneTol T;
+        T.omega = c->d_tol_omega;
+        T.it = c->d_tol_it;
+        const unsigned long long before = c->stats.kernel_launches;
+        cudaGraph_t g = nullptr;
+        CUDA_OR_FAIL(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue_sweep<R>(c, s, k, st, SceneTol());
+        enqueue_chebyshev<R>(c, s, k, 1.0, 0, st, T);
+        launch_iter_next(c, n, st);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        const unsigned long long per_iter = c->stats.kernel_launches - before;
+        c->stats.kernel_launches = before;
+        if (e != cudaSuccess) return fail(AVBD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        if (c->dyn_graph) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(c->dyn_graph, g, &info) != cudaSuccess) {
+                cudaGetLastError();  // a changed shape: instantiated anew below
+                cudaGraphExecDestroy(c->dyn_graph);
+                c->dyn_graph = nullptr;
+            }
+        }
+        if (!c->dyn_graph) {
+            e = cudaGraphInstantiate(&c->dyn_graph, g, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(g);
+                c->dyn_graph = nullptr;
+                return fail(AVBD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+        }
+        cudaGraphDestroy(g);
+        launch_iter_set(c, st);
+        for (unsigned i = 0; i < n; i++) CUDA_OR_FAIL(cudaGraphLaunch(c->dyn_graph, st));
+        c->stats.kernel_launches += per_iter * n;
+    }
+    enqueue_velocity<R>(c, s, k, st);
+    return AVBD_OK;
+}
+
 StepConsts consts(avbd_ctx* c) { return StepConsts{c->params.dt, c->params.g_accel, c->kappa_max}; }
 
 // Picks the threads-per-vertex of the tet solve (1, 2, 4, 8, 16 or 32) by timing one
@@ -1158,6 +1217,32 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
     return AVBD_OK;
 }
 
+// Chebyshev weights omega(0..n-1) of the context's rho in device memory (for
+// the device-driven loops), computed on the host by the recurrence the host
+// loop uses; rebuilt only when n grows or rho changes.
+int ensure_omega_table(avbd_ctx* c, unsigned n, cudaStream_t st) {
+    const double rho = c->solver.iter_acceleration;
+    if (c->omega_tab_n >= n && c->omega_tab_rho == rho) return AVBD_OK;
+    if (c->omega_tab_n < n) {
+        if (c->d_omega_tab) {
+            CUDA_OR_FAIL(cudaStreamSynchronize(st));
+            cudaFree(c->d_omega_tab);
+            c->allocations.erase(std::find(c->allocations.begin(), c->allocations.end(), (void*)c->d_omega_tab));
+            c->d_omega_tab = nullptr;
+            c->omega_tab_n = 0;
+        }
+        if (int r = dalloc(c, &c->d_omega_tab, n)) return r;
+        c->omega_tab_n = n;
+    }
+    std::vector<double> tab(c->omega_tab_n);
+    double w = 1;
+    for (unsigned i = 0; i < c->omega_tab_n; i++) tab[i] = w = omega_at(i, rho, w);
+    CUDA_OR_FAIL(cudaMemcpyAsync(c->d_omega_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, st));
+    CUDA_OR_FAIL(cudaStreamSynchronize(st));
+    c->omega_tab_rho = rho;
+    return AVBD_OK;
+}
+
 // Records the run-to-tolerance step as one CUDA graph: the step start, a
 // conditional while node whose body is one iteration (sweep, Chebyshev,
 // in-sweep decision, candidates' exact residual, stop decision, loop
@@ -1168,22 +1253,7 @@ int autotune_impl(avbd_ctx* c, DevState<R>& s) {
 template <typename R>
 int build_tol_graph(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, unsigned max_it, double tol,
                     const SceneTol& solveT, const SceneTol& resT) {
-    if (c->omega_tab_n < max_it) {
-        if (c->d_omega_tab) {
-            CUDA_OR_FAIL(cudaStreamSynchronize(st));
-            cudaFree(c->d_omega_tab);
-            c->allocations.erase(std::find(c->allocations.begin(), c->allocations.end(), (void*)c->d_omega_tab));
-            c->d_omega_tab = nullptr;
-            c->omega_tab_n = 0;
-        }
-        if (int r = dalloc(c, &c->d_omega_tab, max_it)) return r;
-        c->omega_tab_n = max_it;
-    }
-    std::vector<double> tab(max_it);
-    double w = 1;
-    for (unsigned i = 0; i < max_it; i++) tab[i] = w = omega_at(i, c->solver.iter_acceleration, w);
-    CUDA_OR_FAIL(cudaMemcpyAsync(c->d_omega_tab, tab.data(), sizeof(double) * max_it, cudaMemcpyHostToDevice, st));
-    CUDA_OR_FAIL(cudaStreamSynchronize(st));
+    if (int r = ensure_omega_table(c, max_it, st)) return r;
 
     SceneTol loopT = solveT;
     loopT.omega = c->d_tol_omega;
@@ -1345,10 +1415,16 @@ int step_impl(avbd_ctx* c, DevState<R>& s, unsigned n_steps) {
         c->graph_tol = false;
         c->graph_dirty = false;
     }
+    // a step with dynamic contacts replays a one-iteration graph after its
+    // host part (where graphs are allowed and the stream can be captured)
+    const bool dyn_graph = c->dyn && c->use_graph && !c->ws_guess_pending && st != nullptr &&
+                           st != cudaStreamLegacy && st != cudaStreamPerThread;
     for (unsigned t = 0; t < n_steps; t++) {
         if (capturable) {
             CUDA_OR_FAIL(cudaGraphLaunch(c->graph, st));
             c->stats.kernel_launches += c->launches_per_step;
+        } else if (dyn_graph) {
+            if (int r = step_fixed_dyn_graph<R>(c, s, k, st)) return r;
         } else {
             if (int r = enqueue_step_fixed<R>(c, s, k, st)) return r;
         }

@@ -274,6 +274,12 @@ struct avbd_ctx {
     double* d_tol_omega = nullptr;
     double* d_omega_tab = nullptr;
     unsigned omega_tab_n = 0;
+    double omega_tab_rho = -1;          // the rho the table was computed for
+    // one iteration (sweep, Chebyshev, index advance) of a fixed-iteration
+    // step with dynamic contacts, recorded after the step's host contact
+    // management and replayed solver_iters times; updated in place while
+    // the iteration's launch sequence keeps its shape
+    cudaGraphExec_t dyn_graph = nullptr;
     // (first internal vertex, count, scene) pieces of at most solve_chunk
     // vertices of each scene's solved vertices in each color slab, color by
     // color (offsets solve_range_off): the sweeps and the residual pass of
@@ -406,6 +412,10 @@ void launch_tol_decide_a(avbd_ctx* c, double tol, cudaStream_t st);
 void launch_tol_decide_b(avbd_ctx* c, double tol, unsigned max_it, cudaStream_t st);
 void launch_tol_loop_next(avbd_ctx* c, cudaGraphConditionalHandle h, unsigned max_it, unsigned body_launches,
                           cudaStream_t st);
+// iteration index / Chebyshev weight in device memory for the one-iteration
+// graph of fixed-iteration steps: set to iteration 0, advanced by one
+void launch_iter_set(avbd_ctx* c, cudaStream_t st);
+void launch_iter_next(avbd_ctx* c, unsigned n, cudaStream_t st);
 template <typename R>
 void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st);
 template <typename R>

@@ -1083,6 +1083,24 @@ void launch_tol_loop_next(avbd_ctx* c, cudaGraphConditionalHandle h, unsigned ma
                                      body_launches + 1ull, c->d_counters + 5);
 }
 
+__global__ void k_iter_set(uint32_t* it, double* omega, const double* omega_tab) {
+    *it = 0;
+    *omega = omega_tab[0];
+}
+__global__ void k_iter_next(uint32_t* it, double* omega, const double* omega_tab, unsigned n) {
+    const uint32_t i = *it + 1;
+    *it = i;
+    if (i < n) *omega = omega_tab[i];
+}
+void launch_iter_set(avbd_ctx* c, cudaStream_t st) {
+    k_iter_set<<<1, 1, 0, st>>>(c->d_tol_it, c->d_tol_omega, c->d_omega_tab);
+    count_launch(c);
+}
+void launch_iter_next(avbd_ctx* c, unsigned n, cudaStream_t st) {
+    k_iter_next<<<1, 1, 0, st>>>(c->d_tol_it, c->d_tol_omega, c->d_omega_tab, n);
+    count_launch(c);
+}
+
 template <typename R>
 void launch_debug_block(avbd_ctx* c, DevState<R>& s, const StepConsts& k, unsigned p, double* out, cudaStream_t st) {
     solve_lanes<MODE_DEBUG>(c, s, k, p, 1, st, out, SceneTol());
