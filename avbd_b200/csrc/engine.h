@@ -294,6 +294,7 @@ struct avbd_ctx {
     bool persistent = true;
     uint32_t* d_sweep_sync = nullptr;
     unsigned num_sms = 0;
+    int sweep_blocks_per_sm = 0;        // 0: not queried yet, -1: the kernel cannot run
     unsigned long long host_iterations = 0;  // scene-iterations of fixed-iteration steps
 
     // CUDA graph of one full step: fixed iterations, or (graph_tol) the

@@ -885,9 +885,18 @@ static bool sweep_persistent_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* in
         return false;
     const bool ground = !c->ground.empty();
     auto kern = ground ? k_sweep_persistent<P, RS, HT, 2, true> : k_sweep_persistent<P, RS, HT, 2, false>;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1)
-        return false;
+    // resident blocks per SM of this context's instantiation, queried once
+    if (c->sweep_blocks_per_sm == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1) {
+            cudaGetLastError();
+            c->sweep_blocks_per_sm = -1;
+        } else {
+            c->sweep_blocks_per_sm = per_sm;
+        }
+    }
+    if (c->sweep_blocks_per_sm < 1) return false;
+    const int per_sm = c->sweep_blocks_per_sm;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)per_sm * c->num_sms);
     cfg.blockDim = dim3(256);
