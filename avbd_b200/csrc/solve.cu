@@ -886,9 +886,12 @@ static bool sweep_persistent_t(avbd_ctx* c, DevState<P>& s, const IncRec<RS>* in
     const bool ground = !c->ground.empty();
     auto kern = ground ? k_sweep_persistent<P, RS, HT, 2, true> : k_sweep_persistent<P, RS, HT, 2, false>;
     // resident blocks per SM of this context's instantiation, queried once
+    // (-1 where the device cannot launch cooperative kernels: per-color
+    // launches then)
     if (c->sweep_blocks_per_sm == 0) {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1) {
+        int per_sm = 0, coop = 0;
+        if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device) != cudaSuccess || !coop ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1) {
             cudaGetLastError();
             c->sweep_blocks_per_sm = -1;
         } else {
