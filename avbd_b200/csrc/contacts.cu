@@ -64,20 +64,29 @@ struct DynHost {
         unsigned e_idx;
     };
     std::vector<Det> cur, prev;
-    // ---- adjacency and coloring (reference particle ids)
-    std::vector<unsigned> p_off, p_nbr;          // static neighbours
+    // ---- dynamic adjacency (reference particle ids, built on the host)
     std::vector<unsigned> dyn_off, dnb_off, dnb; // dynamic entries per particle, dynamic neighbours
     std::vector<uint32_t> dyn_ent_ext;           // slot << 4 | pool << 3 | local
-    std::vector<unsigned> color, slab_color;
-    unsigned num_colors = 0;
-    std::vector<unsigned> last_dirty, dirty, next_dirty, touched_frame, cand, touched_conflicted;
-    std::vector<uint8_t> conflicted;
+    std::vector<uint32_t> marks;                 // particles of this stage's new contacts (to mark dirty)
     unsigned rounds = 6;  // ColorList::incrementalRecoloring MAX_COLOR_ITERS
-    // ---- device-side products (engine vertex order)
+    // ---- coloring on the device (reference particle ids): colors, the
+    // dirty set (two lists by round parity), last-dirty labels, conflicts
+    unsigned num_colors = 0;                     // after the last recoloring
+    unsigned dirty_count = 0, conflicted_count = 0;
+    uint32_t *d_color = nullptr, *d_cand = nullptr, *d_last_dirty = nullptr;
+    uint32_t *d_dirty0 = nullptr, *d_dirty1 = nullptr;
+    uint8_t* d_touched = nullptr;
+    uint32_t* d_confl_ext = nullptr;
+    uint32_t *d_p_off = nullptr, *d_p_nbr = nullptr, *d_dnb_off = nullptr, *d_dnb = nullptr;
+    uint32_t *d_marks = nullptr, *d_slab = nullptr;
+    uint32_t* d_ctr = nullptr;                   // RC_* counters
+    uint32_t* d_lc = nullptr;                    // per-color list counts and cursors
+    uint32_t* d_summary = nullptr;               // RC_SUMMARY words for the host
+    uint32_t* h_summary = nullptr;               // pinned copy
+    unsigned dnb_cap = 0, marks_cap = 0;
+    // ---- per-color lists (engine vertex order) on the device
     std::vector<unsigned> off3, off6, offc;      // per color: recolored 3-DOF, 6-DOF, conflicted
-    std::vector<uint32_t> lists, dyn_begin, dyn_ent;
-    std::vector<uint8_t> skip, confl;
-    std::vector<uint8_t> skip_dev, confl_dev;    // what the device holds
+    std::vector<uint32_t> dyn_begin, dyn_ent;
     uint32_t* d_lists = nullptr;
     unsigned ent_cap = 0;
     bool csr_dirty = true;
@@ -163,13 +172,9 @@ int pool_free(DynHost::Pool& P, unsigned slot) {
     return AVBD_OK;
 }
 
-void mark_dirty(DynHost& D, unsigned p) {
-    if (D.last_dirty[p] != 0) {
-        D.last_dirty[p] = 0;
-        D.touched_frame.push_back(p);
-        D.dirty.push_back(p);
-    }
-}
+// ColorList::markParticleDirty: recorded here, applied on the device before
+// the recoloring (k_rc_mark)
+void mark_dirty(DynHost& D, unsigned p) { D.marks.push_back(p); }
 
 // _addCollision: k_start from the smallest mass of the contact's particles,
 // frame from the normal, all its particles dirty
@@ -278,114 +283,195 @@ void build_dynamic_adjacency(DynHost& D, unsigned n) {
     }
 }
 
+// ---------------------------------------------- recoloring on the device
+// ColorList::incrementalRecoloring, finalizeConflicts and the per-color
+// work lists (common/ColorList.hpp:381-522) over reference particle ids.
+// A round computes every dirty particle's candidate from the current colors
+// and only then applies them (the reference's rounds are Jacobi-style), so
+// one kernel per half-round gives the reference's colors exactly; the dirty
+// set, its last-dirty labels and the conflicts are sets, so the order in
+// which threads append to them changes nothing.
+enum : unsigned { RC_CNT0 = 0, RC_CNT1 = 1, RC_CUR = 2, RC_NCONFL = 3, RC_NCOLORS = 4, RC_ERR = 5, RC_NCTR = 8 };
+constexpr unsigned RC_MAXC = 256;  // colors (ColorList's bitset)
+// summary for the host: [num_colors, dirty count, conflicted count, error,
+// off3[0..256], off6[0..256], offc[0..256]]
+constexpr unsigned RC_SUMMARY = 4 + 3 * (RC_MAXC + 1);
+
+struct RcDev {
+    uint32_t *color, *cand, *last_dirty, *dirty0, *dirty1, *ctr;
+    uint8_t* touched;
+    uint32_t* confl;
+    const uint32_t *p_off, *p_nbr, *dnb_off, *dnb;
+};
+
 template <typename F>
-void for_each_neighbor(const DynHost& D, unsigned p, F&& f) {
-    for (unsigned k = D.p_off[p]; k < D.p_off[p + 1]; k++) f(D.p_nbr[k]);
-    for (unsigned k = D.dnb_off[p]; k < D.dnb_off[p + 1]; k++) f(D.dnb[k]);
+AVBD_D void rc_neighbors(const RcDev& R, unsigned p, F&& f) {
+    for (unsigned k = R.p_off[p]; k < R.p_off[p + 1]; k++) f(R.p_nbr[k]);
+    for (unsigned k = R.dnb_off[p]; k < R.dnb_off[p + 1]; k++) f(R.dnb[k]);
 }
 
-int finalize_conflicts(DynHost& D) {
-    for (unsigned p : D.dirty)
-        for_each_neighbor(D, p, [&](unsigned q) {
-            if (D.color[q] == D.color[p]) {
-                if (!D.conflicted[p]) { D.conflicted[p] = 1; D.touched_conflicted.push_back(p); }
-                if (!D.conflicted[q]) { D.conflicted[q] = 1; D.touched_conflicted.push_back(q); }
+// the conflicts of the last stage are cleared, then this stage's new
+// contacts' particles join the dirty set (those already in it keep label 0)
+__global__ void k_rc_mark(RcDev R, const uint32_t* __restrict__ marks, unsigned nmarks) {
+    const unsigned cur = R.ctr[RC_CUR];
+    uint32_t* list = cur ? R.dirty1 : R.dirty0;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < nmarks; j += gridDim.x * blockDim.x) {
+        const unsigned p = marks[j];
+        if (atomicExch(R.last_dirty + p, 0u) != 0u) {
+            R.touched[p] = 1;
+            list[atomicAdd(R.ctr + cur, 1u)] = p;
+        }
+    }
+}
+
+// half-round 1: a dirty particle sharing its color with a lower-numbered
+// neighbour takes the smallest color no neighbour holds
+__global__ void k_rc_cand(RcDev R) {
+    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+    const uint32_t* list = cur ? R.dirty1 : R.dirty0;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+        const unsigned p = list[j], cp = R.color[p];
+        uint32_t bits[RC_MAXC / 32] = {0, 0, 0, 0, 0, 0, 0, 0};
+        bool must = false, over = false;
+        rc_neighbors(R, p, [&](unsigned q) {
+            const unsigned cq = R.color[q];
+            if (cq >= RC_MAXC) {
+                over = true;
+                return;
+            }
+            bits[cq >> 5] |= 1u << (cq & 31u);
+            if (cq == cp && q < p) must = true;
+        });
+        unsigned cand = cp;
+        if (over) {
+            atomicExch(R.ctr + RC_ERR, 1u);
+        } else if (must) {
+            cand = RC_MAXC;
+            for (unsigned w = 0; w < RC_MAXC / 32 && cand == RC_MAXC; w++)
+                if (~bits[w]) cand = w * 32 + (unsigned)__ffs((int)~bits[w]) - 1u;
+            if (cand == RC_MAXC) {
+                atomicExch(R.ctr + RC_ERR, 1u);
+                cand = cp;
+            } else {
+                atomicMax(R.ctr + RC_NCOLORS, cand + 1u);  // cand <= num_colors: one new color at most
+            }
+        }
+        R.cand[p] = cand;
+    }
+}
+
+// half-round 2: candidates applied; every neighbour of a changed particle
+// joins the next round's dirty set, once per round (label = round + 1)
+__global__ void k_rc_apply(RcDev R, unsigned label) {
+    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+    const uint32_t* list = cur ? R.dirty1 : R.dirty0;
+    uint32_t* next = cur ? R.dirty0 : R.dirty1;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+        const unsigned p = list[j];
+        if (R.cand[p] == R.color[p]) continue;
+        R.color[p] = R.cand[p];
+        rc_neighbors(R, p, [&](unsigned q) {
+            if (atomicExch(R.last_dirty + q, label) != label) {
+                R.touched[q] = 1;
+                next[atomicAdd(R.ctr + (cur ^ 1u), 1u)] = q;
             }
         });
-    return AVBD_OK;
+    }
 }
 
-// ColorList::incrementalRecoloring (at most D.rounds rounds, 256 colors)
-int incremental_recoloring(DynHost& D) {
-    for (unsigned p : D.touched_conflicted) D.conflicted[p] = 0;
-    D.touched_conflicted.clear();
-    unsigned iter = 0;
-    bool overflow = false;
-    while (!D.dirty.empty() && iter < D.rounds) {
-        for (unsigned p : D.dirty) {
-            uint64_t bits[4] = {0, 0, 0, 0};
-            bool must = false;
-            for_each_neighbor(D, p, [&](unsigned q) {
-                const unsigned cq = D.color[q];
-                if (cq >= 256) { overflow = true; return; }
-                bits[cq / 64] |= 1ull << (cq % 64);
-                if (cq == D.color[p] && q < p) must = true;
-            });
-            if (overflow) return set_error(AVBD_ERR_COLORS, "Ran out of colors!");
-            if (must) {
-                unsigned cand = UINT32_MAX;
-                for (unsigned w = 0; w < 4 && cand == UINT32_MAX; w++)
-                    if (~bits[w]) cand = w * 64 + (unsigned)__builtin_ctzll(~bits[w]);
-                if (cand == UINT32_MAX) return set_error(AVBD_ERR_COLORS, "Ran out of colors!");
-                D.cand[p] = cand;
-                if (cand >= D.num_colors) D.num_colors++;
-            } else {
-                D.cand[p] = D.color[p];
-            }
-        }
-        D.next_dirty.clear();
-        for (unsigned p : D.dirty) {
-            if (D.cand[p] == D.color[p]) continue;
-            D.color[p] = D.cand[p];
-            for_each_neighbor(D, p, [&](unsigned q) {
-                if (D.last_dirty[q] != iter + 1) {
-                    D.last_dirty[q] = iter + 1;
-                    D.touched_frame.push_back(q);
-                    D.next_dirty.push_back(q);
-                }
-            });
-        }
-        D.dirty.swap(D.next_dirty);
-        iter++;
-    }
-    if (!D.dirty.empty()) finalize_conflicts(D);
-    for (unsigned p : D.touched_frame) D.last_dirty[p] = DIRTY_SENTINEL;
-    D.touched_frame.clear();
-    for (unsigned p : D.dirty) D.last_dirty[p] = 0;
-    return AVBD_OK;
+// the next round's list becomes current, the consumed one is emptied
+__global__ void k_rc_flip(RcDev R) {
+    const unsigned cur = R.ctr[RC_CUR];
+    R.ctr[cur] = 0;
+    R.ctr[RC_CUR] = cur ^ 1u;
 }
 
-// Lists of the engine's vertex order: per color the positional and oriented
-// vertices that have contacts or a color changed by the recoloring (solved by
-// the dynamic instantiation of the solve) and the conflicted vertices to
-// commit; skip and conflict flags per vertex.
-void build_lists(avbd_ctx* c, DynHost& D) {
-    const unsigned n = (unsigned)c->perm.size(), nc = D.num_colors;
-    std::vector<unsigned> c3(nc, 0), c6(nc, 0), cc(nc, 0);
-    D.skip.assign(n, 0);
-    D.confl.assign(n, 0);
-    for (unsigned i = 0; i < n; i++) {
-        const unsigned e = c->perm[i];
-        if (D.conflicted[e]) {
-            D.confl[i] = 1;
-            cc[D.color[e]]++;
-        }
-        if (D.color[e] == D.slab_color[i] && D.dyn_off[e + 1] == D.dyn_off[e]) continue;
-        D.skip[i] = 1;
-        if (c->fixed[e]) continue;
-        if (c->rot[e] != UINT32_MAX) c6[D.color[e]]++;
-        else c3[D.color[e]]++;
+// finalizeConflicts: particles still dirty after the last round and their
+// same-colored neighbours are conflicted
+__global__ void k_rc_conflicts(RcDev R) {
+    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+    const uint32_t* list = cur ? R.dirty1 : R.dirty0;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+        const unsigned p = list[j], cp = R.color[p];
+        rc_neighbors(R, p, [&](unsigned q) {
+            if (R.color[q] != cp) return;
+            if (atomicExch(R.confl + p, 1u) == 0u) atomicAdd(R.ctr + RC_NCONFL, 1u);
+            if (atomicExch(R.confl + q, 1u) == 0u) atomicAdd(R.ctr + RC_NCONFL, 1u);
+        });
     }
-    D.off3.assign(nc + 1, 0);
-    D.off6.assign(nc + 1, 0);
-    D.offc.assign(nc + 1, 0);
+}
+
+// labels written this stage go back to the sentinel ...
+__global__ void k_rc_settle(RcDev R, unsigned n) {
+    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        if (R.touched[p]) {
+            R.touched[p] = 0;
+            R.last_dirty[p] = DIRTY_SENTINEL;
+        }
+}
+// ... and the particles still dirty carry label 0 into the next stage
+__global__ void k_rc_keep(RcDev R) {
+    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+    const uint32_t* list = cur ? R.dirty1 : R.dirty0;
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x)
+        R.last_dirty[list[j]] = 0;
+}
+
+// Per-color lists in the engine's vertex order: a vertex with dynamic
+// entries or a color other than its slab's is skipped by the slab launch and
+// solved from its color's list (positional or oriented; fixed vertices are
+// skipped and not listed); conflicted vertices are listed for the commit.
+// lc: counts [3][256] then cursors [3][256].
+__global__ void k_rc_count(RcDev R, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ slab,
+                           const uint32_t* __restrict__ dyn_begin, const uint8_t* __restrict__ flags,
+                           uint8_t* skip, uint8_t* confl_eng, uint32_t* lc, unsigned n) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned e = perm[i], ce = R.color[e];
+        const uint8_t cf = R.confl[e] ? 1 : 0;
+        confl_eng[i] = cf;
+        if (cf) atomicAdd(lc + 2 * RC_MAXC + ce, 1u);
+        const bool sk = ce != slab[i] || dyn_begin[i + 1] != dyn_begin[i];
+        skip[i] = sk ? 1 : 0;
+        if (!sk || (flags[i] & VF_FIXED)) continue;
+        atomicAdd(lc + ((flags[i] & VF_ORIENTED) ? RC_MAXC : 0u) + ce, 1u);
+    }
+}
+
+// offsets: all positional lists, then all oriented, then all conflicted;
+// the summary the host reads back
+__global__ void k_rc_offsets(RcDev R, uint32_t* lc, uint32_t* summary) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const unsigned nc = min(R.ctr[RC_NCOLORS], RC_MAXC);
     unsigned run = 0;
-    for (unsigned k = 0; k < nc; k++) { D.off3[k] = run; run += c3[k]; }
-    D.off3[nc] = run;
-    for (unsigned k = 0; k < nc; k++) { D.off6[k] = run; run += c6[k]; }
-    D.off6[nc] = run;
-    for (unsigned k = 0; k < nc; k++) { D.offc[k] = run; run += cc[k]; }
-    D.offc[nc] = run;
-    D.lists.assign(run, 0);
-    std::vector<unsigned> u3(D.off3.begin(), D.off3.end() - 1), u6(D.off6.begin(), D.off6.end() - 1),
-        uc(D.offc.begin(), D.offc.end() - 1);
-    for (unsigned i = 0; i < n; i++) {
-        const unsigned e = c->perm[i];
-        if (D.confl[i]) D.lists[uc[D.color[e]]++] = i;
-        if (!D.skip[i] || c->fixed[e]) continue;
-        if (c->rot[e] != UINT32_MAX) D.lists[u6[D.color[e]]++] = i;
-        else D.lists[u3[D.color[e]]++] = i;
+    for (unsigned t = 0; t < 3; t++) {
+        uint32_t* off = summary + 4 + t * (RC_MAXC + 1);
+        for (unsigned k = 0; k < nc; k++) {
+            off[k] = run;
+            lc[3 * RC_MAXC + t * RC_MAXC + k] = run;
+            run += lc[t * RC_MAXC + k];
+        }
+        off[nc] = run;
     }
+    summary[0] = R.ctr[RC_NCOLORS];
+    summary[1] = R.ctr[R.ctr[RC_CUR]];
+    summary[2] = R.ctr[RC_NCONFL];
+    summary[3] = R.ctr[RC_ERR];
+}
+
+__global__ void k_rc_fill(RcDev R, const uint32_t* __restrict__ perm, const uint8_t* __restrict__ skip,
+                          const uint8_t* __restrict__ confl_eng, const uint8_t* __restrict__ flags, uint32_t* lc,
+                          uint32_t* lists, unsigned n) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned ce = R.color[perm[i]];
+        if (confl_eng[i]) lists[atomicAdd(lc + 3 * RC_MAXC + 2 * RC_MAXC + ce, 1u)] = i;
+        if (!skip[i] || (flags[i] & VF_FIXED)) continue;
+        lists[atomicAdd(lc + 3 * RC_MAXC + ((flags[i] & VF_ORIENTED) ? RC_MAXC : 0u) + ce, 1u)] = i;
+    }
+}
+
+RcDev rc_dev(DynHost& D) {
+    return RcDev{D.d_color, D.d_cand, D.d_last_dirty, D.d_dirty0, D.d_dirty1, D.d_ctr,
+                 D.d_touched, D.d_confl_ext, D.d_p_off, D.d_p_nbr, D.d_dnb_off, D.d_dnb};
 }
 
 // the step-start hook of every live contact of both pools: thread i < size0
@@ -462,6 +548,17 @@ int alloc_state(avbd_ctx* c, DevState<R>& s, DynHost& D, std::string& err) {
         !alloc((void**)&s.dyn_ent, sizeof(uint32_t) * D.ent_cap) || !alloc((void**)&s.dyn_skip, n) ||
         !alloc((void**)&s.conflicted, n) || !alloc((void**)&s.buffered, sizeof(V4) * n) ||
         !alloc((void**)&D.d_lists, sizeof(uint32_t) * 2 * (size_t)n))
+        return AVBD_ERR_CUDA;
+    // the recoloring's state; a dynamic entry has at most 4 other particles
+    D.dnb_cap = 4 * D.ent_cap;
+    D.marks_cap = 5 * cap;
+    if (!alloc((void**)&D.d_color, sizeof(uint32_t) * n) || !alloc((void**)&D.d_cand, sizeof(uint32_t) * n) ||
+        !alloc((void**)&D.d_last_dirty, sizeof(uint32_t) * n) || !alloc((void**)&D.d_dirty0, sizeof(uint32_t) * n) ||
+        !alloc((void**)&D.d_dirty1, sizeof(uint32_t) * n) || !alloc((void**)&D.d_touched, n) ||
+        !alloc((void**)&D.d_confl_ext, sizeof(uint32_t) * n) || !alloc((void**)&D.d_dnb_off, sizeof(uint32_t) * (n + 1)) ||
+        !alloc((void**)&D.d_dnb, sizeof(uint32_t) * D.dnb_cap) || !alloc((void**)&D.d_marks, sizeof(uint32_t) * D.marks_cap) ||
+        !alloc((void**)&D.d_slab, sizeof(uint32_t) * n) || !alloc((void**)&D.d_ctr, sizeof(uint32_t) * RC_NCTR) ||
+        !alloc((void**)&D.d_lc, sizeof(uint32_t) * 6 * RC_MAXC) || !alloc((void**)&D.d_summary, sizeof(uint32_t) * RC_SUMMARY))
         return AVBD_ERR_CUDA;
     cudaStream_t st = c->stream;
     cudaMemsetAsync(s.dyn_begin, 0, sizeof(uint32_t) * (n + 1), st);
@@ -560,18 +657,7 @@ int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vecto
     // a merge may add this stage's contacts before it frees the last stage's,
     // so each pool holds up to twice the narrow phase's capacity
     D->cap = 2 * c->lbvh.contact_capacity;
-    D->p_off = p_off;
-    D->p_nbr = p_nbr;
-    D->color = c->color;
     D->num_colors = c->num_colors;
-    D->slab_color.assign(n, 0);
-    for (unsigned k = 0; k < c->num_colors; k++)
-        for (unsigned i = c->color_begin[k]; i < c->color_begin[k + 1]; i++) D->slab_color[i] = k;
-    D->last_dirty.assign(n, DIRTY_SENTINEL);
-    D->cand.assign(n, 0);
-    D->conflicted.assign(n, 0);
-    D->skip_dev.assign(n, 0);
-    D->confl_dev.assign(n, 0);
     D->dyn_off.assign(n + 1, 0);
     D->dnb_off.assign(n + 1, 0);
     D->off3.assign(D->num_colors + 1, 0);
@@ -580,11 +666,47 @@ int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vecto
     c->dyn = D;
     const bool d64 = c->solver.precision != AVBD_PRECISION_FP32;
     int rc = d64 ? alloc_state<double>(c, c->d, *D, err) : alloc_state<float>(c, c->f, *D, err);
-    if (rc) dyn_destroy(c);
-    return rc;
+    if (rc) {
+        dyn_destroy(c);
+        return rc;
+    }
+    // the set-up coloring, the static neighbours and each engine vertex's
+    // slab color go to the device once; no particle is dirty yet
+    std::vector<uint32_t> slab(n, 0), ctr(RC_NCTR, 0);
+    for (unsigned k = 0; k < c->num_colors; k++)
+        for (unsigned i = c->color_begin[k]; i < c->color_begin[k + 1]; i++) slab[i] = k;
+    ctr[RC_NCOLORS] = c->num_colors;
+    cudaStream_t st = c->stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    };
+    auto dalloc = [&](uint32_t** q, size_t count) {
+        *q = nullptr;
+        if (cudaMalloc((void**)q, sizeof(uint32_t) * (count ? count : 1)) != cudaSuccess) return false;
+        c->allocations.push_back((void*)*q);
+        return true;
+    };
+    bool ok = cudaMallocHost((void**)&D->h_summary, sizeof(uint32_t) * RC_SUMMARY) == cudaSuccess &&
+              dalloc(&D->d_p_off, n + 1) && dalloc(&D->d_p_nbr, p_nbr.size());
+    ok = ok && up(D->d_color, c->color.data(), sizeof(uint32_t) * n) && up(D->d_slab, slab.data(), sizeof(uint32_t) * n) &&
+         up(D->d_ctr, ctr.data(), sizeof(uint32_t) * RC_NCTR) &&
+         up(D->d_p_off, p_off.data(), sizeof(uint32_t) * (n + 1)) &&
+         up(D->d_p_nbr, p_nbr.data(), sizeof(uint32_t) * p_nbr.size()) &&
+         cudaMemsetAsync(D->d_last_dirty, 0xFF, sizeof(uint32_t) * n, st) == cudaSuccess &&
+         cudaMemsetAsync(D->d_touched, 0, n, st) == cudaSuccess &&
+         cudaMemsetAsync(D->d_confl_ext, 0, sizeof(uint32_t) * n, st) == cudaSuccess &&
+         cudaMemsetAsync(D->d_dnb_off, 0, sizeof(uint32_t) * (n + 1), st) == cudaSuccess &&
+         cudaStreamSynchronize(st) == cudaSuccess;
+    if (!ok) {
+        if (err.empty()) err = "recoloring state: CUDA call failed";
+        dyn_destroy(c);
+        return AVBD_ERR_CUDA;
+    }
+    return AVBD_OK;
 }
 
 void dyn_destroy(avbd_ctx* c) {
+    if (c->dyn && c->dyn->h_summary) cudaFreeHost(c->dyn->h_summary);
     delete c->dyn;
     c->dyn = nullptr;
 }
@@ -598,8 +720,63 @@ void dyn_positional_list(const avbd_ctx* c, const uint32_t** list, unsigned* cou
 }
 
 int dyn_coloring(const avbd_ctx* c, unsigned* colors) {
-    const auto& col = c->dyn ? c->dyn->color : c->color;
-    std::copy(col.begin(), col.end(), colors);
+    if (!c->dyn) {
+        std::copy(c->color.begin(), c->color.end(), colors);
+        return AVBD_OK;
+    }
+    const size_t n = c->color.size();
+    DYN_CUDA(cudaMemcpyAsync(colors, c->dyn->d_color, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+    DYN_CUDA(cudaStreamSynchronize(c->stream));
+    return AVBD_OK;
+}
+
+// The recoloring, the conflicts and the per-color lists of one stage on the
+// device (after the merge's marks and the dynamic adjacency are uploaded),
+// then the per-color list offsets, the color count and the error flag read
+// back: the host needs them to launch the stage's sweeps.
+int dyn_recolor_device(avbd_ctx* c, const uint32_t* dyn_begin, const uint8_t* flags, uint8_t* skip,
+                       uint8_t* confl_eng, cudaStream_t st) {
+    DynHost& D = *c->dyn;
+    const unsigned n = (unsigned)c->perm.size();
+    const RcDev R = rc_dev(D);
+    const unsigned nm = (unsigned)D.marks.size();
+    if (nm > D.marks_cap) return set_error(AVBD_ERR_CAPACITY, "dirty marks exceed their capacity");
+    if (nm) DYN_CUDA(cudaMemcpyAsync(D.d_marks, D.marks.data(), sizeof(uint32_t) * nm, cudaMemcpyHostToDevice, st));
+    D.marks.clear();
+    // the last stage's conflicts are cleared (ColorList.hpp:381-389)
+    DYN_CUDA(cudaMemsetAsync(D.d_confl_ext, 0, sizeof(uint32_t) * n, st));
+    DYN_CUDA(cudaMemsetAsync(D.d_ctr + RC_NCONFL, 0, sizeof(uint32_t), st));
+    const unsigned gb = nblk(n, 256);
+    if (nm) {
+        k_rc_mark<<<nblk(nm, 256), 256, 0, st>>>(R, D.d_marks, nm);
+        count_launch(c);
+    }
+    for (unsigned it = 0; it < D.rounds; it++) {
+        k_rc_cand<<<gb, 256, 0, st>>>(R);
+        k_rc_apply<<<gb, 256, 0, st>>>(R, it + 1);
+        k_rc_flip<<<1, 1, 0, st>>>(R);
+        count_launch(c, 3);
+    }
+    k_rc_conflicts<<<gb, 256, 0, st>>>(R);
+    k_rc_settle<<<gb, 256, 0, st>>>(R, n);
+    k_rc_keep<<<gb, 256, 0, st>>>(R);
+    DYN_CUDA(cudaMemsetAsync(D.d_lc, 0, sizeof(uint32_t) * 6 * RC_MAXC, st));
+    k_rc_count<<<gb, 256, 0, st>>>(R, c->d_perm, D.d_slab, dyn_begin, flags, skip, confl_eng, D.d_lc, n);
+    k_rc_offsets<<<1, 32, 0, st>>>(R, D.d_lc, D.d_summary);
+    k_rc_fill<<<gb, 256, 0, st>>>(R, c->d_perm, skip, confl_eng, flags, D.d_lc, D.d_lists, n);
+    count_launch(c, 6);
+    DYN_CUDA(cudaGetLastError());
+    DYN_CUDA(cudaMemcpyAsync(D.h_summary, D.d_summary, sizeof(uint32_t) * RC_SUMMARY, cudaMemcpyDeviceToHost, st));
+    DYN_CUDA(cudaStreamSynchronize(st));
+    const uint32_t* h = D.h_summary;
+    if (h[3]) return set_error(AVBD_ERR_COLORS, "Ran out of colors!");
+    D.num_colors = std::min(h[0], RC_MAXC);
+    D.dirty_count = h[1];
+    D.conflicted_count = h[2];
+    const unsigned nc = D.num_colors;
+    D.off3.assign(h + 4, h + 4 + nc + 1);
+    D.off6.assign(h + 4 + (RC_MAXC + 1), h + 4 + (RC_MAXC + 1) + nc + 1);
+    D.offc.assign(h + 4 + 2 * (RC_MAXC + 1), h + 4 + 2 * (RC_MAXC + 1) + nc + 1);
     return AVBD_OK;
 }
 
@@ -654,10 +831,9 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     if (int r = handle_detections(c, D)) return r;
     const unsigned n = (unsigned)c->perm.size();
     build_dynamic_adjacency(D, n);
-    if (int r = incremental_recoloring(D)) return r;
-    build_lists(c, D);
 
-    // uploads: pool records, dynamic adjacency (engine order), flags, lists
+    // uploads: pool records, dynamic adjacency (engine order for the solve,
+    // reference order for the recoloring)
     for (int pl = 0; pl < 2; pl++)
         if (int r = upload_pool<R>(c, s.cp[pl], D.pool[pl], st)) return r;
     if (D.csr_dirty) {
@@ -677,20 +853,13 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
         if (D.dyn_begin[n])
             DYN_CUDA(cudaMemcpyAsync(s.dyn_ent, D.dyn_ent.data(), sizeof(uint32_t) * D.dyn_begin[n],
                                      cudaMemcpyHostToDevice, st));
+        if (D.dnb_off[n] > D.dnb_cap) return set_error(AVBD_ERR_CAPACITY, "dynamic neighbours exceed their capacity");
+        DYN_CUDA(cudaMemcpyAsync(D.d_dnb_off, D.dnb_off.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));
+        if (D.dnb_off[n])
+            DYN_CUDA(cudaMemcpyAsync(D.d_dnb, D.dnb.data(), sizeof(uint32_t) * D.dnb_off[n], cudaMemcpyHostToDevice, st));
         D.csr_dirty = false;
     }
-    if (D.skip != D.skip_dev) {
-        DYN_CUDA(cudaMemcpyAsync(s.dyn_skip, D.skip.data(), n, cudaMemcpyHostToDevice, st));
-        D.skip_dev = D.skip;
-    }
-    if (D.confl != D.confl_dev) {
-        DYN_CUDA(cudaMemcpyAsync(s.conflicted, D.confl.data(), n, cudaMemcpyHostToDevice, st));
-        D.confl_dev = D.confl;
-    }
-    if (!D.lists.empty())
-        DYN_CUDA(cudaMemcpyAsync(D.d_lists, D.lists.data(), sizeof(uint32_t) * D.lists.size(), cudaMemcpyHostToDevice,
-                                 st));
-    DYN_CUDA(cudaStreamSynchronize(st));
+    if (int r = dyn_recolor_device(c, s.dyn_begin, s.flags, s.dyn_skip, s.conflicted, st)) return r;
     // the contacts' step-start hook, at the positions of the step start
     const unsigned s0 = D.pool[0].size, s1 = D.pool[1].size;
     if (s0 + s1) {
@@ -745,8 +914,8 @@ int avbd_dynamic_info(avbd_ctx* c, unsigned out[8]) {
     out[0] = D.pool[0].count;
     out[1] = D.pool[0].size;
     out[2] = D.num_colors;
-    out[3] = (unsigned)D.touched_conflicted.size();
-    out[4] = (unsigned)D.dirty.size();
+    out[3] = D.conflicted_count;
+    out[4] = D.dirty_count;
     out[5] = (unsigned)D.dyn_ent_ext.size();
     out[6] = D.pool[1].count;
     out[7] = D.pool[1].size;
