@@ -304,18 +304,21 @@ struct RcDev {
     const uint32_t *p_off, *p_nbr, *dnb_off, *dnb;
 };
 
+// the lane's share of p's neighbours: static ones, then dynamic ones,
+// every 32nd from `lane`
 template <typename F>
-AVBD_D void rc_neighbors(const RcDev& R, unsigned p, F&& f) {
-    for (unsigned k = R.p_off[p]; k < R.p_off[p + 1]; k++) f(R.p_nbr[k]);
-    for (unsigned k = R.dnb_off[p]; k < R.dnb_off[p + 1]; k++) f(R.dnb[k]);
+AVBD_D void rc_neighbors_lane(const RcDev& R, unsigned p, unsigned lane, F&& f) {
+    const unsigned s0 = R.p_off[p], ds = R.p_off[p + 1] - s0;
+    const unsigned d0 = R.dnb_off[p], dd = R.dnb_off[p + 1] - d0;
+    for (unsigned k = lane; k < ds + dd; k += 32) f(k < ds ? R.p_nbr[s0 + k] : R.dnb[d0 + k - ds]);
 }
 
 // the conflicts of the last stage are cleared, then this stage's new
 // contacts' particles join the dirty set (those already in it keep label 0)
-__global__ void k_rc_mark(RcDev R, const uint32_t* __restrict__ marks, unsigned nmarks) {
+AVBD_D void rc_mark(const RcDev& R, const uint32_t* __restrict__ marks, unsigned nmarks, unsigned t0, unsigned dt) {
     const unsigned cur = R.ctr[RC_CUR];
     uint32_t* list = cur ? R.dirty1 : R.dirty0;
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < nmarks; j += gridDim.x * blockDim.x) {
+    for (unsigned j = t0; j < nmarks; j += dt) {
         const unsigned p = marks[j];
         if (atomicExch(R.last_dirty + p, 0u) != 0u) {
             R.touched[p] = 1;
@@ -325,15 +328,16 @@ __global__ void k_rc_mark(RcDev R, const uint32_t* __restrict__ marks, unsigned 
 }
 
 // half-round 1: a dirty particle sharing its color with a lower-numbered
-// neighbour takes the smallest color no neighbour holds
-__global__ void k_rc_cand(RcDev R) {
+// neighbour takes the smallest color no neighbour holds (one warp per
+// particle, the neighbours' color bits or-reduced over the lanes)
+AVBD_D void rc_cand(const RcDev& R, unsigned warp, unsigned nwarps, unsigned lane) {
     const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+    for (unsigned j = warp; j < cnt; j += nwarps) {  // one warp per dirty particle
         const unsigned p = list[j], cp = R.color[p];
         uint32_t bits[RC_MAXC / 32] = {0, 0, 0, 0, 0, 0, 0, 0};
         bool must = false, over = false;
-        rc_neighbors(R, p, [&](unsigned q) {
+        rc_neighbors_lane(R, p, lane, [&](unsigned q) {
             const unsigned cq = R.color[q];
             if (cq >= RC_MAXC) {
                 over = true;
@@ -342,6 +346,11 @@ __global__ void k_rc_cand(RcDev R) {
             bits[cq >> 5] |= 1u << (cq & 31u);
             if (cq == cp && q < p) must = true;
         });
+#pragma unroll
+        for (unsigned w = 0; w < RC_MAXC / 32; w++) bits[w] = __reduce_or_sync(0xffffffffu, bits[w]);
+        must = __any_sync(0xffffffffu, must);
+        over = __any_sync(0xffffffffu, over);
+        if (lane != 0) continue;
         unsigned cand = cp;
         if (over) {
             atomicExch(R.ctr + RC_ERR, 1u);
@@ -362,15 +371,16 @@ __global__ void k_rc_cand(RcDev R) {
 
 // half-round 2: candidates applied; every neighbour of a changed particle
 // joins the next round's dirty set, once per round (label = round + 1)
-__global__ void k_rc_apply(RcDev R, unsigned label) {
+AVBD_D void rc_apply(const RcDev& R, unsigned label, unsigned warp, unsigned nwarps, unsigned lane) {
     const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
     uint32_t* next = cur ? R.dirty0 : R.dirty1;
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
-        const unsigned p = list[j];
-        if (R.cand[p] == R.color[p]) continue;
-        R.color[p] = R.cand[p];
-        rc_neighbors(R, p, [&](unsigned q) {
+    for (unsigned j = warp; j < cnt; j += nwarps) {
+        const unsigned p = list[j], cand = R.cand[p];
+        if (cand == R.color[p]) continue;  // the same answer on every lane of the warp
+        __syncwarp();                       // every lane has read the old color
+        if (lane == 0) R.color[p] = cand;
+        rc_neighbors_lane(R, p, lane, [&](unsigned q) {
             if (atomicExch(R.last_dirty + q, label) != label) {
                 R.touched[q] = 1;
                 next[atomicAdd(R.ctr + (cur ^ 1u), 1u)] = q;
@@ -380,7 +390,7 @@ __global__ void k_rc_apply(RcDev R, unsigned label) {
 }
 
 // the next round's list becomes current, the consumed one is emptied
-__global__ void k_rc_flip(RcDev R) {
+AVBD_D void rc_flip(const RcDev& R) {
     const unsigned cur = R.ctr[RC_CUR];
     R.ctr[cur] = 0;
     R.ctr[RC_CUR] = cur ^ 1u;
@@ -388,12 +398,12 @@ __global__ void k_rc_flip(RcDev R) {
 
 // finalizeConflicts: particles still dirty after the last round and their
 // same-colored neighbours are conflicted
-__global__ void k_rc_conflicts(RcDev R) {
+AVBD_D void rc_conflicts(const RcDev& R, unsigned warp, unsigned nwarps, unsigned lane) {
     const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x) {
+    for (unsigned j = warp; j < cnt; j += nwarps) {
         const unsigned p = list[j], cp = R.color[p];
-        rc_neighbors(R, p, [&](unsigned q) {
+        rc_neighbors_lane(R, p, lane, [&](unsigned q) {
             if (R.color[q] != cp) return;
             if (atomicExch(R.confl + p, 1u) == 0u) atomicAdd(R.ctr + RC_NCONFL, 1u);
             if (atomicExch(R.confl + q, 1u) == 0u) atomicAdd(R.ctr + RC_NCONFL, 1u);
@@ -402,18 +412,18 @@ __global__ void k_rc_conflicts(RcDev R) {
 }
 
 // labels written this stage go back to the sentinel ...
-__global__ void k_rc_settle(RcDev R, unsigned n) {
-    for (unsigned p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+AVBD_D void rc_settle(const RcDev& R, unsigned n, unsigned t0, unsigned dt) {
+    for (unsigned p = t0; p < n; p += dt)
         if (R.touched[p]) {
             R.touched[p] = 0;
             R.last_dirty[p] = DIRTY_SENTINEL;
         }
 }
 // ... and the particles still dirty carry label 0 into the next stage
-__global__ void k_rc_keep(RcDev R) {
+AVBD_D void rc_keep(const RcDev& R, unsigned t0, unsigned dt) {
     const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
-    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x)
+    for (unsigned j = t0; j < cnt; j += dt)
         R.last_dirty[list[j]] = 0;
 }
 
@@ -422,10 +432,20 @@ __global__ void k_rc_keep(RcDev R) {
 // solved from its color's list (positional or oriented; fixed vertices are
 // skipped and not listed); conflicted vertices are listed for the commit.
 // lc: counts [3][256] then cursors [3][256].
-__global__ void k_rc_count(RcDev R, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ slab,
-                           const uint32_t* __restrict__ dyn_begin, const uint8_t* __restrict__ flags,
-                           uint8_t* skip, uint8_t* confl_eng, uint32_t* lc, unsigned n) {
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+struct RcLists {
+    const uint32_t *perm, *slab, *dyn_begin;
+    const uint8_t* flags;
+    uint8_t *skip, *confl_eng;
+    uint32_t *lc, *lists, *summary;
+    unsigned n;
+};
+
+AVBD_D void rc_count(const RcDev& R, const RcLists& L, unsigned t0, unsigned dt) {
+    const uint32_t *perm = L.perm, *slab = L.slab, *dyn_begin = L.dyn_begin;
+    const uint8_t* flags = L.flags;
+    uint8_t *skip = L.skip, *confl_eng = L.confl_eng;
+    uint32_t* lc = L.lc;
+    for (unsigned i = t0; i < L.n; i += dt) {
         const unsigned e = perm[i], ce = R.color[e];
         const uint8_t cf = R.confl[e] ? 1 : 0;
         confl_eng[i] = cf;
@@ -439,8 +459,8 @@ __global__ void k_rc_count(RcDev R, const uint32_t* __restrict__ perm, const uin
 
 // offsets: all positional lists, then all oriented, then all conflicted;
 // the summary the host reads back
-__global__ void k_rc_offsets(RcDev R, uint32_t* lc, uint32_t* summary) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+AVBD_D void rc_offsets(const RcDev& R, const RcLists& L) {
+    uint32_t *lc = L.lc, *summary = L.summary;
     const unsigned nc = min(R.ctr[RC_NCOLORS], RC_MAXC);
     unsigned run = 0;
     for (unsigned t = 0; t < 3; t++) {
@@ -458,15 +478,59 @@ __global__ void k_rc_offsets(RcDev R, uint32_t* lc, uint32_t* summary) {
     summary[3] = R.ctr[RC_ERR];
 }
 
-__global__ void k_rc_fill(RcDev R, const uint32_t* __restrict__ perm, const uint8_t* __restrict__ skip,
-                          const uint8_t* __restrict__ confl_eng, const uint8_t* __restrict__ flags, uint32_t* lc,
-                          uint32_t* lists, unsigned n) {
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+AVBD_D void rc_fill(const RcDev& R, const RcLists& L, unsigned t0, unsigned dt) {
+    const uint32_t* perm = L.perm;
+    const uint8_t *skip = L.skip, *confl_eng = L.confl_eng, *flags = L.flags;
+    uint32_t *lc = L.lc, *lists = L.lists;
+    for (unsigned i = t0; i < L.n; i += dt) {
         const unsigned ce = R.color[perm[i]];
         if (confl_eng[i]) lists[atomicAdd(lc + 3 * RC_MAXC + 2 * RC_MAXC + ce, 1u)] = i;
         if (!skip[i] || (flags[i] & VF_FIXED)) continue;
         lists[atomicAdd(lc + 3 * RC_MAXC + ((flags[i] & VF_ORIENTED) ? RC_MAXC : 0u) + ce, 1u)] = i;
     }
+}
+
+// the passes over every vertex as grid-wide kernels ...
+#define RC_GRID blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x
+__global__ void k_rc_settle(RcDev R, unsigned n) { rc_settle(R, n, RC_GRID); }
+__global__ void k_rc_offsets(RcDev R, RcLists L) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) rc_offsets(R, L);
+}
+__global__ void k_rc_fill(RcDev R, RcLists L) { rc_fill(R, L, RC_GRID); }
+#undef RC_GRID
+
+// ... and the phases over the dirty set (small: the particles of new
+// contacts and their neighbourhoods) in one block: the conflicts and list
+// counts cleared, the marks, every round, the conflicts, separated by block
+// barriers (global writes of the block's own threads are visible after
+// them); one launch instead of 3 per round
+__global__ void __launch_bounds__(1024) k_rc_rounds(RcDev R, uint32_t* lc, unsigned n,
+                                                    const uint32_t* __restrict__ marks, unsigned nmarks,
+                                                    unsigned rounds) {
+    const unsigned t0 = threadIdx.x, dt = blockDim.x;
+    for (unsigned p = t0; p < n; p += dt) R.confl[p] = 0;  // the last stage's conflicts
+    for (unsigned k = t0; k < 6 * RC_MAXC; k += dt) lc[k] = 0;
+    if (t0 == 0) R.ctr[RC_NCONFL] = 0;
+    __syncthreads();
+    rc_mark(R, marks, nmarks, t0, dt);
+    __syncthreads();
+    const unsigned warp = t0 >> 5, nwarps = dt >> 5, lane = t0 & 31u;
+    for (unsigned it = 0; it < rounds; it++) {
+        rc_cand(R, warp, nwarps, lane);
+        __syncthreads();
+        rc_apply(R, it + 1, warp, nwarps, lane);
+        __syncthreads();
+        if (t0 == 0) rc_flip(R);
+        __syncthreads();
+    }
+    rc_conflicts(R, warp, nwarps, lane);
+}
+
+// the list counts, with the carried-over labels of the still-dirty particles
+// set by block 0 (after the settle kernel, independent of the counts)
+__global__ void k_rc_count_keep(RcDev R, RcLists L) {
+    if (blockIdx.x == 0) rc_keep(R, threadIdx.x, blockDim.x);
+    rc_count(R, L, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 RcDev rc_dev(DynHost& D) {
@@ -743,28 +807,14 @@ int dyn_recolor_device(avbd_ctx* c, const uint32_t* dyn_begin, const uint8_t* fl
     if (nm > D.marks_cap) return set_error(AVBD_ERR_CAPACITY, "dirty marks exceed their capacity");
     if (nm) DYN_CUDA(cudaMemcpyAsync(D.d_marks, D.marks.data(), sizeof(uint32_t) * nm, cudaMemcpyHostToDevice, st));
     D.marks.clear();
-    // the last stage's conflicts are cleared (ColorList.hpp:381-389)
-    DYN_CUDA(cudaMemsetAsync(D.d_confl_ext, 0, sizeof(uint32_t) * n, st));
-    DYN_CUDA(cudaMemsetAsync(D.d_ctr + RC_NCONFL, 0, sizeof(uint32_t), st));
+    const RcLists L{c->d_perm, D.d_slab, dyn_begin, flags, skip, confl_eng, D.d_lc, D.d_lists, D.d_summary, n};
     const unsigned gb = nblk(n, 256);
-    if (nm) {
-        k_rc_mark<<<nblk(nm, 256), 256, 0, st>>>(R, D.d_marks, nm);
-        count_launch(c);
-    }
-    for (unsigned it = 0; it < D.rounds; it++) {
-        k_rc_cand<<<gb, 256, 0, st>>>(R);
-        k_rc_apply<<<gb, 256, 0, st>>>(R, it + 1);
-        k_rc_flip<<<1, 1, 0, st>>>(R);
-        count_launch(c, 3);
-    }
-    k_rc_conflicts<<<gb, 256, 0, st>>>(R);
+    k_rc_rounds<<<1, 1024, 0, st>>>(R, D.d_lc, n, D.d_marks, nm, D.rounds);
     k_rc_settle<<<gb, 256, 0, st>>>(R, n);
-    k_rc_keep<<<gb, 256, 0, st>>>(R);
-    DYN_CUDA(cudaMemsetAsync(D.d_lc, 0, sizeof(uint32_t) * 6 * RC_MAXC, st));
-    k_rc_count<<<gb, 256, 0, st>>>(R, c->d_perm, D.d_slab, dyn_begin, flags, skip, confl_eng, D.d_lc, n);
-    k_rc_offsets<<<1, 32, 0, st>>>(R, D.d_lc, D.d_summary);
-    k_rc_fill<<<gb, 256, 0, st>>>(R, c->d_perm, skip, confl_eng, flags, D.d_lc, D.d_lists, n);
-    count_launch(c, 6);
+    k_rc_count_keep<<<gb, 256, 0, st>>>(R, L);
+    k_rc_offsets<<<1, 32, 0, st>>>(R, L);
+    k_rc_fill<<<gb, 256, 0, st>>>(R, L);
+    count_launch(c, 5);
     DYN_CUDA(cudaGetLastError());
     DYN_CUDA(cudaMemcpyAsync(D.h_summary, D.d_summary, sizeof(uint32_t) * RC_SUMMARY, cudaMemcpyDeviceToHost, st));
     DYN_CUDA(cudaStreamSynchronize(st));
