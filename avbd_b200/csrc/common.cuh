@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "avbd.h"
+
 #define AVBD_HD __host__ __device__ __forceinline__
 #define AVBD_D __device__ __forceinline__
 
@@ -127,4 +129,40 @@ AVBD_D void lu_solve_d(double (&A)[N][N], double (&b)[N], double (&x)[N]) {
         for (int j = i + 1; j < N; j++) s -= A[i][j] * x[j];
         x[i] = s / A[i][i];
     }
+
+}
+
+// Barrier over every block of a cooperative launch.  sync[0] counts the
+// arrivals, sync[1] is the generation: thread 0 of the last block to arrive
+// resets the count and advances the generation, the others poll it at most
+// `limit` times and then set AVBD_ERR_BARRIER_TIMEOUT in *err.  A block
+// returns false when that error (or any other in *err) is set, so that every
+// block leaves the kernel; the polls are bounded, so none waits forever.
+AVBD_D bool grid_barrier_bounded(unsigned* sync, int* err, unsigned limit) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = *(volatile unsigned*)(sync + 1);
+        int good = 1;
+        __threadfence();
+        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
+            atomicExch(sync, 0u);
+            __threadfence();
+            atomicAdd(sync + 1, 1u);
+        } else {
+            unsigned polls = 0;
+            while (*(volatile unsigned*)(sync + 1) == gen) {
+                if (polls++ >= limit || *(volatile int*)err != 0) {
+                    good = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (!good) atomicCAS(err, 0, (int)AVBD_ERR_BARRIER_TIMEOUT);
+        ok = good && *(volatile int*)err == 0;
+    }
+    __syncthreads();
+    return ok != 0;
 }

@@ -84,6 +84,7 @@ struct DynHost {
     uint32_t* d_summary = nullptr;               // RC_SUMMARY words for the host
     uint32_t* h_summary = nullptr;               // pinned copy
     unsigned dnb_cap = 0, marks_cap = 0;
+    unsigned coop_blocks = 0;                    // grid of the cooperative rounds kernel (0: one block)
     // ---- per-color lists (engine vertex order) on the device
     std::vector<unsigned> off3, off6, offc;      // per color: recolored 3-DOF, 6-DOF, conflicted
     std::vector<uint32_t> dyn_begin, dyn_ent;
@@ -291,7 +292,12 @@ void build_dynamic_adjacency(DynHost& D, unsigned n) {
 // one kernel per half-round gives the reference's colors exactly; the dirty
 // set, its last-dirty labels and the conflicts are sets, so the order in
 // which threads append to them changes nothing.
-enum : unsigned { RC_CNT0 = 0, RC_CNT1 = 1, RC_CUR = 2, RC_NCONFL = 3, RC_NCOLORS = 4, RC_ERR = 5, RC_NCTR = 8 };
+enum : unsigned {
+    RC_CNT0 = 0, RC_CNT1 = 1, RC_CUR = 2, RC_NCONFL = 3, RC_NCOLORS = 4, RC_ERR = 5,
+    RC_SYNC = 6,   // two words: the cooperative kernel's grid barrier
+    RC_BERR = 8,   // its status (AVBD_ERR_BARRIER_TIMEOUT)
+    RC_NCTR = 12
+};
 constexpr unsigned RC_MAXC = 256;  // colors (ColorList's bitset)
 // summary for the host: [num_colors, dirty count, conflicted count, error,
 // off3[0..256], off6[0..256], offc[0..256]]
@@ -330,8 +336,8 @@ AVBD_D void rc_mark(const RcDev& R, const uint32_t* __restrict__ marks, unsigned
 // half-round 1: a dirty particle sharing its color with a lower-numbered
 // neighbour takes the smallest color no neighbour holds (one warp per
 // particle, the neighbours' color bits or-reduced over the lanes)
-AVBD_D void rc_cand(const RcDev& R, unsigned warp, unsigned nwarps, unsigned lane) {
-    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+AVBD_D void rc_cand(const RcDev& R, unsigned cur, unsigned warp, unsigned nwarps, unsigned lane) {
+    const unsigned cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
     for (unsigned j = warp; j < cnt; j += nwarps) {  // one warp per dirty particle
         const unsigned p = list[j], cp = R.color[p];
@@ -371,8 +377,8 @@ AVBD_D void rc_cand(const RcDev& R, unsigned warp, unsigned nwarps, unsigned lan
 
 // half-round 2: candidates applied; every neighbour of a changed particle
 // joins the next round's dirty set, once per round (label = round + 1)
-AVBD_D void rc_apply(const RcDev& R, unsigned label, unsigned warp, unsigned nwarps, unsigned lane) {
-    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+AVBD_D void rc_apply(const RcDev& R, unsigned cur, unsigned label, unsigned warp, unsigned nwarps, unsigned lane) {
+    const unsigned cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
     uint32_t* next = cur ? R.dirty0 : R.dirty1;
     for (unsigned j = warp; j < cnt; j += nwarps) {
@@ -389,17 +395,10 @@ AVBD_D void rc_apply(const RcDev& R, unsigned label, unsigned warp, unsigned nwa
     }
 }
 
-// the next round's list becomes current, the consumed one is emptied
-AVBD_D void rc_flip(const RcDev& R) {
-    const unsigned cur = R.ctr[RC_CUR];
-    R.ctr[cur] = 0;
-    R.ctr[RC_CUR] = cur ^ 1u;
-}
-
 // finalizeConflicts: particles still dirty after the last round and their
 // same-colored neighbours are conflicted
-AVBD_D void rc_conflicts(const RcDev& R, unsigned warp, unsigned nwarps, unsigned lane) {
-    const unsigned cur = R.ctr[RC_CUR], cnt = R.ctr[cur];
+AVBD_D void rc_conflicts(const RcDev& R, unsigned cur, unsigned warp, unsigned nwarps, unsigned lane) {
+    const unsigned cnt = R.ctr[cur];
     const uint32_t* list = cur ? R.dirty1 : R.dirty0;
     for (unsigned j = warp; j < cnt; j += nwarps) {
         const unsigned p = list[j], cp = R.color[p];
@@ -475,7 +474,7 @@ AVBD_D void rc_offsets(const RcDev& R, const RcLists& L) {
     summary[0] = R.ctr[RC_NCOLORS];
     summary[1] = R.ctr[R.ctr[RC_CUR]];
     summary[2] = R.ctr[RC_NCONFL];
-    summary[3] = R.ctr[RC_ERR];
+    summary[3] = R.ctr[RC_ERR] ? 1u : (R.ctr[RC_BERR] ? 2u : 0u);
 }
 
 AVBD_D void rc_fill(const RcDev& R, const RcLists& L, unsigned t0, unsigned dt) {
@@ -499,31 +498,49 @@ __global__ void k_rc_offsets(RcDev R, RcLists L) {
 __global__ void k_rc_fill(RcDev R, RcLists L) { rc_fill(R, L, RC_GRID); }
 #undef RC_GRID
 
-// ... and the phases over the dirty set (small: the particles of new
-// contacts and their neighbourhoods) in one block: the conflicts and list
-// counts cleared, the marks, every round, the conflicts, separated by block
-// barriers (global writes of the block's own threads are visible after
-// them); one launch instead of 3 per round
-__global__ void __launch_bounds__(1024) k_rc_rounds(RcDev R, uint32_t* lc, unsigned n,
-                                                    const uint32_t* __restrict__ marks, unsigned nmarks,
-                                                    unsigned rounds) {
-    const unsigned t0 = threadIdx.x, dt = blockDim.x;
+// ... and the phases over the dirty set (the particles of new contacts and
+// their neighbourhoods): the conflicts and list counts cleared, the marks,
+// every round (candidates, then their application), the conflicts.  Round r
+// reads the dirty list cur ^ (r & 1) and appends to the other, whose count
+// its candidate phase has zeroed (nobody reads it then).  Either as one
+// cooperative launch over the SMs, the phases separated by bounded grid
+// barriers, or, where the device cannot launch cooperatively, in one block,
+// separated by block barriers.
+__device__ uint32_t g_rc_wait_polls = AVBD_DEFAULT_WAIT_POLLS;
+
+template <bool COOP>
+__global__ void __launch_bounds__(COOP ? 256 : 1024) k_rc_rounds(RcDev R, uint32_t* lc, unsigned n,
+                                                                  const uint32_t* __restrict__ marks,
+                                                                  unsigned nmarks, unsigned rounds) {
+    const unsigned t0 = COOP ? blockIdx.x * blockDim.x + threadIdx.x : threadIdx.x;
+    const unsigned dt = COOP ? gridDim.x * blockDim.x : blockDim.x;
+    const unsigned warp = t0 >> 5, nwarps = dt >> 5, lane = threadIdx.x & 31u;
+    const unsigned limit = *(volatile uint32_t*)&g_rc_wait_polls;
+    unsigned* sync = R.ctr + RC_SYNC;
+    int* berr = reinterpret_cast<int*>(R.ctr + RC_BERR);
+    auto barrier = [&]() -> bool {
+        if constexpr (COOP) return grid_barrier_bounded(sync, berr, limit);
+        __syncthreads();
+        return true;
+    };
+    const unsigned cur0 = R.ctr[RC_CUR];
     for (unsigned p = t0; p < n; p += dt) R.confl[p] = 0;  // the last stage's conflicts
     for (unsigned k = t0; k < 6 * RC_MAXC; k += dt) lc[k] = 0;
     if (t0 == 0) R.ctr[RC_NCONFL] = 0;
-    __syncthreads();
+    if (!barrier()) return;
     rc_mark(R, marks, nmarks, t0, dt);
-    __syncthreads();
-    const unsigned warp = t0 >> 5, nwarps = dt >> 5, lane = t0 & 31u;
+    if (!barrier()) return;
     for (unsigned it = 0; it < rounds; it++) {
-        rc_cand(R, warp, nwarps, lane);
-        __syncthreads();
-        rc_apply(R, it + 1, warp, nwarps, lane);
-        __syncthreads();
-        if (t0 == 0) rc_flip(R);
-        __syncthreads();
+        const unsigned cur = cur0 ^ (it & 1u);
+        if (t0 == 0) R.ctr[cur ^ 1u] = 0;
+        rc_cand(R, cur, warp, nwarps, lane);
+        if (!barrier()) return;
+        rc_apply(R, cur, it + 1, warp, nwarps, lane);
+        if (!barrier()) return;
     }
-    rc_conflicts(R, warp, nwarps, lane);
+    const unsigned cur = cur0 ^ (rounds & 1u);
+    if (t0 == 0) R.ctr[RC_CUR] = cur;
+    rc_conflicts(R, cur, warp, nwarps, lane);
 }
 
 // the list counts, with the carried-over labels of the still-dirty particles
@@ -740,6 +757,11 @@ int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vecto
     for (unsigned k = 0; k < c->num_colors; k++)
         for (unsigned i = c->color_begin[k]; i < c->color_begin[k + 1]; i++) slab[i] = k;
     ctr[RC_NCOLORS] = c->num_colors;
+    int coop = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device) == cudaSuccess && coop &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rc_rounds<true>, 256, 0) == cudaSuccess && per_sm > 0)
+        D->coop_blocks = c->num_sms;  // one block per SM: always co-resident
+    cudaGetLastError();
     cudaStream_t st = c->stream;
     auto up = [&](void* dst, const void* src, size_t bytes) {
         return bytes == 0 || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -783,6 +805,11 @@ void dyn_positional_list(const avbd_ctx* c, const uint32_t** list, unsigned* cou
     *count = D.off3.back() - D.off3.front();
 }
 
+int contacts_set_wait_limit(unsigned polls) {
+    cudaError_t e = cudaMemcpyToSymbol(g_rc_wait_polls, &polls, sizeof(polls));
+    return e == cudaSuccess ? AVBD_OK : set_error(AVBD_ERR_CUDA, cudaGetErrorString(e));
+}
+
 int dyn_coloring(const avbd_ctx* c, unsigned* colors) {
     if (!c->dyn) {
         std::copy(c->color.begin(), c->color.end(), colors);
@@ -809,7 +836,21 @@ int dyn_recolor_device(avbd_ctx* c, const uint32_t* dyn_begin, const uint8_t* fl
     D.marks.clear();
     const RcLists L{c->d_perm, D.d_slab, dyn_begin, flags, skip, confl_eng, D.d_lc, D.d_lists, D.d_summary, n};
     const unsigned gb = nblk(n, 256);
-    k_rc_rounds<<<1, 1024, 0, st>>>(R, D.d_lc, n, D.d_marks, nm, D.rounds);
+    if (D.coop_blocks) {
+        DYN_CUDA(cudaMemsetAsync(D.d_ctr + RC_SYNC, 0, sizeof(uint32_t) * 3, st));  // barrier and its status
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(D.coop_blocks);
+        cfg.blockDim = dim3(256);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        DYN_CUDA(cudaLaunchKernelEx(&cfg, k_rc_rounds<true>, R, D.d_lc, n, (const uint32_t*)D.d_marks, nm, D.rounds));
+    } else {
+        k_rc_rounds<false><<<1, 1024, 0, st>>>(R, D.d_lc, n, D.d_marks, nm, D.rounds);
+    }
     k_rc_settle<<<gb, 256, 0, st>>>(R, n);
     k_rc_count_keep<<<gb, 256, 0, st>>>(R, L);
     k_rc_offsets<<<1, 32, 0, st>>>(R, L);
@@ -819,6 +860,8 @@ int dyn_recolor_device(avbd_ctx* c, const uint32_t* dyn_begin, const uint8_t* fl
     DYN_CUDA(cudaMemcpyAsync(D.h_summary, D.d_summary, sizeof(uint32_t) * RC_SUMMARY, cudaMemcpyDeviceToHost, st));
     DYN_CUDA(cudaStreamSynchronize(st));
     const uint32_t* h = D.h_summary;
+    if (h[3] == 2)
+        return set_error(AVBD_ERR_BARRIER_TIMEOUT, "a grid-barrier wait of the recoloring gave up");
     if (h[3]) return set_error(AVBD_ERR_COLORS, "Ran out of colors!");
     D.num_colors = std::min(h[0], RC_MAXC);
     D.dirty_count = h[1];

@@ -385,6 +385,8 @@ template <typename R>
 bool launch_sweep_persistent(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st, const SceneTol& T);
 // poll limit of the persistent sweep's grid barriers (avbd_debug_set_wait_limit)
 int solve_set_wait_limit(unsigned polls);
+// poll limit of the recoloring's grid barriers (avbd_debug_set_wait_limit)
+int contacts_set_wait_limit(unsigned polls);
 template <typename R>
 void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it, cudaStream_t st,
                            const SceneTol& T = SceneTol());

@@ -692,6 +692,7 @@ int avbd_debug_set_wait_limit(int device, unsigned polls) {
         return set_error(AVBD_ERR_NO_DEVICE, "cudaSetDevice failed");
     cudaError_t e = cudaMemcpyToSymbol(g_wait_polls, &polls, sizeof(polls));
     int rc = e == cudaSuccess ? solve_set_wait_limit(polls) : AVBD_OK;
+    if (e == cudaSuccess && rc == AVBD_OK) rc = contacts_set_wait_limit(polls);
     if (e == cudaSuccess && rc == AVBD_OK) e = cudaDeviceSynchronize();
     cudaSetDevice(prev);
     if (rc != AVBD_OK) return rc;

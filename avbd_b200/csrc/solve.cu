@@ -583,40 +583,8 @@ __global__ void __launch_bounds__(256, SolveMinBlocks<P, RS>::value) k_solve_tet
 // up (avbd_debug_set_wait_limit lowers it so that tests can make it run out).
 __device__ uint32_t g_sweep_wait_polls = AVBD_DEFAULT_WAIT_POLLS;
 
-// Barrier over every block of a cooperative launch.  sync[0] counts the
-// arrivals, sync[1] is the generation: thread 0 of the last block to arrive
-// resets the count and advances the generation, the others poll it at most
-// g_sweep_wait_polls times and then set AVBD_ERR_BARRIER_TIMEOUT.  A block
-// returns false when that error (or any other device error) is set, so that
-// every block leaves the kernel; the polls are bounded, so none waits forever.
 AVBD_D bool grid_barrier(unsigned* sync, int* err) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned limit = *(volatile uint32_t*)&g_sweep_wait_polls;
-        const unsigned gen = *(volatile unsigned*)(sync + 1);
-        int good = 1;
-        __threadfence();
-        if (atomicAdd(sync, 1u) == gridDim.x - 1) {
-            atomicExch(sync, 0u);
-            __threadfence();
-            atomicAdd(sync + 1, 1u);
-        } else {
-            unsigned polls = 0;
-            while (*(volatile unsigned*)(sync + 1) == gen) {
-                if (polls++ >= limit || *(volatile int*)err != 0) {
-                    good = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        if (!good) atomicCAS(err, 0, (int)AVBD_ERR_BARRIER_TIMEOUT);
-        ok = good && *(volatile int*)err == 0;
-    }
-    __syncthreads();
-    return ok != 0;
+    return grid_barrier_bounded(sync, err, *(volatile uint32_t*)&g_sweep_wait_polls);
 }
 
 // The whole sweep of a run-to-tolerance iteration in one cooperative launch:

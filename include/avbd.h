@@ -435,12 +435,13 @@ AVBD_API int avbd_mlp_destroy(avbd_mlp* m);
  * waits of the persistent sweep (unless AVBD_PERSISTENT=0 is in the
  * environment when a context is created, each run-to-tolerance sweep of a
  * tetrahedral context runs as one cooperative launch whose blocks meet at a
- * grid barrier between colors).  A wait that gives up
+ * grid barrier between colors), and of the dynamic contacts' recoloring
+ * (its rounds run as one cooperative launch per step).  A wait that gives up
  * sets AVBD_ERR_BARRIER_TIMEOUT, which the launching call (avbd_step for the
- * sweep) returns; every result of that launch is then invalid.  The MLP
- * kernels still wait, bounded, for the MMAs they issued before they free
- * their tensor memory, and every block of the sweep leaves the kernel, so the
- * context stays usable.  Tests lower the limit to make the wait run out
+ * sweep and the recoloring) returns; every result of that launch is then
+ * invalid.  The MLP kernels still wait, bounded, for the MMAs they issued
+ * before they free their tensor memory, and every block of the sweep or the
+ * recoloring leaves the kernel, so the context stays usable.  Tests lower the limit to make the wait run out
  * without any fault. */
 #define AVBD_DEFAULT_WAIT_POLLS (1u << 22)
 AVBD_API int avbd_debug_set_wait_limit(int device, unsigned polls);

@@ -186,3 +186,31 @@ def test_recorded_iteration_matches_launch_by_launch(monkeypatch, precision):
     assert a.dynamic_info()["rod_live"] > 0
     a.close()
     b.close()
+
+
+def test_recoloring_barrier_timeout_is_reported():
+    """The recoloring's rounds run as one cooperative launch whose phases
+    meet at bounded grid barriers.  With a wait limit of 0 every block but
+    the last to arrive gives up: the step returns AVBD_ERR_BARRIER_TIMEOUT
+    before any list it would have built is used, and with the limit restored
+    the context steps again."""
+    from avbd_b200 import _lib
+    from avbd_b200._lib import AvbdError
+    sc = scenes.rods_on_cube()
+    e = Context()
+    sc.load(e, precision="fp32")
+    e.finalize()
+    e.step(2)
+    L = _lib.load()
+    try:
+        assert L.avbd_debug_set_wait_limit(0, 0) == 0
+        with pytest.raises(AvbdError) as ex:
+            e.step(1)
+            e.synchronize()
+        assert ex.value.code == 6  # AVBD_ERR_BARRIER_TIMEOUT
+    finally:
+        assert L.avbd_debug_set_wait_limit(0, _lib.DEFAULT_WAIT_POLLS) == 0
+    e.step(3)
+    e.synchronize()
+    assert np.isfinite(e.positions()).all()
+    e.close()
