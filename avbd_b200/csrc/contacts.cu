@@ -64,9 +64,9 @@ struct DynHost {
         unsigned e_idx;
     };
     std::vector<Det> cur, prev;
-    // ---- dynamic adjacency (reference particle ids, built on the host)
-    std::vector<unsigned> dyn_off, dnb_off, dnb; // dynamic entries per particle, dynamic neighbours
-    std::vector<uint32_t> dyn_ent_ext;           // slot << 4 | pool << 3 | local
+    // ---- dynamic adjacency (built on the device when contacts come or go)
+    unsigned num_entries = 0;                    // dynamic entries (slot << 4 | pool << 3 | local)
+    uint32_t *d_cnt_eng = nullptr, *d_cnt_ext = nullptr;  // per-vertex counts, then fill cursors
     std::vector<uint32_t> marks;                 // particles of this stage's new contacts (to mark dirty)
     unsigned rounds = 6;  // ColorList::incrementalRecoloring MAX_COLOR_ITERS
     // ---- coloring on the device (reference particle ids): colors, the
@@ -87,7 +87,6 @@ struct DynHost {
     unsigned coop_blocks = 0;                    // grid of the cooperative rounds kernel (0: one block)
     // ---- per-color lists (engine vertex order) on the device
     std::vector<unsigned> off3, off6, offc;      // per color: recolored 3-DOF, 6-DOF, conflicted
-    std::vector<uint32_t> dyn_begin, dyn_ent;
     uint32_t* d_lists = nullptr;
     unsigned ent_cap = 0;
     bool csr_dirty = true;
@@ -246,44 +245,6 @@ int handle_detections(avbd_ctx* c, DynHost& D) {
     return AVBD_OK;
 }
 
-// DynamicParticleAdjacency::buildAdjacency over the live slots in slot order
-void build_dynamic_adjacency(DynHost& D, unsigned n) {
-    D.dyn_off.assign(n + 1, 0);
-    D.dnb_off.assign(n + 1, 0);
-    for (int pl = 0; pl < 2; pl++) {
-        const DynHost::Pool& P = D.pool[pl];
-        const int np = pl == POOL_TRI_ROD ? 5 : 4;
-        for (unsigned s = 0; s < P.size; s++) {
-            if (!P.active[s]) continue;
-            for (int k = 0; k < np; k++) {
-                D.dyn_off[P.rec[s].p[k] + 1]++;
-                D.dnb_off[P.rec[s].p[k] + 1] += np - 1;
-            }
-        }
-    }
-    for (unsigned p = 0; p < n; p++) {
-        D.dyn_off[p + 1] += D.dyn_off[p];
-        D.dnb_off[p + 1] += D.dnb_off[p];
-    }
-    D.dyn_ent_ext.assign(D.dyn_off[n], 0);
-    D.dnb.assign(D.dnb_off[n], 0);
-    std::vector<unsigned> ec(D.dyn_off.begin(), D.dyn_off.end() - 1), nc(D.dnb_off.begin(), D.dnb_off.end() - 1);
-    for (int pl = 0; pl < 2; pl++) {  // DynamicEnergyType order: triangle-rigid, triangle-rod
-        const DynHost::Pool& P = D.pool[pl];
-        const unsigned np = pl == POOL_TRI_ROD ? 5 : 4;
-        for (unsigned s = 0; s < P.size; s++) {
-            if (!P.active[s]) continue;
-            const DynHost::Rec& e = P.rec[s];
-            for (unsigned k = 0; k < np; k++) {
-                const unsigned p = e.p[k];
-                D.dyn_ent_ext[ec[p]++] = (s << 4) | ((unsigned)pl << 3) | k;
-                for (unsigned k2 = 0; k2 < np; k2++)
-                    if (k2 != k) D.dnb[nc[p]++] = e.p[k2];
-            }
-        }
-    }
-}
-
 // ---------------------------------------------- recoloring on the device
 // ColorList::incrementalRecoloring, finalizeConflicts and the per-color
 // work lists (common/ColorList.hpp:381-522) over reference particle ids.
@@ -296,12 +257,14 @@ enum : unsigned {
     RC_CNT0 = 0, RC_CNT1 = 1, RC_CUR = 2, RC_NCONFL = 3, RC_NCOLORS = 4, RC_ERR = 5,
     RC_SYNC = 6,   // two words: the cooperative kernel's grid barrier
     RC_BERR = 8,   // its status (AVBD_ERR_BARRIER_TIMEOUT)
+    RC_NENT = 9,   // dynamic entries of the current adjacency
+    RC_AERR = 10,  // the adjacency outgrew its buffers
     RC_NCTR = 12
 };
 constexpr unsigned RC_MAXC = 256;  // colors (ColorList's bitset)
 // summary for the host: [num_colors, dirty count, conflicted count, error,
-// off3[0..256], off6[0..256], offc[0..256]]
-constexpr unsigned RC_SUMMARY = 4 + 3 * (RC_MAXC + 1);
+// off3[0..256], off6[0..256], offc[0..256], dynamic entries]
+constexpr unsigned RC_SUMMARY = 4 + 3 * (RC_MAXC + 1) + 1;
 
 struct RcDev {
     uint32_t *color, *cand, *last_dirty, *dirty0, *dirty1, *ctr;
@@ -471,10 +434,11 @@ AVBD_D void rc_offsets(const RcDev& R, const RcLists& L) {
         }
         off[nc] = run;
     }
+    summary[4 + 3 * (RC_MAXC + 1)] = R.ctr[RC_NENT];
     summary[0] = R.ctr[RC_NCOLORS];
     summary[1] = R.ctr[R.ctr[RC_CUR]];
     summary[2] = R.ctr[RC_NCONFL];
-    summary[3] = R.ctr[RC_ERR] ? 1u : (R.ctr[RC_BERR] ? 2u : 0u);
+    summary[3] = R.ctr[RC_ERR] ? 1u : (R.ctr[RC_BERR] ? 2u : (R.ctr[RC_AERR] ? 3u : 0u));
 }
 
 AVBD_D void rc_fill(const RcDev& R, const RcLists& L, unsigned t0, unsigned dt) {
@@ -548,6 +512,138 @@ __global__ void __launch_bounds__(COOP ? 256 : 1024) k_rc_rounds(RcDev R, uint32
 __global__ void k_rc_count_keep(RcDev R, RcLists L) {
     if (blockIdx.x == 0) rc_keep(R, threadIdx.x, blockDim.x);
     rc_count(R, L, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// ------------------------------------------- dynamic adjacency on the device
+// DynamicParticleAdjacency::buildAdjacency (common/DynamicParticleAdjacency.hpp:33-118)
+// over the live slots of both pools: per engine vertex the entries of its
+// contacts in the reference's order (pool 0 then pool 1, ascending slot) for
+// the solve, whose block sums follow it; per reference particle the other
+// particles of its contacts for the recoloring (a set: any order).
+// Counts, one exclusive scan each, a fill through per-vertex cursors, then
+// each engine vertex's few entries sorted by (pool, slot).
+template <typename R>
+AVBD_D void adj_slot(const ContactPoolDev<R>& P, unsigned pl, unsigned s, unsigned (&ids)[5], unsigned& np) {
+    const uint4 q = P.p[s];
+    np = pl ? 5u : 4u;
+    ids[0] = q.x;
+    ids[1] = q.y;
+    ids[2] = q.z;
+    ids[3] = q.w;
+    ids[4] = pl ? P.p5[s] : 0u;
+}
+
+template <typename R>
+__global__ void k_adj_count(DevState<R> s, unsigned size0, unsigned size1, const uint32_t* __restrict__ perm,
+                            uint32_t* cnt_eng, uint32_t* cnt_ext) {
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned pl = 0;
+    if (k >= size0) {
+        k -= size0;
+        pl = 1;
+        if (k >= size1) return;
+    }
+    const ContactPoolDev<R>& P = s.cp[pl];
+    if (!(P.flag[k] & CF_ACTIVE)) return;
+    unsigned ids[5], np;
+    adj_slot(P, pl, k, ids, np);
+    for (unsigned j = 0; j < np; j++) {
+        atomicAdd(cnt_eng + ids[j], 1u);
+        atomicAdd(cnt_ext + perm[ids[j]], np - 1u);
+    }
+}
+
+// exclusive scan of n + 1 counts (the last is 0) into off, the counts become
+// the fill cursors; one block, a warp per contiguous segment (as the radix
+// sort's histogram scan); total into *total
+__global__ void __launch_bounds__(1024) k_adj_scan(uint32_t* cnt, uint32_t* off, unsigned n1, uint32_t* total) {
+    __shared__ uint32_t wsum[32];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned seg = (n1 + 31u) / 32u;
+    const unsigned b = min(warp * seg, n1), e = min(b + seg, n1);
+    uint32_t t = 0;
+    for (unsigned k = b + lane; k < e; k += 32u) t += cnt[k];
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) t += __shfl_xor_sync(0xffffffffu, t, m);
+    if (lane == 0) wsum[warp] = t;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = wsum[lane];
+        uint32_t incl = v;
+#pragma unroll
+        for (int m = 1; m < 32; m <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, m);
+            if (lane >= (unsigned)m) incl += u;
+        }
+        wsum[lane] = incl - v;
+        if (lane == 31 && total) *total = incl;
+    }
+    __syncthreads();
+    uint32_t carry = wsum[warp];
+    for (unsigned k0 = b; k0 < e; k0 += 32u) {
+        const unsigned k = k0 + lane;
+        const uint32_t v = k < e ? cnt[k] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int m = 1; m < 32; m <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, m);
+            if (lane >= (unsigned)m) incl += u;
+        }
+        if (k < e) {
+            off[k] = carry + incl - v;
+            cnt[k] = carry + incl - v;  // the cursor of vertex k
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+}
+
+template <typename R>
+__global__ void k_adj_fill(DevState<R> s, unsigned size0, unsigned size1, const uint32_t* __restrict__ perm,
+                           uint32_t* cur_eng, uint32_t* cur_ext, uint32_t* dnb, unsigned ent_cap, unsigned dnb_cap,
+                           uint32_t* err) {
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned pl = 0;
+    if (k >= size0) {
+        k -= size0;
+        pl = 1;
+        if (k >= size1) return;
+    }
+    const ContactPoolDev<R>& P = s.cp[pl];
+    if (!(P.flag[k] & CF_ACTIVE)) return;
+    unsigned ids[5], np;
+    adj_slot(P, pl, k, ids, np);
+    for (unsigned j = 0; j < np; j++) {
+        const unsigned pos = atomicAdd(cur_eng + ids[j], 1u);
+        if (pos < ent_cap) s.dyn_ent[pos] = (k << 4) | (pl << 3) | j;
+        else atomicExch(err, 1u);
+        const unsigned e = perm[ids[j]];
+        for (unsigned j2 = 0; j2 < np; j2++) {
+            if (j2 == j) continue;
+            const unsigned q = atomicAdd(cur_ext + e, 1u);
+            if (q < dnb_cap) dnb[q] = perm[ids[j2]];
+            else atomicExch(err, 1u);
+        }
+    }
+}
+
+// each engine vertex's entries in (pool, slot) order
+template <typename R>
+__global__ void k_adj_order(DevState<R> s, unsigned n, unsigned ent_cap) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned b = s.dyn_begin[i], e = min(s.dyn_begin[i + 1], ent_cap);
+    for (unsigned a = b + 1; a < e; a++) {  // insertion sort: a few entries per vertex
+        const uint32_t v = s.dyn_ent[a];
+        const uint32_t key = ((v >> 3) & 1u) << 28 | (v >> 4);
+        unsigned j = a;
+        while (j > b) {
+            const uint32_t w = s.dyn_ent[j - 1];
+            if ((((w >> 3) & 1u) << 28 | (w >> 4)) <= key) break;
+            s.dyn_ent[j] = w;
+            j--;
+        }
+        s.dyn_ent[j] = v;
+    }
 }
 
 RcDev rc_dev(DynHost& D) {
@@ -639,7 +735,8 @@ int alloc_state(avbd_ctx* c, DevState<R>& s, DynHost& D, std::string& err) {
         !alloc((void**)&D.d_confl_ext, sizeof(uint32_t) * n) || !alloc((void**)&D.d_dnb_off, sizeof(uint32_t) * (n + 1)) ||
         !alloc((void**)&D.d_dnb, sizeof(uint32_t) * D.dnb_cap) || !alloc((void**)&D.d_marks, sizeof(uint32_t) * D.marks_cap) ||
         !alloc((void**)&D.d_slab, sizeof(uint32_t) * n) || !alloc((void**)&D.d_ctr, sizeof(uint32_t) * RC_NCTR) ||
-        !alloc((void**)&D.d_lc, sizeof(uint32_t) * 6 * RC_MAXC) || !alloc((void**)&D.d_summary, sizeof(uint32_t) * RC_SUMMARY))
+        !alloc((void**)&D.d_lc, sizeof(uint32_t) * 6 * RC_MAXC) || !alloc((void**)&D.d_summary, sizeof(uint32_t) * RC_SUMMARY) ||
+        !alloc((void**)&D.d_cnt_eng, sizeof(uint32_t) * (n + 1)) || !alloc((void**)&D.d_cnt_ext, sizeof(uint32_t) * (n + 1)))
         return AVBD_ERR_CUDA;
     cudaStream_t st = c->stream;
     cudaMemsetAsync(s.dyn_begin, 0, sizeof(uint32_t) * (n + 1), st);
@@ -739,8 +836,6 @@ int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vecto
     // so each pool holds up to twice the narrow phase's capacity
     D->cap = 2 * c->lbvh.contact_capacity;
     D->num_colors = c->num_colors;
-    D->dyn_off.assign(n + 1, 0);
-    D->dnb_off.assign(n + 1, 0);
     D->off3.assign(D->num_colors + 1, 0);
     D->off6.assign(D->num_colors + 1, 0);
     D->offc.assign(D->num_colors + 1, 0);
@@ -862,6 +957,8 @@ int dyn_recolor_device(avbd_ctx* c, const uint32_t* dyn_begin, const uint8_t* fl
     const uint32_t* h = D.h_summary;
     if (h[3] == 2)
         return set_error(AVBD_ERR_BARRIER_TIMEOUT, "a grid-barrier wait of the recoloring gave up");
+    if (h[3] == 3) return set_error(AVBD_ERR_CAPACITY, "dynamic adjacency exceeds its capacity");
+    D.num_entries = h[4 + 3 * (RC_MAXC + 1)];
     if (h[3]) return set_error(AVBD_ERR_COLORS, "Ran out of colors!");
     D.num_colors = std::min(h[0], RC_MAXC);
     D.dirty_count = h[1];
@@ -923,33 +1020,24 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     std::sort(D.cur.begin(), D.cur.end(), [](const DynHost::Det& a, const DynHost::Det& b) { return a.key < b.key; });
     if (int r = handle_detections(c, D)) return r;
     const unsigned n = (unsigned)c->perm.size();
-    build_dynamic_adjacency(D, n);
 
     // uploads: pool records, dynamic adjacency (engine order for the solve,
     // reference order for the recoloring)
     for (int pl = 0; pl < 2; pl++)
         if (int r = upload_pool<R>(c, s.cp[pl], D.pool[pl], st)) return r;
-    if (D.csr_dirty) {
-        D.dyn_begin.assign(n + 1, 0);
-        for (unsigned i = 0; i < n; i++) {
-            const unsigned e = c->perm[i];
-            D.dyn_begin[i + 1] = D.dyn_begin[i] + (D.dyn_off[e + 1] - D.dyn_off[e]);
-        }
-        D.dyn_ent.resize(D.dyn_begin[n]);
-        for (unsigned i = 0; i < n; i++) {
-            const unsigned e = c->perm[i];
-            std::copy(D.dyn_ent_ext.begin() + D.dyn_off[e], D.dyn_ent_ext.begin() + D.dyn_off[e + 1],
-                      D.dyn_ent.begin() + D.dyn_begin[i]);
-        }
-        if (D.dyn_begin[n] > D.ent_cap) return set_error(AVBD_ERR_CAPACITY, "dynamic adjacency exceeds its capacity");
-        DYN_CUDA(cudaMemcpyAsync(s.dyn_begin, D.dyn_begin.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));
-        if (D.dyn_begin[n])
-            DYN_CUDA(cudaMemcpyAsync(s.dyn_ent, D.dyn_ent.data(), sizeof(uint32_t) * D.dyn_begin[n],
-                                     cudaMemcpyHostToDevice, st));
-        if (D.dnb_off[n] > D.dnb_cap) return set_error(AVBD_ERR_CAPACITY, "dynamic neighbours exceed their capacity");
-        DYN_CUDA(cudaMemcpyAsync(D.d_dnb_off, D.dnb_off.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, st));
-        if (D.dnb_off[n])
-            DYN_CUDA(cudaMemcpyAsync(D.d_dnb, D.dnb.data(), sizeof(uint32_t) * D.dnb_off[n], cudaMemcpyHostToDevice, st));
+    if (D.csr_dirty) {  // contacts came or went: the dynamic adjacency anew, on the device
+        const unsigned s0 = D.pool[0].size, s1 = D.pool[1].size;
+        DYN_CUDA(cudaMemsetAsync(D.d_cnt_eng, 0, sizeof(uint32_t) * (n + 1), st));
+        DYN_CUDA(cudaMemsetAsync(D.d_cnt_ext, 0, sizeof(uint32_t) * (n + 1), st));
+        DYN_CUDA(cudaMemsetAsync(D.d_ctr + RC_AERR, 0, sizeof(uint32_t), st));
+        if (s0 + s1) k_adj_count<R><<<nblk(s0 + s1, 128), 128, 0, st>>>(s, s0, s1, c->d_perm, D.d_cnt_eng, D.d_cnt_ext);
+        k_adj_scan<<<1, 1024, 0, st>>>(D.d_cnt_eng, s.dyn_begin, n + 1, D.d_ctr + RC_NENT);
+        k_adj_scan<<<1, 1024, 0, st>>>(D.d_cnt_ext, D.d_dnb_off, n + 1, nullptr);
+        if (s0 + s1)
+            k_adj_fill<R><<<nblk(s0 + s1, 128), 128, 0, st>>>(s, s0, s1, c->d_perm, D.d_cnt_eng, D.d_cnt_ext, D.d_dnb,
+                                                             D.ent_cap, D.dnb_cap, D.d_ctr + RC_AERR);
+        k_adj_order<R><<<nblk(n, 256), 256, 0, st>>>(s, n, D.ent_cap);
+        count_launch(c, 6);
         D.csr_dirty = false;
     }
     if (int r = dyn_recolor_device(c, s.dyn_begin, s.flags, s.dyn_skip, s.conflicted, st)) return r;
@@ -1009,7 +1097,7 @@ int avbd_dynamic_info(avbd_ctx* c, unsigned out[8]) {
     out[2] = D.num_colors;
     out[3] = D.conflicted_count;
     out[4] = D.dirty_count;
-    out[5] = (unsigned)D.dyn_ent_ext.size();
+    out[5] = D.num_entries;
     out[6] = D.pool[1].count;
     out[7] = D.pool[1].size;
     return AVBD_OK;
