@@ -85,6 +85,8 @@ struct DynHost {
     uint32_t* h_summary = nullptr;               // pinned copy
     unsigned dnb_cap = 0, marks_cap = 0;
     unsigned coop_blocks = 0;                    // grid of the cooperative rounds kernel (0: one block)
+    uint8_t* stage[2] = {nullptr, nullptr};      // pinned staging of each pool's upload
+    size_t stage_cap[2] = {0, 0};
     // ---- per-color lists (engine vertex order) on the device
     std::vector<unsigned> off3, off6, offc;      // per color: recolored 3-DOF, 6-DOF, conflicted
     uint32_t* d_lists = nullptr;
@@ -778,25 +780,44 @@ int download_pool(const ContactPoolDev<R>& S, DynHost::Pool& D, cudaStream_t st)
     return AVBD_OK;
 }
 
+// The pool's records by slot (engine particle ids, state precision) into a
+// pinned staging area that persists across stages, then copied to the device
+// asynchronously: the next stage reuses the area only after its own
+// synchronisation, which follows these copies on the stream.
 template <typename R>
-int upload_pool(avbd_ctx* c, ContactPoolDev<R>& S, const DynHost::Pool& D, cudaStream_t st) {
+int upload_pool(avbd_ctx* c, ContactPoolDev<R>& S, const DynHost::Pool& D, DynHost& H, int pl, cudaStream_t st) {
     using V4 = typename Vec4Of<R>::T;
     const unsigned m = D.size;
     if (m == 0) return AVBD_OK;
-    std::vector<uint4> p(m);
-    std::vector<uint32_t> p5(m, 0);
-    std::vector<V4> vn(m), vt(m), vb(m), vbar(m), vcpl(m), vk(m), vlam(m);
-    std::vector<uint8_t> f(m);
+    const size_t need = (size_t)m * (7 * sizeof(V4) + sizeof(uint4) + sizeof(uint32_t) + 1);
+    if (H.stage_cap[pl] < need) {
+        DYN_CUDA(cudaStreamSynchronize(st));  // copies from the old area are done
+        if (H.stage[pl]) cudaFreeHost(H.stage[pl]);
+        H.stage[pl] = nullptr;
+        H.stage_cap[pl] = 0;
+        DYN_CUDA(cudaMallocHost((void**)&H.stage[pl], 2 * need));
+        H.stage_cap[pl] = 2 * need;
+    }
+    uint8_t* base = H.stage[pl];
+    V4* vn = reinterpret_cast<V4*>(base);
+    V4 *vt = vn + m, *vb = vt + m, *vbar = vb + m, *vcpl = vbar + m, *vk = vcpl + m, *vlam = vk + m;
+    uint4* p = reinterpret_cast<uint4*>(vlam + m);
+    uint32_t* p5 = reinterpret_cast<uint32_t*>(p + m);
+    uint8_t* f = reinterpret_cast<uint8_t*>(p5 + m);
     auto v4 = [](const double a[3], double w) {
         V4 o;
         o.x = (R)a[0]; o.y = (R)a[1]; o.z = (R)a[2]; o.w = (R)w;
         return o;
     };
+    const double z3[3] = {0, 0, 0};
+    const V4 zero = v4(z3, 0);
     for (unsigned i = 0; i < m; i++) {
         const DynHost::Rec& e = D.rec[i];
         if (!D.active[i]) {
             f[i] = 0;
             p[i] = make_uint4(0, 0, 0, 0);
+            p5[i] = 0;
+            vn[i] = vt[i] = vb[i] = vbar[i] = vcpl[i] = vk[i] = vlam[i] = zero;
             continue;
         }
         p[i] = make_uint4(c->inv[e.p[0]], c->inv[e.p[1]], c->inv[e.p[2]], c->inv[e.p[3]]);
@@ -810,18 +831,16 @@ int upload_pool(avbd_ctx* c, ContactPoolDev<R>& S, const DynHost::Pool& D, cudaS
         vlam[i] = v4(e.lam, e.lam[3]);
         f[i] = e.flag;
     }
-    DYN_CUDA(cudaMemcpyAsync(S.p, p.data(), sizeof(uint4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.p5, p5.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.n, vn.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.t, vt.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.b, vb.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.bar, vbar.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.cpl, vcpl.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.k, vk.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.lam, vlam.data(), sizeof(V4) * m, cudaMemcpyHostToDevice, st));
-    DYN_CUDA(cudaMemcpyAsync(S.flag, f.data(), m, cudaMemcpyHostToDevice, st));
-    // the host vectors are pageable: the copies complete before the call returns
-    DYN_CUDA(cudaStreamSynchronize(st));
+    DYN_CUDA(cudaMemcpyAsync(S.p, p, sizeof(uint4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.p5, p5, sizeof(uint32_t) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.n, vn, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.t, vt, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.b, vb, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.bar, vbar, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.cpl, vcpl, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.k, vk, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.lam, vlam, sizeof(V4) * m, cudaMemcpyHostToDevice, st));
+    DYN_CUDA(cudaMemcpyAsync(S.flag, f, m, cudaMemcpyHostToDevice, st));
     return AVBD_OK;
 }
 
@@ -887,7 +906,12 @@ int dyn_create(avbd_ctx* c, const std::vector<unsigned>& p_off, const std::vecto
 }
 
 void dyn_destroy(avbd_ctx* c) {
-    if (c->dyn && c->dyn->h_summary) cudaFreeHost(c->dyn->h_summary);
+    if (c->dyn) {
+        if (c->dyn->h_summary || c->dyn->stage[0] || c->dyn->stage[1]) cudaStreamSynchronize(c->stream);
+        if (c->dyn->h_summary) cudaFreeHost(c->dyn->h_summary);
+        for (uint8_t* b : c->dyn->stage)
+            if (b) cudaFreeHost(b);
+    }
     delete c->dyn;
     c->dyn = nullptr;
 }
@@ -1024,7 +1048,7 @@ int dyn_manage(avbd_ctx* c, DevState<R>& s, const StepConsts& k, cudaStream_t st
     // uploads: pool records, dynamic adjacency (engine order for the solve,
     // reference order for the recoloring)
     for (int pl = 0; pl < 2; pl++)
-        if (int r = upload_pool<R>(c, s.cp[pl], D.pool[pl], st)) return r;
+        if (int r = upload_pool<R>(c, s.cp[pl], D.pool[pl], D, pl, st)) return r;
     if (D.csr_dirty) {  // contacts came or went: the dynamic adjacency anew, on the device
         const unsigned s0 = D.pool[0].size, s1 = D.pool[1].size;
         DYN_CUDA(cudaMemsetAsync(D.d_cnt_eng, 0, sizeof(uint32_t) * (n + 1), st));
