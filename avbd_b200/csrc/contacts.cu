@@ -489,6 +489,9 @@ __global__ void __launch_bounds__(COOP ? 256 : 1024) k_rc_rounds(RcDev R, uint32
         __syncthreads();
         return true;
     };
+    // an adjacency that outgrew its buffers is not read (the stage reports
+    // AVBD_ERR_CAPACITY); every block returns here, before any barrier
+    if (R.ctr[RC_AERR]) return;
     const unsigned cur0 = R.ctr[RC_CUR];
     for (unsigned p = t0; p < n; p += dt) R.confl[p] = 0;  // the last stage's conflicts
     for (unsigned k = t0; k < 6 * RC_MAXC; k += dt) lc[k] = 0;
