@@ -17,17 +17,19 @@
 //   VBDSolver::_commitConflictedInColor                      simulation/VBDSolver.hpp:82-87,108-119
 //
 // Layout.  The narrow phase leaves its detections on the device; the host
-// reads them with the pool's multipliers, runs the merge, the tombstone pool,
-// the dynamic adjacency and the incremental recoloring in the reference's
-// particle numbering (the order the recoloring's "lower index" rule and the
-// pool's slot order depend on), then uploads the pool records and, in the
-// engine's color-major vertex order, the dynamic adjacency, the conflict
-// flags and per-color lists.  The vertex slabs of the static coloring stay in
-// place: a vertex with contacts or a color changed by the recoloring is
-// skipped by its slab's launch and solved from its color's list by the
-// solve's dynamic instantiation; colors beyond the static ones have lists
-// only.  The pool is small (tens to thousands of contacts per step), so this
-// host pass costs less than one of the step's sweeps.
+// reads them with the pool's multipliers and runs the key-ordered merge and
+// the tombstone pool (slots are popped and pushed in key order), then
+// uploads the pool records and the particles to mark dirty.  On the device:
+// the dynamic adjacency when contacts came or went (engine vertex order for
+// the solve, reference particle numbering for the recoloring), the
+// incremental recoloring in the reference's numbering (its "lower index"
+// rule depends on it), the conflicts and the per-color lists in the engine's
+// color-major vertex order; the color count and list offsets come back to
+// the host, which launches the stage's sweeps.  The vertex slabs of the
+// static coloring stay in place: a vertex with contacts or a color changed by
+// the recoloring is skipped by its slab's launch and solved from its color's
+// list by the solve's dynamic instantiation; colors beyond the static ones
+// have lists only.
 #include <algorithm>
 #include <cmath>
 
