@@ -916,6 +916,7 @@ template <typename R>
 void launch_chebyshev_dual(avbd_ctx* c, DevState<R>& s, const StepConsts& k, double omega, unsigned it,
                            cudaStream_t st, const SceneTol& T) {
     (void)k;
+    if (s.no == s.n) return;  // every particle oriented: k_chebyshev_rot covers them
     k_chebyshev_dual<R><<<nblocks(s.n, 256), 256, 0, st>>>(s, (R)omega, it, T);
     count_launch(c);
 }
