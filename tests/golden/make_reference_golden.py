@@ -1,7 +1,7 @@
 """Writes tests/golden/reference_outputs.npz: outputs of the reference
 implementation itself (oracle/_ref/libavbd_ref.so, built from the reference's
 unmodified sources by oracle/Makefile) on seeded synthetic scenes of the
-BASELINE shapes.
+benchmark configurations' shapes.
 
     python tests/golden/make_reference_golden.py
 

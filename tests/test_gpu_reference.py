@@ -9,8 +9,7 @@ Here the CUDA engine runs the same scenes through the C-ABI:
   candidate pairs of the step-1 collision stage are identical (FP64 inputs);
 * positions stay within the stated fraction of the bounding-box diagonal of
   the reference's: 1e-9 for the FP64 engine, 1e-6 for MIXED (FP32 element
-  records), 1e-5 for FP32 on the C1 cube (no contact), the bars
-  BASELINE's north star states for this comparison;
+  records), 1e-5 for FP32 on the C1 cube (no contact);
 * contact pools (slots, particles) are identical and their multipliers agree
   to 1e-6 relative.
 """
