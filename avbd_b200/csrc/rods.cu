@@ -388,7 +388,7 @@ enum { RMODE_SOLVE = 0, RMODE_RESIDUAL = 1, RMODE_DEBUG = 2 };
 // (A_s = S A S, S = diag(A)^-1/2) and an LDL^T factorisation of A_s.  A rod
 // node's block mixes translational stiffness (EA/L ~ 1e5 N/m) with
 // rotational terms (EI/L ~ 1 N m) and has a 2-norm condition number ~2e5;
-// scaled, ~2 (at most ~10 on the C3 scene).  Returns the pivot ratio
+// scaled, ~2 (at most ~10 on 256 rods of 100 segments).  Returns the pivot ratio
 // max(d)/min(d) of the scaled factorisation as the condition estimate
 // (infinite when a pivot is not positive); the caller re-solves in FP64
 // above its threshold.
