@@ -60,3 +60,22 @@ def test_kernels_are_sm100a(lib):
     out = subprocess.run(["cuobjdump", "--list-elf", os.path.join(ROOT, "avbd_b200", "libavbd_b200.so")],
                          capture_output=True, text=True).stdout
     assert "sm_100a" in out
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/avbd.h is what a cgo / FFI binding includes: it must compile as
+    strict C99 on its own."""
+    src = tmp_path / "c_abi.c"
+    src.write_text('#include "avbd.h"\nint main(void) { return avbd_version() == 0; }\n')
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                           "-I" + os.path.join(ROOT, "include"), "-fsyntax-only", str(src)])
+
+
+def test_cpp_facade_compiles_and_links(lib, tmp_path):
+    """The C++ facade (include/avbd/avbd.hpp) with its test program compiles
+    warning-free and links against the library (run by the GPU tests)."""
+    lib_dir = os.path.join(ROOT, "avbd_b200")
+    subprocess.check_call(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-O2",
+                           "-I" + os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "facade_step.cpp"),
+                           "-L" + lib_dir, "-lavbd_b200", "-Wl,-rpath," + lib_dir, "-o", str(tmp_path / "facade_step")])
+    assert (tmp_path / "facade_step").exists()
