@@ -56,6 +56,21 @@ def test_standardise_keeps_the_padding_neutral():
     assert np.allclose(mean[live], 2.0, atol=0.2) and np.allclose(std[live], 3.0, rtol=0.1)
 
 
+def test_residual_weights_grow_with_the_block_stiffness():
+    from avbd_b200.train_warmstart import residual_weights
+    F = torch.zeros((3, warmstart.IN_PAD), dtype=torch.bfloat16)
+    # features 18-20: log(1 + H_aa h^2 / m) = 0, log 2, log 101
+    for r, lam in enumerate((0.0, 1.0, 100.0)):
+        F[r, 18:21] = float(np.log1p(lam))
+    w = residual_weights(F)
+    assert abs(float(w.mean()) - 1.0) < 1e-6
+    # (1 + mean_a H_aa h^2/m)^2 of the BF16-rounded features, normalised
+    lam = np.expm1(F[:, 18:21].float().numpy().astype(np.float64)).mean(1)
+    raw = (1.0 + lam) ** 2
+    assert np.allclose(w.numpy(), raw / raw.mean(), rtol=1e-5)
+    assert w[0] < w[1] < w[2]
+
+
 def test_fold_gives_the_raw_feature_network():
     rng = np.random.default_rng(2)
     p = _random_params(4)
