@@ -59,6 +59,35 @@ def test_batched_scene_count():
     assert len(r.calls["add_particles"]) == 5
 
 
+def test_benchmark_batch_sizes_and_ranges():
+    """The 1024-cube batch of seed 0: 4,921,807 vertices and 25,132,554 tets,
+    n in 4..24 cells per side, E in [1e4, 1e7], nu in [0.3, 0.49]."""
+    P = [scenes.batched_cube_params(0, s) for s in range(1024)]
+    n = np.array([p[0] for p in P])
+    E = np.array([p[1] for p in P])
+    nu = np.array([p[2] for p in P])
+    assert int(((n + 1) ** 3).sum()) == 4_921_807 and int((6 * n ** 3).sum()) == 25_132_554
+    assert n.min() == 4 and n.max() == 24
+    assert 1e4 <= E.min() and E.max() <= 1e7 and 0.3 <= nu.min() and nu.max() <= 0.49
+    for P0 in P[:4]:
+        R = P0[3]
+        assert np.allclose(R @ R.T, np.eye(3), atol=1e-12) and np.isclose(np.linalg.det(R), 1.0)
+
+
+def test_batch_subset_reproduces_its_scenes():
+    """A subset of the batch (the CPU baselines' samples, the parity tests'
+    scenes) holds exactly the cubes the full batch has at those ids."""
+    def particles(ids):
+        r = Recorder()
+        scenes.batched_cubes(num_scenes=1024, seed=0, scene_ids=ids).load(r)
+        return r.calls["add_particles"]
+    a = particles([2, 5, 9])
+    b = particles([9])
+    c = particles([5])
+    assert np.array_equal(a[2][0], b[0][0]) and np.array_equal(a[2][1], b[0][1])
+    assert np.array_equal(a[1][0], c[0][0])
+
+
 def test_rods_and_spheres_setup():
     """Rod::Rod set-up (simobject/Rod.cpp:10-68): lumped masses and inertias,
     Cosserat stiffness, frames advanced by Exp_s3(kappa ds)."""
