@@ -44,6 +44,33 @@ def test_traffic_estimate_scales_the_measured_ratio(bench):
     assert bench.traffic_for("no_such_workload", 1e9) is None
 
 
+def test_clock_record_from_sampler_rows(bench, tmp_path):
+    """The clocks object of the JSON line from nvidia-smi's CSV rows: the
+    median SM clock of the samples under load (above half the maximum), the
+    maximum, and every throttle reason seen active."""
+    class Done:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    rows = ["0, 345, 1965, 150.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "0, 1800, 1965, 990.5, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1830, 1965, 995.0, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1950, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "garbage line"]
+    path = tmp_path / "clocks.csv"
+    path.write_text("\n".join(rows) + "\n")
+    c = bench.Clocks(0)
+    c.proc, c.path = Done(), str(path)
+    rec = c.stop()
+    assert rec == {"sm_mhz": 1830.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 4}
+    assert not path.exists()
+    # no sampler (nvidia-smi missing): no record
+    assert bench.Clocks(0).stop() is None
+
+
 def test_batch_partition_is_balanced_by_tets():
     from avbd_b200 import dist
     from avbd_b200.scenes import batched_cube_params
