@@ -71,6 +71,18 @@ def test_clock_record_from_sampler_rows(bench, tmp_path):
     assert bench.Clocks(0).stop() is None
 
 
+def test_reference_arm_runs_on_rank_zero_only():
+    """Under torchrun the reference arm's rank 0 alone times the CPU
+    reference; the other ranks exit 0 without work or output."""
+    import subprocess
+    import sys
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
+
+
 def test_batch_partition_is_balanced_by_tets():
     from avbd_b200 import dist
     from avbd_b200.scenes import batched_cube_params
